@@ -1,0 +1,87 @@
+/* gpu_rules_api.h — C ABI of libgpu_rules.so (B200 engine).
+ *
+ * Drop-in replacement for the reference library's interface
+ * (GPU_03/gpu_rules_api.h): the five reference entry points keep their
+ * names, argument meaning, return codes and the result struct layout, so
+ * the existing Scala/JNA binding (GPU_03/GpuRulesLib.scala:23-58) loads this
+ * library unchanged.  The remaining entry points are additive.
+ *
+ * Counting semantics are those of the reference's CPU implementation
+ * (CPU_01_nonparallel/SupportCounting.cpp): injective variable bindings, no
+ * ground triple used twice in one grounding (the head triple included for
+ * support), and the body size always computed.
+ */
+#ifndef GPU_RULES_API_H
+#define GPU_RULES_API_H
+
+#include <stddef.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* Result of one rule.  Same fields, order and natural alignment as the
+ * reference (GPU_03/gpu_rules_api.h:21-30): 56 bytes on x86-64 with offsets
+ * 0, 4, 8, 16, 24, 32, 40, 48.  Counts above INT_MAX saturate at INT_MAX. */
+typedef struct {
+    int    support;       /* head triples whose body has a grounding          */
+    int    headSize;      /* triples of the head predicate                     */
+    int    headSupport;   /* head triples matching the head's constants        */
+    double headCoverage;  /* support / headSize (0 when headSize is 0)         */
+    int    bodySize;      /* distinct (hS, hO) pairs with a body grounding     */
+    double confidence;    /* support / bodySize (0 when bodySize is 0)         */
+    double supportMs;     /* device time of the support phase (ms)             */
+    double confidenceMs;  /* device time of the body-size phase (ms)           */
+} GpuRuleResult;
+
+/* Replaces gpu_load_graph (GPU_03/gpu_rules_api.h:43).
+ * Parses the Turtle file, builds the index and keeps it resident on the
+ * current CUDA device.  Returns an opaque context, or NULL on a parse,
+ * memory or CUDA error (the process is never terminated). */
+void* gpu_load_graph(const char* ttlPath);
+
+/* Replaces gpu_evaluate_rule (GPU_03/gpu_rules_api.h:59).
+ * Evaluates one rule in the text syntax, e.g.
+ *   "(?a <http://ex/livesIn> ?b) => (?a <http://ex/bornIn> ?b)"
+ * One device launch per phase.  Returns 0 on success (also for rules the
+ * engine does not support: more than 8 body atoms or 16 variables, which
+ * yield zero measures except headSize/headSupport, as in the reference),
+ * -1 on null arguments, a malformed rule or a CUDA error.
+ * Not thread-safe within one context; distinct contexts are independent. */
+int gpu_evaluate_rule(void* ctx, const char* ruleText, GpuRuleResult* out);
+
+/* Replaces gpu_evaluate_rule_json (GPU_03/gpu_rules_api.h:72).
+ * Same as gpu_evaluate_rule for one rule in the RDFRules JSON export format. */
+int gpu_evaluate_rule_json(void* ctx, const char* ruleJson, GpuRuleResult* out);
+
+/* Replaces gpu_free_graph (GPU_03/gpu_rules_api.h:79).  NULL is ignored. */
+void gpu_free_graph(void* ctx);
+
+/* Replaces gpu_query_vram (GPU_03/gpu_rules_api.h:87).
+ * Free and total memory of the current device; 0 on success, -1 without a
+ * CUDA device. */
+int gpu_query_vram(size_t* freeBytesOut, size_t* totalBytesOut);
+
+/* ---- additive entry points (no counterpart in the reference) ---- */
+
+/* Evaluates n rules (text, or JSON when isJson != 0) in one persistent
+ * device launch that covers both phases of every rule.  out[i] receives
+ * rule i's result; status[i] (optional) receives 0 on success or -1 when
+ * rule i does not parse (its result is then zero).  deviceMs (optional)
+ * receives the device time of the whole batch.  Per-rule supportMs and
+ * confidenceMs are 0 in this mode.  Returns 0, or -1 on null arguments or a
+ * CUDA error. */
+int gpu_evaluate_rules_batch(void* ctx, const char* const* rules, int n, int isJson,
+                             GpuRuleResult* out, int* status, double* deviceMs);
+
+/* Number of entities, predicates and distinct triples of a loaded graph. */
+int gpu_graph_stats(void* ctx, long long* entities, long long* predicates, long long* triples);
+
+/* Last error message of the calling thread ("" if none). */
+const char* gpu_last_error(void);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* GPU_RULES_API_H */

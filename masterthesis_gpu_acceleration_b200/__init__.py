@@ -1,0 +1,170 @@
+"""B200 rule-evaluation engine: Python host binding of libgpu_rules.so.
+
+This mirrors the reference's JVM binding (GPU_03/GpuRulesLib.scala:23-116):
+``GpuRuleResult`` has the same fields in the same order, and ``GpuRulesLib``
+checks device memory, loads the graph once, evaluates rules one by one and
+frees the graph on ``close()``.  ``evaluate_rules_batch`` is the additive
+batched entry point (one persistent device launch for many rules).
+
+Everything below calls the compiled library; there is no Python or CPU
+evaluation path.  Importing works without a GPU; loading a graph needs one.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+from pathlib import Path
+from typing import Sequence
+
+PKG_DIR = Path(__file__).resolve().parent
+LIB_DIR = PKG_DIR / "lib"
+LIB_PATH = LIB_DIR / "libgpu_rules.so"
+
+#: symbols declared in include/gpu_rules_api.h
+API_SYMBOLS = (
+    "gpu_load_graph",
+    "gpu_evaluate_rule",
+    "gpu_evaluate_rule_json",
+    "gpu_free_graph",
+    "gpu_query_vram",
+    "gpu_evaluate_rules_batch",
+    "gpu_graph_stats",
+    "gpu_last_error",
+)
+
+
+class GpuRuleResult(ctypes.Structure):
+    """Same layout as GpuRuleResult in include/gpu_rules_api.h (56 bytes)."""
+
+    _fields_ = [
+        ("support", ctypes.c_int),
+        ("headSize", ctypes.c_int),
+        ("headSupport", ctypes.c_int),
+        ("headCoverage", ctypes.c_double),
+        ("bodySize", ctypes.c_int),
+        ("confidence", ctypes.c_double),
+        ("supportMs", ctypes.c_double),
+        ("confidenceMs", ctypes.c_double),
+    ]
+
+    def as_dict(self) -> dict:
+        return {name: getattr(self, name) for name, _ in self._fields_}
+
+    def __repr__(self) -> str:  # mirrors GpuRulesLib.scala:39-42
+        return (f"support={self.support}, headSize={self.headSize}, headCoverage={self.headCoverage}, "
+                f"bodySize={self.bodySize}, confidence={self.confidence}, "
+                f"supportMs={self.supportMs} ms, confidenceMs={self.confidenceMs} ms")
+
+
+_lib = None
+
+
+def load_library(path: os.PathLike | str | None = None) -> ctypes.CDLL:
+    """Loads libgpu_rules.so (built in-tree); raises if it is missing."""
+    global _lib
+    if _lib is not None and path is None:
+        return _lib
+    p = Path(path) if path is not None else LIB_PATH
+    if not p.exists():
+        raise RuntimeError(f"{p} is missing: build it with `python -m masterthesis_gpu_acceleration_b200.build`")
+    lib = ctypes.CDLL(str(p))
+    lib.gpu_load_graph.restype = ctypes.c_void_p
+    lib.gpu_load_graph.argtypes = [ctypes.c_char_p]
+    lib.gpu_evaluate_rule.restype = ctypes.c_int
+    lib.gpu_evaluate_rule.argtypes = [ctypes.c_void_p, ctypes.c_char_p, ctypes.POINTER(GpuRuleResult)]
+    lib.gpu_evaluate_rule_json.restype = ctypes.c_int
+    lib.gpu_evaluate_rule_json.argtypes = [ctypes.c_void_p, ctypes.c_char_p, ctypes.POINTER(GpuRuleResult)]
+    lib.gpu_free_graph.restype = None
+    lib.gpu_free_graph.argtypes = [ctypes.c_void_p]
+    lib.gpu_query_vram.restype = ctypes.c_int
+    lib.gpu_query_vram.argtypes = [ctypes.POINTER(ctypes.c_size_t), ctypes.POINTER(ctypes.c_size_t)]
+    lib.gpu_evaluate_rules_batch.restype = ctypes.c_int
+    lib.gpu_evaluate_rules_batch.argtypes = [
+        ctypes.c_void_p, ctypes.POINTER(ctypes.c_char_p), ctypes.c_int, ctypes.c_int,
+        ctypes.POINTER(GpuRuleResult), ctypes.POINTER(ctypes.c_int), ctypes.POINTER(ctypes.c_double)]
+    lib.gpu_graph_stats.restype = ctypes.c_int
+    lib.gpu_graph_stats.argtypes = [ctypes.c_void_p] + [ctypes.POINTER(ctypes.c_longlong)] * 3
+    lib.gpu_last_error.restype = ctypes.c_char_p
+    lib.gpu_last_error.argtypes = []
+    if path is None:
+        _lib = lib
+    return lib
+
+
+def query_vram() -> tuple[int, int]:
+    """(free, total) bytes of the current device; raises without a device."""
+    lib = load_library()
+    free, total = ctypes.c_size_t(), ctypes.c_size_t()
+    if lib.gpu_query_vram(ctypes.byref(free), ctypes.byref(total)) != 0:
+        raise RuntimeError("gpu_query_vram failed — no CUDA device?")
+    return free.value, total.value
+
+
+class GpuRulesLib:
+    """Graph resident on the GPU between calls (GPU_03/GpuRulesLib.scala:61-116)."""
+
+    def __init__(self, ttl_path: os.PathLike | str):
+        self._lib = load_library()
+        query_vram()
+        ctx = self._lib.gpu_load_graph(str(ttl_path).encode())
+        if not ctx:
+            err = self._lib.gpu_last_error().decode(errors="replace")
+            raise RuntimeError(f"gpu_load_graph failed for: {ttl_path} ({err})")
+        self._ctx = ctypes.c_void_p(ctx)
+
+    # -- reference entry points -------------------------------------------------
+    def evaluate_rule(self, rule_text: str) -> GpuRuleResult:
+        res = GpuRuleResult()
+        rc = self._lib.gpu_evaluate_rule(self._handle(), rule_text.encode(), ctypes.byref(res))
+        if rc != 0:
+            raise RuntimeError(f"gpu_evaluate_rule error code {rc} for: {rule_text} "
+                               f"({self._lib.gpu_last_error().decode(errors='replace')})")
+        return res
+
+    def evaluate_rule_json(self, rule_json: str) -> GpuRuleResult:
+        res = GpuRuleResult()
+        rc = self._lib.gpu_evaluate_rule_json(self._handle(), rule_json.encode(), ctypes.byref(res))
+        if rc != 0:
+            raise RuntimeError(f"gpu_evaluate_rule_json error code {rc}")
+        return res
+
+    # -- additive entry points ---------------------------------------------------
+    def evaluate_rules_batch(self, rules: Sequence[str], is_json: bool = False):
+        """Returns (results, statuses, device_ms) for all rules in one launch."""
+        n = len(rules)
+        arr = (ctypes.c_char_p * max(n, 1))(*[r.encode() for r in rules])
+        out = (GpuRuleResult * max(n, 1))()
+        st = (ctypes.c_int * max(n, 1))()
+        ms = ctypes.c_double()
+        rc = self._lib.gpu_evaluate_rules_batch(self._handle(), arr, n, int(is_json), out, st, ctypes.byref(ms))
+        if rc != 0:
+            raise RuntimeError(f"gpu_evaluate_rules_batch failed "
+                               f"({self._lib.gpu_last_error().decode(errors='replace')})")
+        return list(out)[:n], list(st)[:n], ms.value
+
+    def stats(self) -> dict:
+        e, p, t = ctypes.c_longlong(), ctypes.c_longlong(), ctypes.c_longlong()
+        self._lib.gpu_graph_stats(self._handle(), ctypes.byref(e), ctypes.byref(p), ctypes.byref(t))
+        return {"entities": e.value, "predicates": p.value, "triples": t.value}
+
+    def close(self) -> None:
+        if getattr(self, "_ctx", None) is not None and self._ctx.value:
+            self._lib.gpu_free_graph(self._ctx)
+            self._ctx = None
+
+    def _handle(self):
+        if self._ctx is None:
+            raise RuntimeError("graph already freed")
+        return self._ctx
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass

@@ -1,0 +1,136 @@
+// common.hpp — types shared by the host planner and the device engine.
+//
+// Limits follow the reference (GPU_03/gpu_common.cuh:25-27): at most 16
+// distinct variables and 8 body atoms per rule.
+#pragma once
+#include <cstdint>
+#ifndef __CUDACC__
+#define __host__
+#define __device__
+#endif
+
+namespace gr {
+
+constexpr int kMaxVars = 16;
+constexpr int kMaxBody = 8;
+constexpr int kMaxConsts = 20;
+constexpr int kTupleHead = 2;                  // [root index, hO rank]
+constexpr int kMaxTuple = kTupleHead + kMaxVars;
+constexpr int kMaxChecks = 16;
+constexpr int kMaxUsed = 40;
+
+// One slot of the (predicate, direction, key) -> edge range table.
+// tag = pred * 2 + dir; tag 0xffffffff marks an empty slot.
+struct alignas(16) HashSlot {
+    uint32_t tag, key, beg, end;
+};
+constexpr uint32_t kEmptyTag = 0xffffffffu;
+
+__host__ __device__ inline uint32_t slot_hash(uint32_t tag, uint32_t key) {
+    uint64_t x = ((uint64_t)tag << 32) | key;
+    x ^= x >> 33; x *= 0xff51afd7ed558ccdull;
+    x ^= x >> 33; x *= 0xc4ceb9fe1a85ec53ull;
+    x ^= x >> 33;
+    return (uint32_t)x;
+}
+
+// Device-resident graph index.  Triples are stored once per direction:
+// dir 0 (SPO) keys edges by subject and stores objects as values, dir 1
+// (POS) keys them by object and stores subjects.  Within a direction edges
+// are sorted by (predicate, key, value), so each (predicate, key) row is a
+// contiguous, sorted run of values.
+struct DevIndex {
+    // per direction, per edge
+    const int32_t* val[2];       // neighbour value
+    const int32_t* valRank[2];   // rank of the value among the predicate's distinct values
+                                 // in that position (= its row index in the other direction)
+    const int32_t* src[2];       // the edge's key
+    const int32_t* srcRank[2];   // rank of the key among the predicate's keys in this direction
+    // per direction, per row
+    const int32_t* rowKey[2];
+    const int32_t* rowBeg[2];    // rows + 1 entries (edge offsets)
+    // per direction, per predicate
+    const int32_t* predRow[2];   // P + 1 entries
+    const int32_t* predEdge[2];  // P + 1 entries
+    // (predicate, direction, key) -> edge range, open addressing
+    const struct HashSlot* hash;
+    uint32_t hashMask;
+    int32_t nPred;
+    int32_t nEnt;
+    int64_t nTriples;
+};
+
+// Term reference inside a plan: r >= 0 is a tuple position; r < 0 is
+// constant number (-1 - r).
+using TermRef = int16_t;
+
+struct DevCheck {        // membership filter: the triple (s, pred, o) must exist
+    int32_t pred;
+    TermRef s, o;
+    int8_t dir;          // direction probed (0: key = s, 1: key = o)
+    int8_t pad[3];
+};
+
+struct DevUsed {         // used-triple rule: reject when the two triples are equal
+    TermRef sA, oA, sB, oB;
+};
+
+enum StepKind : int8_t { kExpand = 0, kScan = 1 };
+
+struct DevStep {
+    int32_t pred;
+    int8_t dir;          // EXPAND: direction of the lookup; SCAN: always 0
+    int8_t kind;
+    int8_t sameVar;      // SCAN with one variable in both positions
+    int8_t nNew;         // values appended to the tuple (1 or 2)
+    TermRef keyRef;      // EXPAND: the bound key
+    int8_t hoWhich;      // 0: hO not bound here; 1/2: hO is the first/second new value
+    int8_t pad;
+};
+
+enum PlanMode : int32_t { kExist = 0, kPairs = 1 };
+enum RootKind : int32_t { kRootEdges = 0, kRootRows = 1 };
+
+// One phase (support or body size) of one rule.
+struct DevPlan {
+    int32_t mode;            // kExist: count roots with a grounding; kPairs: count distinct (root, hO)
+    int32_t m;               // binding steps
+    int32_t resultSlot;      // index into the u64 result array
+    int32_t rootKind;        // kRootEdges: edges of rootDir in [task.beg, task.end)
+                             // kRootRows: rows of rootDir in [task.beg, task.end), hS = row key
+    int32_t rootDir;
+    int32_t rootPred;
+    int8_t rootAppendKey;    // edges: append the edge key to the tuple
+    int8_t rootAppendVal;    // edges: append the edge value
+    int8_t rootKeyEqVal;     // edges: require key == value
+    int8_t rootKeyNeVal;     // edges: require key != value
+    TermRef rootValConst;    // edges: require value == constant (-1 - k), or 0 for none
+    int16_t pad0;
+    // filters per level (level 0 = roots, level l = after step l)
+    int8_t chkBeg[kMaxBody + 1], chkN[kMaxBody + 1];
+    int8_t usedBeg[kMaxBody + 1], usedN[kMaxBody + 1];
+    int32_t wo;              // kPairs: bitmap row width (size of hO's value domain)
+    int32_t hoLevel;         // kPairs: level whose step binds hO (1..m)
+    int32_t cap;             // frontier capacity per level (items)
+    int32_t groupMax;        // max roots per task
+    int32_t tupleLen[kMaxBody + 1];
+    int32_t consts[kMaxConsts];
+    DevStep steps[kMaxBody];
+    DevCheck checks[kMaxChecks];
+    DevUsed used[kMaxUsed];
+    uint32_t* gBitmap;            // kPairs with a global bitmap (null: shared memory)
+    int64_t gRowBase;             // first root of the plan, for global bitmap rows
+};
+
+struct DevTask {
+    int32_t plan;
+    int32_t beg, end;        // root range
+    int32_t pad;
+};
+
+// Engine launch geometry and shared-memory budget.
+constexpr int kBlock = 512;
+constexpr int kItemInts = 8192;        // frontier storage per block (ints)
+constexpr int kBitmapWords = 16384;    // per-block dedup bitmap (u32 words) = 64 KiB
+
+}  // namespace gr

@@ -1,0 +1,38 @@
+// index.hpp — host-side graph index (the device copy mirrors it).
+#pragma once
+#include <cstdint>
+#include <utility>
+#include <vector>
+
+#include "common.hpp"
+
+namespace gr {
+
+struct HostIndex {
+    int32_t nPred = 0, nEnt = 0;
+    int64_t nTriples = 0;
+    std::vector<int32_t> val[2], valRank[2], src[2], srcRank[2];
+    std::vector<int32_t> rowKey[2], rowBeg[2];
+    std::vector<int32_t> predRow[2], predEdge[2];
+    std::vector<HashSlot> hash;
+    uint32_t hashMask = 0;
+
+    int64_t pred_size(int32_t p) const {
+        return (p < 0 || p >= nPred) ? 0 : predEdge[0][p + 1] - predEdge[0][p];
+    }
+    int64_t pred_rows(int32_t p, int d) const {
+        return (p < 0 || p >= nPred) ? 0 : predRow[d][p + 1] - predRow[d][p];
+    }
+    // Edge range [beg, end) of row (p, d, key); (0, 0) if absent.
+    std::pair<int32_t, int32_t> row_range(int32_t p, int d, int32_t key) const;
+    bool has_triple(int32_t p, int32_t s, int32_t o) const;
+    double avg_degree(int32_t p, int d) const {
+        int64_t r = pred_rows(p, d);
+        return r ? (double)pred_size(p) / (double)r : 0.0;
+    }
+};
+
+// Builds the index from (s, p, o) triples (duplicates removed).
+HostIndex build_index(const std::vector<int32_t>& spo, int32_t nEnt, int32_t nPred);
+
+}  // namespace gr

@@ -1,0 +1,401 @@
+// kernels.cu — the rule-evaluation engine for sm_100a.
+//
+// One persistent kernel serves both phases of every rule.  Blocks pull
+// tasks (a plan and a range of roots) from a device queue.  A task is
+// evaluated as a depth-first search over *chunks*: the block keeps, for each
+// plan level, a bounded frontier of partial bindings in shared memory and
+// always extends the deepest level that still has work.  Extending a level
+// lays the neighbour lists of up to kBlock frontier items end to end (one
+// hash lookup per item, a block-wide prefix sum) and hands the resulting
+// candidates to threads one per slot, so a hub with 50,000 neighbours is
+// spread over the whole block instead of serialising one thread.  Frontier
+// memory is bounded by construction (each round produces at most `cap`
+// items), so any fan-out fits.
+//
+// Outputs:
+//  * kExist: roots with at least one complete grounding (a bit per root);
+//    support counts head triples, body size with hS == hO counts hS values.
+//  * kPairs: distinct (root, hO) pairs for the body size; each root is one
+//    hS value, the hO value is replaced by its rank in the value domain of
+//    the atom that binds it, and the pairs go into a per-task bitmap in
+//    shared memory (or a per-plan bitmap in global memory for very large
+//    domains).  Counting is done on insertion (atomicOr returns the old
+//    word), so there is no separate popcount pass, and shared bitmaps never
+//    touch HBM.  A partial binding whose (root, hO) pair is already present
+//    is dropped, which is the reference's early prune
+//    (CPU_01_nonparallel/SupportCounting.cpp:284-290).
+//
+// The reference's kernels (GPU_03/gpu_kernels.cuh:34-443) run one thread
+// per head triple or per first-atom triple with template-unrolled
+// recursion; this engine replaces them as a whole.
+#include <cuda_runtime.h>
+
+#include <cstdint>
+
+#include "common.hpp"
+
+namespace gr {
+
+constexpr int kWarps = kBlock / 32;
+constexpr int kLeafChunk = 4 * kBlock;
+
+struct BlockState {
+    int task;
+    int k;
+    int curItem[kMaxBody + 1];
+    long long curOff[kMaxBody + 1];
+    int count[kMaxBody + 1];
+    int levelOff[kMaxBody + 1];
+    long long warpSum[kWarps];
+    unsigned long long red[kWarps];
+};
+
+struct Smem {
+    DevPlan plan;
+    BlockState st;
+    int wBeg[kBlock];
+    long long wLen[kBlock];
+    long long wPre[kBlock];
+    int items[kItemInts];
+    uint32_t bitmap[kBitmapWords];
+};
+
+__device__ __forceinline__ int2 row_lookup(const DevIndex& ix, int pred, int dir, int key) {
+    if (key < 0) return make_int2(0, 0);
+    const uint32_t tag = (uint32_t)pred * 2u + (uint32_t)dir;
+    uint32_t i = slot_hash(tag, (uint32_t)key) & ix.hashMask;
+    for (uint32_t probe = 0; probe <= ix.hashMask; ++probe) {
+        const uint4 s = __ldg(reinterpret_cast<const uint4*>(ix.hash) + i);
+        if (s.x == kEmptyTag) break;
+        if (s.x == tag && s.y == (uint32_t)key) return make_int2((int)s.z, (int)s.w);
+        i = (i + 1) & ix.hashMask;
+    }
+    return make_int2(0, 0);
+}
+
+__device__ __forceinline__ bool has_edge(const DevIndex& ix, int pred, int dir, int key, int target) {
+    const int2 r = row_lookup(ix, pred, dir, key);
+    int lo = r.x, hi = r.y;
+    const int* v = ix.val[dir];
+    while (lo < hi) {
+        const int mid = (lo + hi) >> 1;
+        if (__ldg(v + mid) < target) lo = mid + 1; else hi = mid;
+    }
+    return lo < r.y && __ldg(v + lo) == target;
+}
+
+template <class Val>
+__device__ __forceinline__ bool pass_filters(const DevPlan& P, const DevIndex& ix, int lvl, Val val) {
+    const int cb = P.chkBeg[lvl], cn = P.chkN[lvl];
+    for (int c = 0; c < cn; ++c) {
+        const DevCheck& C = P.checks[cb + c];
+        const int s = val(C.s), o = val(C.o);
+        if (!has_edge(ix, C.pred, C.dir, C.dir == 0 ? s : o, C.dir == 0 ? o : s)) return false;
+    }
+    const int ub = P.usedBeg[lvl], un = P.usedN[lvl];
+    for (int u = 0; u < un; ++u) {
+        const DevUsed& U = P.used[ub + u];
+        if (val(U.sA) == val(U.sB) && val(U.oA) == val(U.oB)) return false;
+    }
+    return true;
+}
+
+// Inclusive block scan of one 64-bit value per thread.
+__device__ __forceinline__ long long block_scan(long long x, BlockState& st) {
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+#pragma unroll
+    for (int d = 1; d < 32; d <<= 1) {
+        const long long y = __shfl_up_sync(0xffffffffu, x, d);
+        if (lane >= d) x += y;
+    }
+    if (lane == 31) st.warpSum[warp] = x;
+    __syncthreads();
+    if (warp == 0) {
+        long long w = lane < kWarps ? st.warpSum[lane] : 0;
+#pragma unroll
+        for (int d = 1; d < 32; d <<= 1) {
+            const long long y = __shfl_up_sync(0xffffffffu, w, d);
+            if (lane >= d) w += y;
+        }
+        if (lane < kWarps) st.warpSum[lane] = w;
+    }
+    __syncthreads();
+    return warp ? x + st.warpSum[warp - 1] : x;
+}
+
+__device__ __forceinline__ unsigned long long block_sum(unsigned long long x, BlockState& st) {
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+#pragma unroll
+    for (int d = 16; d; d >>= 1) x += __shfl_down_sync(0xffffffffu, x, d);
+    if (lane == 0) st.red[warp] = x;
+    __syncthreads();
+    unsigned long long t = 0;
+    if (threadIdx.x == 0)
+        for (int w = 0; w < kWarps; ++w) t += st.red[w];
+    return t;  // valid in thread 0
+}
+
+__device__ __forceinline__ void run_task(Smem& sm, const DevIndex& ix, const DevTask& task,
+                                         unsigned long long* results, int* status) {
+    const DevPlan& P = sm.plan;
+    BlockState& S = sm.st;
+    const int tid = threadIdx.x;
+    const int G = task.end - task.beg;
+    const bool pairs = P.mode == kPairs;
+    const bool shared = !(pairs && P.gBitmap);
+    uint32_t* bm = shared ? sm.bitmap : P.gBitmap;
+    const long long rowBase = shared ? 0 : (long long)task.beg - P.gRowBase;
+
+    // clear the task's dedup bits
+    const int nWords = shared ? (int)(pairs ? (((long long)G * P.wo + 31) >> 5) : ((G + 31) >> 5)) : 0;
+    for (int i = tid; i < nWords; i += kBlock) sm.bitmap[i] = 0u;
+    if (tid == 0) {
+        S.k = 0;
+        int off = 0;
+        for (int l = 0; l <= kMaxBody; ++l) {
+            S.curItem[l] = 0;
+            S.curOff[l] = 0;
+            S.count[l] = 0;
+            S.levelOff[l] = off;
+            if (l < P.m || (P.m == 0 && l == 0)) off += P.cap * P.tupleLen[l];
+        }
+    }
+    __syncthreads();
+
+    // ---- level 0: roots ----
+    {
+        const int len0 = P.tupleLen[0];
+        for (int i = tid; i < G; i += kBlock) {
+            const int r = task.beg + i;
+            int tv[kTupleHead + 2];
+            tv[0] = i;
+            tv[1] = 0;
+            int nv = kTupleHead;
+            bool ok = true;
+            if (P.rootKind == kRootRows) {
+                tv[nv++] = __ldg(ix.rowKey[P.rootDir] + r);
+            } else {
+                const int key = __ldg(ix.src[P.rootDir] + r);
+                const int v = __ldg(ix.val[P.rootDir] + r);
+                if (P.rootKeyEqVal && key != v) ok = false;
+                if (P.rootKeyNeVal && key == v) ok = false;
+                if (P.rootValConst < 0 && v != P.consts[-1 - P.rootValConst]) ok = false;
+                if (P.rootAppendKey) tv[nv++] = key;
+                if (P.rootAppendVal) tv[nv++] = v;
+            }
+            if (ok && nv != len0) { ok = false; atomicOr(status, 2); }
+            if (ok) {
+                ok = pass_filters(P, ix, 0, [&](TermRef ref) -> int {
+                    return ref < 0 ? P.consts[-1 - ref] : tv[ref < nv ? ref : 0];
+                });
+            }
+            if (ok) {
+                const int slot = atomicAdd(&S.count[0], 1);
+                if (slot < P.cap) {
+                    int* dst = sm.items + S.levelOff[0] + slot * len0;
+                    for (int q = 0; q < len0; ++q) dst[q] = tv[q];
+                } else {
+                    atomicOr(status, 4);
+                }
+            }
+        }
+    }
+    __syncthreads();
+
+    unsigned long long myNew = 0;
+    if (P.m == 0) {
+        for (int i = tid; i < S.count[0] && i < P.cap; i += kBlock) {
+            const int root = sm.items[S.levelOff[0] + i * P.tupleLen[0]];
+            atomicOr(&sm.bitmap[root >> 5], 1u << (root & 31));
+        }
+    } else {
+        for (;;) {
+            __syncthreads();
+            const int k = S.k;
+            const int w0 = S.curItem[k];
+            const int cnt = min(S.count[k], P.cap);
+            if (w0 >= cnt) {
+                if (k == 0) break;
+                __syncthreads();
+                if (tid == 0) S.k = k - 1;
+                continue;
+            }
+            const int nw = min(kBlock, cnt - w0);
+            const int lenK = P.tupleLen[k];
+            const int* baseK = sm.items + S.levelOff[k];
+            const DevStep& stp = P.steps[k];
+            const bool leaf = (k + 1 == P.m);
+            const bool itemHasRank = pairs && P.hoLevel >= 1 && k >= P.hoLevel;
+
+            // window: the neighbour segment of each item
+            int myBeg = 0;
+            long long myLen = 0;
+            if (tid < nw) {
+                const int* it = baseK + (w0 + tid) * lenK;
+                bool pruned = false;
+                if (!pairs) {
+                    pruned = (sm.bitmap[it[0] >> 5] >> (it[0] & 31)) & 1u;
+                } else if (itemHasRank) {
+                    const long long bit = (rowBase + it[0]) * (long long)P.wo + it[1];
+                    pruned = (bm[bit >> 5] >> (bit & 31)) & 1u;
+                }
+                if (!pruned) {
+                    if (stp.kind == kExpand) {
+                        const int key = stp.keyRef < 0 ? P.consts[-1 - stp.keyRef] : it[stp.keyRef];
+                        const int2 r = row_lookup(ix, stp.pred, stp.dir, key);
+                        myBeg = r.x;
+                        myLen = r.y - r.x;
+                    } else {
+                        myBeg = __ldg(ix.predEdge[0] + stp.pred);
+                        myLen = __ldg(ix.predEdge[0] + stp.pred + 1) - myBeg;
+                    }
+                    if (tid == 0) {
+                        const long long off = S.curOff[k];
+                        myBeg += (int)off;
+                        myLen = myLen > off ? myLen - off : 0;
+                    }
+                }
+            }
+            sm.wBeg[tid] = myBeg;
+            sm.wLen[tid] = myLen;
+            if (tid == 0 && !leaf) S.count[k + 1] = 0;
+            const long long pre = block_scan(myLen, S);
+            sm.wPre[tid] = pre;
+            __syncthreads();
+            const long long total = sm.wPre[nw - 1];
+            const long long take = min(total, (long long)(leaf ? kLeafChunk : P.cap));
+            const int lenN = leaf ? 0 : P.tupleLen[k + 1];
+            int* baseN = leaf ? nullptr : sm.items + S.levelOff[k + 1];
+
+            for (long long j = tid; j < take; j += kBlock) {
+                int lo = 0, hi = nw - 1;
+                while (lo < hi) {
+                    const int mid = (lo + hi) >> 1;
+                    if (sm.wPre[mid] > j) hi = mid; else lo = mid + 1;
+                }
+                const long long start = sm.wPre[lo] - sm.wLen[lo];
+                const int e = sm.wBeg[lo] + (int)(j - start);
+                const int* par = baseK + (w0 + lo) * lenK;
+                const int root = par[0];
+                if (!pairs && ((sm.bitmap[root >> 5] >> (root & 31)) & 1u)) continue;
+                int n0, n1 = 0;
+                if (stp.kind == kExpand) {
+                    n0 = __ldg(ix.val[stp.dir] + e);
+                } else {
+                    n0 = __ldg(ix.src[0] + e);
+                    n1 = __ldg(ix.val[0] + e);
+                    if (stp.sameVar ? (n0 != n1) : (n0 == n1)) continue;
+                }
+                bool ok = true;
+                for (int q = kTupleHead; q < lenK; ++q) {
+                    const int x = par[q];
+                    if (x == n0 || (stp.nNew == 2 && x == n1)) { ok = false; break; }
+                }
+                if (!ok) continue;
+                ok = pass_filters(P, ix, k + 1, [&](TermRef ref) -> int {
+                    if (ref < 0) return P.consts[-1 - ref];
+                    if (ref < lenK) return par[ref];
+                    return ref == lenK ? n0 : n1;
+                });
+                if (!ok) continue;
+                int rank = par[1];
+                if (pairs && stp.hoWhich) {
+                    if (stp.kind == kExpand) rank = __ldg(ix.valRank[stp.dir] + e);
+                    else rank = stp.hoWhich == 1 ? __ldg(ix.srcRank[0] + e) : __ldg(ix.valRank[0] + e);
+                    if (!leaf) {
+                        const long long bit = (rowBase + root) * (long long)P.wo + rank;
+                        if ((bm[bit >> 5] >> (bit & 31)) & 1u) continue;
+                    }
+                }
+                if (leaf) {
+                    if (!pairs) {
+                        atomicOr(&sm.bitmap[root >> 5], 1u << (root & 31));
+                    } else {
+                        const long long bit = (rowBase + root) * (long long)P.wo + rank;
+                        const uint32_t mask = 1u << (bit & 31);
+                        const uint32_t old = atomicOr(&bm[bit >> 5], mask);
+                        myNew += (old & mask) ? 0ull : 1ull;
+                    }
+                } else {
+                    const int slot = atomicAdd(&S.count[k + 1], 1);
+                    if (slot >= P.cap) { atomicOr(status, 8); continue; }
+                    int* dst = baseN + slot * lenN;
+                    dst[0] = root;
+                    dst[1] = rank;
+                    for (int q = kTupleHead; q < lenK; ++q) dst[q] = par[q];
+                    dst[lenK] = n0;
+                    if (stp.nNew == 2) dst[lenK + 1] = n1;
+                }
+            }
+            __syncthreads();
+            if (tid == 0) {
+                if (take >= total) {
+                    S.curItem[k] = w0 + nw;
+                    S.curOff[k] = 0;
+                } else {
+                    int lo = 0, hi = nw - 1;
+                    while (lo < hi) {
+                        const int mid = (lo + hi) >> 1;
+                        if (sm.wPre[mid] > take) hi = mid; else lo = mid + 1;
+                    }
+                    long long off = take - (sm.wPre[lo] - sm.wLen[lo]);
+                    if (lo == 0) off += S.curOff[k];
+                    S.curItem[k] = w0 + lo;
+                    S.curOff[k] = off;
+                }
+                if (!leaf && S.count[k + 1] > 0) {
+                    S.k = k + 1;
+                    S.curItem[k + 1] = 0;
+                    S.curOff[k + 1] = 0;
+                }
+            }
+        }
+    }
+    __syncthreads();
+
+    // ---- result ----
+    unsigned long long mine = 0;
+    if (!pairs) {
+        for (int i = tid; i < ((G + 31) >> 5); i += kBlock) mine += __popc(sm.bitmap[i]);
+    } else {
+        mine = myNew;
+    }
+    const unsigned long long tot = block_sum(mine, S);
+    if (tid == 0 && tot) atomicAdd(results + P.resultSlot, tot);
+}
+
+__global__ void __launch_bounds__(kBlock, 2)
+engine_kernel(DevIndex ix, const DevPlan* __restrict__ plans, const DevTask* __restrict__ tasks,
+              int nTasks, int* taskCounter, unsigned long long* results, int* status) {
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    Smem& sm = *reinterpret_cast<Smem*>(smem_raw);
+    for (;;) {
+        if (threadIdx.x == 0) sm.st.task = atomicAdd(taskCounter, 1);
+        __syncthreads();
+        const int t = sm.st.task;
+        if (t >= nTasks) return;
+        const DevTask task = tasks[t];
+        const int* src = reinterpret_cast<const int*>(plans + task.plan);
+        int* dst = reinterpret_cast<int*>(&sm.plan);
+        for (int i = threadIdx.x; i < (int)(sizeof(DevPlan) / 4); i += kBlock) dst[i] = src[i];
+        __syncthreads();
+        run_task(sm, ix, task, results, status);
+        __syncthreads();
+    }
+}
+
+size_t engine_smem_bytes() { return sizeof(Smem); }
+
+cudaError_t engine_configure() {
+    return cudaFuncSetAttribute(engine_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sizeof(Smem));
+}
+
+cudaError_t engine_launch(const DevIndex& ix, const DevPlan* plans, const DevTask* tasks, int nTasks,
+                          int* taskCounter, unsigned long long* results, int* status, int grid,
+                          cudaStream_t stream) {
+    if (nTasks <= 0) return cudaSuccess;
+    engine_kernel<<<grid, kBlock, sizeof(Smem), stream>>>(ix, plans, tasks, nTasks, taskCounter, results, status);
+    return cudaGetLastError();
+}
+
+}  // namespace gr

@@ -1,0 +1,374 @@
+// planner.cpp — turns a parsed rule into device plans.
+//
+// Semantics (CPU_01_nonparallel/SupportCounting.cpp):
+//  * support (474-552): head triples that match the head pattern injectively
+//    (9-34) and admit a body grounding; the head triple counts as used.
+//  * body size (563-631): distinct (hS, hO) over body groundings, with the
+//    keys of the smallest body atom containing hS as hS candidates; hS == hO,
+//    or hO absent from the body, counts candidates with a grounding.
+//  * injective bindings: a newly bound variable differs from every bound
+//    variable (SupportCounting.hpp:43-48); constants take no part.
+//  * used triples: no ground triple appears twice in one grounding
+//    (SupportCounting.hpp:50-55).  With injective variables two atoms can
+//    only ground to the same triple if they have the same predicate and no
+//    position holds two different variables.  Atoms that are identical term
+//    for term always collide (the count is 0); atoms that might collide
+//    because a constant meets a variable get a runtime comparison.
+//
+// Plan shape: the bound variables form a tuple [root, hO rank, v0, v1, ...]
+// in binding order.  Atoms are grounded greedily: every atom whose terms are
+// all bound becomes a membership check as soon as possible; otherwise the
+// atom with one bound term and the smallest average fan-out is expanded from
+// that term; otherwise the smallest predicate is scanned.  The order only
+// affects speed: every complete grounding satisfies the same constraints
+// whichever order finds it (the reference's greedy choice in
+// SupportCounting.cpp:38-79 is likewise a speed heuristic).
+#include "planner.hpp"
+
+#include <algorithm>
+#include <cstring>
+#include <limits>
+
+namespace gr {
+namespace {
+
+enum Rel { kEq, kNe, kMaybe };
+
+Rel rel(const Term& a, const Term& b) {
+    if (a.isVar == b.isVar) return a.id == b.id ? kEq : kNe;
+    return kMaybe;
+}
+
+bool has_unknown(const Atom& a) {
+    return a.pred < 0 || (!a.s.isVar && a.s.id < 0) || (!a.o.isVar && a.o.id < 0);
+}
+
+struct Builder {
+    const HostIndex& ix;
+    DevPlan& P;
+    int32_t pos[kMaxVars];
+    int32_t tupleLen = kTupleHead;
+    int32_t nConsts = 0;
+    bool ok = true;
+
+    Builder(const HostIndex& x, DevPlan& p) : ix(x), P(p) {
+        for (int i = 0; i < kMaxVars; ++i) pos[i] = -1;
+    }
+    bool bound(const Term& t) const { return !t.isVar || pos[t.id] >= 0; }
+    void bind(int32_t var) {
+        if (pos[var] < 0) pos[var] = tupleLen++;
+    }
+    TermRef ref(const Term& t) {
+        if (t.isVar) return (TermRef)pos[t.id];
+        for (int k = 0; k < nConsts; ++k)
+            if (P.consts[k] == t.id) return (TermRef)(-1 - k);
+        if (nConsts >= kMaxConsts) { ok = false; return 0; }
+        P.consts[nConsts] = t.id;
+        return (TermRef)(-1 - nConsts++);
+    }
+};
+
+int check_dir(const HostIndex& ix, int32_t p) {
+    return ix.avg_degree(p, 0) <= ix.avg_degree(p, 1) ? 0 : 1;
+}
+
+// Grounding order for `body` given the variables already bound in `b`.
+// `head` (support phase) is the used head triple, or null.  Returns false
+// when two atoms always ground to the same triple.
+bool build_steps(Builder& b, const std::vector<Atom>& body, const Atom* head, int32_t hO, bool pairs) {
+    DevPlan& P = b.P;
+    const HostIndex& ix = b.ix;
+    int nb = (int)body.size();
+    std::vector<int> level(nb, -1);
+    std::vector<int> order;
+    std::vector<std::vector<DevCheck>> checks(kMaxBody + 1);
+    auto add_checks = [&](int lvl) {
+        for (int i = 0; i < nb; ++i) {
+            if (level[i] >= 0 || !b.bound(body[i].s) || !b.bound(body[i].o)) continue;
+            level[i] = lvl;
+            order.push_back(i);
+            DevCheck c{};
+            c.pred = body[i].pred;
+            c.s = b.ref(body[i].s);
+            c.o = b.ref(body[i].o);
+            c.dir = (int8_t)check_dir(ix, body[i].pred);
+            checks[lvl].push_back(c);
+        }
+    };
+    P.tupleLen[0] = b.tupleLen;
+    add_checks(0);
+    int lvl = 0;
+    while ((int)order.size() < nb) {
+        int best = -1, bestDir = 0;
+        double bestFan = std::numeric_limits<double>::infinity();
+        for (int i = 0; i < nb; ++i) {
+            if (level[i] >= 0) continue;
+            bool sB = b.bound(body[i].s), oB = b.bound(body[i].o);
+            if (sB == oB) continue;
+            int d = sB ? 0 : 1;
+            double fan = ix.avg_degree(body[i].pred, d);
+            if (fan < bestFan) { bestFan = fan; best = i; bestDir = d; }
+        }
+        ++lvl;
+        DevStep& st = P.steps[lvl - 1];
+        st = DevStep{};
+        if (best >= 0) {
+            const Atom& a = body[best];
+            st.kind = kExpand;
+            st.pred = a.pred;
+            st.dir = (int8_t)bestDir;
+            st.keyRef = b.ref(bestDir == 0 ? a.s : a.o);
+            const Term& nv = bestDir == 0 ? a.o : a.s;
+            b.bind(nv.id);
+            st.nNew = 1;
+            st.hoWhich = (pairs && nv.id == hO) ? 1 : 0;
+        } else {
+            int64_t bestSize = std::numeric_limits<int64_t>::max();
+            for (int i = 0; i < nb; ++i) {
+                if (level[i] >= 0) continue;
+                int64_t sz = ix.pred_size(body[i].pred);
+                if (sz < bestSize) { bestSize = sz; best = i; }
+            }
+            const Atom& a = body[best];
+            st.kind = kScan;
+            st.pred = a.pred;
+            st.dir = 0;
+            if (a.s.id == a.o.id) {
+                st.sameVar = 1;
+                st.nNew = 1;
+                b.bind(a.s.id);
+                st.hoWhich = (pairs && a.s.id == hO) ? 1 : 0;
+            } else {
+                st.nNew = 2;
+                b.bind(a.s.id);
+                b.bind(a.o.id);
+                st.hoWhich = !pairs ? 0 : (a.s.id == hO ? 1 : (a.o.id == hO ? 2 : 0));
+            }
+        }
+        level[best] = lvl;
+        order.push_back(best);
+        P.tupleLen[lvl] = b.tupleLen;
+        add_checks(lvl);
+    }
+    P.m = lvl;
+
+    // used-triple comparisons, attached where the later atom is grounded
+    std::vector<std::vector<DevUsed>> used(kMaxBody + 1);
+    std::vector<const Atom*> seq;
+    std::vector<int> seqLevel;
+    if (head) { seq.push_back(head); seqLevel.push_back(0); }
+    for (int i : order) { seq.push_back(&body[i]); seqLevel.push_back(level[i]); }
+    for (size_t j = 0; j < seq.size(); ++j) {
+        for (size_t i = 0; i < j; ++i) {
+            const Atom& A = *seq[i];
+            const Atom& B = *seq[j];
+            if (A.pred != B.pred) continue;
+            Rel rs = rel(A.s, B.s), ro = rel(A.o, B.o);
+            if (rs == kNe || ro == kNe) continue;
+            if (rs == kEq && ro == kEq) return false;
+            DevUsed u{b.ref(A.s), b.ref(A.o), b.ref(B.s), b.ref(B.o)};
+            used[seqLevel[j]].push_back(u);
+        }
+    }
+    int nc = 0, nu = 0;
+    for (int l = 0; l <= kMaxBody; ++l) {
+        P.chkBeg[l] = (int8_t)nc;
+        P.chkN[l] = (int8_t)checks[l].size();
+        for (auto& c : checks[l]) {
+            if (nc >= kMaxChecks) { b.ok = false; break; }
+            P.checks[nc++] = c;
+        }
+        P.usedBeg[l] = (int8_t)nu;
+        P.usedN[l] = (int8_t)used[l].size();
+        for (auto& u : used[l]) {
+            if (nu >= kMaxUsed) { b.ok = false; break; }
+            P.used[nu++] = u;
+        }
+    }
+    return true;
+}
+
+void finish_capacity(DevPlan& P) {
+    int sum = 0;
+    if (P.m == 0) sum = P.tupleLen[0];
+    for (int l = 0; l < P.m; ++l) sum += P.tupleLen[l];
+    int cap = (kItemInts / std::max(sum, 1)) & ~31;
+    P.cap = std::max(cap, 32);
+    P.groupMax = P.cap;
+    if (P.mode == kPairs && P.wo > 0) {
+        int64_t g = (int64_t)kBitmapWords * 32 / P.wo;
+        P.groupMax = (int32_t)std::min<int64_t>(P.groupMax, g);
+    }
+}
+
+}  // namespace
+
+RulePlan plan_rule(const Rule& rule, const HostIndex& ix) {
+    RulePlan rp;
+    const Atom& h = rule.head;
+    int nb = (int)rule.body.size();
+    // head measures (SupportCounting.cpp:482-503)
+    if (h.pred >= 0 && h.pred < ix.nPred) {
+        rp.headSize = ix.pred_size(h.pred);
+        bool sC = !h.s.isVar, oC = !h.o.isVar;
+        if (!sC && !oC) rp.headSupport = rp.headSize;
+        else if (sC && !oC) { auto r = ix.row_range(h.pred, 0, h.s.id); rp.headSupport = r.second - r.first; }
+        else if (!sC && oC) { auto r = ix.row_range(h.pred, 1, h.o.id); rp.headSupport = r.second - r.first; }
+        else rp.headSupport = (h.s.id >= 0 && h.o.id >= 0 && ix.has_triple(h.pred, h.s.id, h.o.id)) ? 1 : 0;
+    }
+    if (nb > kMaxBody || rule.nVars > kMaxVars) {
+        rp.status = kRuleUnsupported;
+        rp.headSupport = rp.headSize;   // GPU_03/gpu_rules_lib.cu:345-357
+        return rp;
+    }
+    bool bodyUnknown = false;
+    for (const auto& a : rule.body) bodyUnknown |= has_unknown(a);
+    bool bodyDup = false;   // two identical body atoms: no grounding at all
+    for (int i = 0; i < nb; ++i)
+        for (int j = i + 1; j < nb; ++j)
+            if (rule.body[i].pred == rule.body[j].pred && rel(rule.body[i].s, rule.body[j].s) == kEq &&
+                rel(rule.body[i].o, rule.body[j].o) == kEq)
+                bodyDup = true;
+
+    // ---- support ----
+    PhasePlan& S = rp.support;
+    S.how = kStatic;
+    S.value = 0;
+    if (h.pred >= 0 && rp.headSupport > 0 && !bodyUnknown && !bodyDup) {
+        if (nb == 0) {
+            // every matching head triple counts (bodyExists of an empty body)
+            if (h.s.isVar && h.o.isVar) {
+                int64_t n = 0;
+                for (int32_t e = ix.predEdge[0][h.pred]; e < ix.predEdge[0][h.pred + 1]; ++e) {
+                    bool eq = ix.src[0][e] == ix.val[0][e];
+                    n += (h.s.id == h.o.id) ? eq : !eq;
+                }
+                S.value = n;
+            } else {
+                S.value = rp.headSupport;
+            }
+        } else {
+            DevPlan& P = S.plan;
+            std::memset(&P, 0, sizeof(P));
+            Builder b(ix, P);
+            P.mode = kExist;
+            P.rootKind = kRootEdges;
+            P.rootPred = h.pred;
+            std::pair<int32_t, int32_t> range{ix.predEdge[0][h.pred], ix.predEdge[0][h.pred + 1]};
+            if (h.s.isVar && h.o.isVar) {
+                P.rootDir = 0;
+                P.rootAppendKey = 1;
+                b.bind(h.s.id);
+                if (h.s.id == h.o.id) P.rootKeyEqVal = 1;
+                else { P.rootAppendVal = 1; P.rootKeyNeVal = 1; b.bind(h.o.id); }
+            } else if (!h.s.isVar && h.o.isVar) {
+                P.rootDir = 0;
+                range = ix.row_range(h.pred, 0, h.s.id);
+                P.rootAppendVal = 1;
+                b.bind(h.o.id);
+            } else if (h.s.isVar && !h.o.isVar) {
+                P.rootDir = 1;
+                range = ix.row_range(h.pred, 1, h.o.id);
+                P.rootAppendVal = 1;
+                b.bind(h.s.id);
+            } else {
+                P.rootDir = 0;
+                range = ix.row_range(h.pred, 0, h.s.id);
+                P.rootValConst = b.ref(h.o);
+            }
+            if (build_steps(b, rule.body, &h, -1, false) && b.ok) {
+                finish_capacity(P);
+                S.how = kDevice;
+                S.rootBeg = range.first;
+                S.rootEnd = range.second;
+                S.estCost = (double)(range.second - range.first);
+            } else if (!b.ok) {
+                rp.status = kRuleUnsupported;
+            }
+        }
+    }
+
+    // ---- body size ----
+    PhasePlan& B = rp.body;
+    B.how = kStatic;
+    B.value = 0;
+    if (nb > 0 && h.s.isVar && h.o.isVar && !bodyUnknown && !bodyDup) {
+        int32_t hS = h.s.id, hO = h.o.id;
+        int seedPred = -1, seedDir = 0;
+        int64_t bestSize = std::numeric_limits<int32_t>::max();
+        for (const auto& a : rule.body) {
+            int64_t sz = ix.pred_size(a.pred);
+            if (a.s.isVar && a.s.id == hS && sz < bestSize) { seedPred = a.pred; seedDir = 0; bestSize = sz; }
+            if (a.o.isVar && a.o.id == hS && sz < bestSize) { seedPred = a.pred; seedDir = 1; bestSize = sz; }
+        }
+        bool hoInBody = false;
+        for (const auto& a : rule.body)
+            hoInBody |= (a.s.isVar && a.s.id == hO) || (a.o.isVar && a.o.id == hO);
+        if (seedPred >= 0) {
+            DevPlan& P = B.plan;
+            std::memset(&P, 0, sizeof(P));
+            Builder b(ix, P);
+            bool pairs = hS != hO && hoInBody;
+            P.mode = pairs ? kPairs : kExist;
+            P.rootKind = kRootRows;
+            P.rootDir = seedDir;
+            P.rootPred = seedPred;
+            b.bind(hS);
+            if (build_steps(b, rule.body, nullptr, hO, pairs) && b.ok) {
+                if (pairs) {
+                    for (int l = 0; l < P.m; ++l) {
+                        const DevStep& st = P.steps[l];
+                        if (!st.hoWhich) continue;
+                        P.hoLevel = l + 1;
+                        if (st.kind == kExpand) P.wo = (int32_t)ix.pred_rows(st.pred, 1 - st.dir);
+                        else P.wo = (int32_t)ix.pred_rows(st.pred, st.hoWhich == 1 ? 0 : 1);
+                    }
+                }
+                finish_capacity(P);
+                B.how = kDevice;
+                B.rootBeg = ix.predRow[seedDir][seedPred];
+                B.rootEnd = ix.predRow[seedDir][seedPred + 1];
+                B.needsGlobalBitmap = pairs && (int64_t)P.wo > (int64_t)kBitmapWords * 32;
+                B.estCost = (double)(ix.predEdge[seedDir][seedPred + 1] - ix.predEdge[seedDir][seedPred]);
+            } else if (!b.ok) {
+                rp.status = kRuleUnsupported;
+            }
+        }
+    }
+    if (rp.status != kRuleOk) {
+        rp.support = PhasePlan{};
+        rp.body = PhasePlan{};
+        rp.headSupport = rp.headSize;
+    }
+    return rp;
+}
+
+void make_tasks(const PhasePlan& ph, int32_t planIdx, const HostIndex& ix,
+                std::vector<DevTask>& out, std::vector<double>* cost) {
+    const DevPlan& P = ph.plan;
+    int32_t g = std::max(P.groupMax, 1);
+    if (ph.needsGlobalBitmap) g = std::min(P.cap, 512);
+    const int64_t kMaxRowWork = 1 << 14;
+    int32_t r = ph.rootBeg;
+    while (r < ph.rootEnd) {
+        int32_t e = r;
+        int64_t work = 0;
+        if (P.rootKind == kRootRows) {
+            const auto& rb = ix.rowBeg[P.rootDir];
+            while (e < ph.rootEnd && e - r < g) {
+                int64_t w = 1 + (rb[e + 1] - rb[e]);
+                if (e > r && work + w > kMaxRowWork) break;
+                work += w;
+                ++e;
+            }
+        } else {
+            e = std::min<int32_t>(ph.rootEnd, r + g);
+            work = e - r;
+        }
+        out.push_back(DevTask{planIdx, r, e, 0});
+        if (cost) cost->push_back((double)work);
+        r = e;
+    }
+}
+
+}  // namespace gr
