@@ -1,0 +1,346 @@
+#!/usr/bin/env python
+"""Benchmark: rules/s of the batched persistent engine on one or more B200s.
+
+Workload (one step): all 10,000 rules of the DBpedia-shaped configuration
+(c3: 100,000 entities, 600 Zipf(1.1) predicates, 206,000 triples, chain
+rules of 1-4 body atoms), support and body size of every rule, exact counts.
+The graph and rules are seeded synthetic data with the reference's shapes
+(its datasets are not distributed).
+
+    value   rules/s of the prepared batch: plans and tasks resident on the
+            device, one CUDA-graph launch of the persistent kernel per step,
+            device time between CUDA events on the engine's stream; L2 is
+            flushed (256 MiB write) before every step, outside the timed span
+    e2e     rules/s through gpu_evaluate_rules_batch with host rule strings:
+            parse, plan, pinned host->device copy, kernel, device->host copy
+    per_rule  the plain form, one launch per phase per rule via
+            gpu_evaluate_rule (the reference library's calling pattern)
+
+Multi-GPU (torchrun): each rank evaluates its own 10,000-rule set (rule seed =
+rank) over the same graph; no data-path collective; value = all ranks' rules
+/ max over ranks of the timed device span ("scaling": "weak").
+
+--impl reference: the reference's own CPU implementation of the path
+(CPU_01_nonparallel, compiled in oracle/_ref) with all host threads on
+bounded samples of the same rules; rank 0 only.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import math
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import threading
+import time
+from pathlib import Path
+
+import numpy as np
+
+ROOT = Path(__file__).resolve().parent
+sys.path.insert(0, str(ROOT))
+
+METRIC = "rules/s batched vs per-rule on 1 B200 (exact counts); p99 latency; HBM GB/s"
+WORKLOAD = "c3: DBpedia-shaped, 100k entities, 600 predicates, 206k triples, 10,000 chain rules (1-4 atoms)"
+FLUSH_BYTES = 256 << 20
+CPU_SAMPLE_STRIDE = 20
+
+
+def parse_args():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="engine", choices=["engine", "reference"])
+    ap.add_argument("--config", default="c3")
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-per-rule", action="store_true")
+    ap.add_argument("--data", default=os.environ.get("KG_DATA_DIR", str(Path(tempfile.gettempdir()) / "kg_synth_data")))
+    return ap.parse_args()
+
+
+def dist_env():
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    return rank, world, local
+
+
+def data_for(args, rank: int) -> Path:
+    from masterthesis_gpu_acceleration_b200 import synth
+    d = Path(args.data) / (f"{args.config}" if rank == 0 else f"{args.config}_r{rank}")
+    return synth.generate(args.config, d, seed=0, rule_seed=None if rank == 0 else rank)
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons sampled every 200 ms."""
+
+    QUERY = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+             "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+             "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index: int):
+        self.index = index
+        self.proc = None
+        self.out = tempfile.NamedTemporaryFile("w+", suffix=".csv", delete=False)
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--id={self.index}", f"--query-gpu={self.QUERY}", "--format=csv,noheader,nounits",
+                 "-lms", "200"], stdout=self.out, stderr=subprocess.DEVNULL)
+        except OSError:
+            self.proc = None
+        return self
+
+    def stop(self) -> dict:
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+        self.out.flush()
+        rows = []
+        for line in Path(self.out.name).read_text().splitlines():
+            f = [x.strip() for x in line.split(",")]
+            if len(f) >= 9:
+                rows.append(f)
+        os.unlink(self.out.name)
+        if not rows:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": [], "samples": 0}
+        sm = [float(r[1]) for r in rows if r[1].replace(".", "").isdigit()]
+        smax = [float(r[2]) for r in rows if r[2].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[i] for r in rows for i in range(4) if r[5 + i].lower().startswith("active")})
+        loaded = [x for x in sm if smax and x > 0.5 * max(smax)] or sm
+        return {"sm_mhz": statistics.median(loaded) if loaded else None,
+                "sm_max_mhz": max(smax) if smax else None, "reasons": reasons, "samples": len(rows)}
+
+
+def measured_peaks() -> dict:
+    p = ROOT / "MEASURED_PEAKS.json"
+    if p.exists():
+        d = json.loads(p.read_text())
+        return {"hbm_gbs": d["hbm_gbs"], "source": "measured"}
+    return {"hbm_gbs": 6650.0, "source": "fallback"}
+
+
+def profile_traffic() -> float | None:
+    """DRAM bytes per launch of the engine kernel on this workload, from the
+    committed ncu summary (profiles/engine_kernel_c3.json), if present."""
+    p = ROOT / "profiles" / "engine_kernel_c3.json"
+    if p.exists():
+        return json.loads(p.read_text()).get("dram_bytes_per_launch")
+    return None
+
+
+def cpu_baseline(d: Path, rules: list[str], timeout: float = 300.0) -> dict:
+    """The reference's CPU_01 code, one thread, on every 20th rule."""
+    import oracle
+    sample = rules[::CPU_SAMPLE_STRIDE]
+    desc = f"every {CPU_SAMPLE_STRIDE}th c3 rule ({len(sample)} of {len(rules)}), support + body size, 1 thread"
+    with tempfile.TemporaryDirectory() as t:
+        rf = Path(t) / "rules.txt"
+        rf.write_text("\n".join(sample) + "\n")
+        if oracle.ref_available():
+            _, summ = oracle.run_reference(d / "graph.ttl", rf, threads=1, quiet=True, timeout=timeout)
+            secs = summ["eval_wall_ms"] / 1e3
+            kind = "reference"
+        else:
+            from masterthesis_gpu_acceleration_b200 import synth
+            g = oracle.OracleGraph(synth.read_triples(d), int(synth.read_meta(d)["predicates"]))
+            ir = oracle.split_ir(synth.read_rule_ir(d))[::CPU_SAMPLE_STRIDE]
+            secs = oracle.time_oracle(g, np.concatenate(ir), len(ir))
+            kind = "port"
+    return {"value": len(sample) / secs, "unit": "rules/s", "cores": 1, "kind": kind, "sample": desc,
+            "seconds": secs}
+
+
+def reference_arm(args):
+    rank, world, _ = dist_env()
+    if rank != 0:
+        return
+    import oracle
+    d = data_for(args, 0)
+    from masterthesis_gpu_acceleration_b200 import synth
+    rules = synth.read_rules(d)
+    threads = os.cpu_count() or 1
+    steps, warm = args.steps, args.warmup
+    stride = CPU_SAMPLE_STRIDE * max(1, math.ceil((steps + warm) / 13))
+    base = {"metric": METRIC, "unit": "rules/s", "higher_is_better": True, "impl": "reference",
+            "n_gpus": args.gpus, "steps": steps, "warmup": warm, "dtype": "int32", "data": "synthetic",
+            "scaling": "weak", "vs_baseline": None,
+            "config": {"workload": WORKLOAD, "parallelism": f"{threads} host threads, rules spread over threads",
+                       "global_batch": len(rules[::stride])}}
+    if not oracle.ref_available():
+        kind = "port"
+    else:
+        kind = "reference"
+    total_rules, total_s = 0, 0.0
+    with tempfile.TemporaryDirectory() as t:
+        for step in range(warm + steps):
+            sample = rules[step % stride::stride]
+            rf = Path(t) / f"rules{step}.txt"
+            rf.write_text("\n".join(sample) + "\n")
+            if kind == "reference":
+                _, summ = oracle.run_reference(d / "graph.ttl", rf, threads=threads, quiet=True, timeout=900)
+                secs = summ["eval_wall_ms"] / 1e3
+            else:
+                g = oracle.OracleGraph(synth.read_triples(d), int(synth.read_meta(d)["predicates"]))
+                ir = oracle.split_ir(synth.read_rule_ir(d))[step % stride::stride]
+                secs = oracle.time_oracle(g, np.concatenate(ir), len(ir))
+            if step >= warm:
+                total_rules += len(sample)
+                total_s += secs
+    value = total_rules / total_s
+    desc = (f"per step every {stride}th c3 rule (offset = step), {threads} threads "
+            f"(CPU_01_nonparallel per rule, rules spread over threads)")
+    line = dict(base)
+    line.update({"value": value, "ms_per_step": 1e3 * total_s / steps,
+                 "cpu_baseline": {"value": value, "unit": "rules/s", "cores": threads if kind == "reference" else 1,
+                                  "kind": kind, "sample": desc},
+                 "e2e": {"value": value, "unit": "rules/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}})
+    print(json.dumps(line), flush=True)
+
+
+def engine_arm(args):
+    import torch
+    rank, world, local = dist_env()
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
+    else:
+        torch.cuda.set_device(0)
+    dev = torch.cuda.current_device()
+
+    def barrier():
+        torch.cuda.synchronize()
+        if world > 1:
+            import torch.distributed as dist
+            dist.barrier()
+        torch.cuda.synchronize()
+
+    def allmax(x: float) -> float:
+        if world == 1:
+            return x
+        import torch.distributed as dist
+        t = torch.tensor([x], dtype=torch.float64, device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        return float(t.item())
+
+    import masterthesis_gpu_acceleration_b200 as eng
+    from masterthesis_gpu_acceleration_b200 import synth
+    d = data_for(args, rank)
+    rules = synth.read_rules(d)
+    lib = eng.GpuRulesLib(d / "graph.ttl")
+    batch = lib.prepare_batch(rules)
+    info = batch.info()
+
+    # ---- device-resident batched form ----
+    for _ in range(args.warmup):
+        batch.run(FLUSH_BYTES)
+    barrier()
+    vis = [x for x in os.environ.get("CUDA_VISIBLE_DEVICES", "").split(",") if x.strip()]
+    phys = int(vis[dev]) if dev < len(vis) and vis[dev].strip().isdigit() else dev
+    clocks = ClockSampler(phys).start()
+    total_ms = 0.0
+    results = None
+    for _ in range(args.steps):
+        results, st, ms = batch.run(FLUSH_BYTES)
+        total_ms += ms
+    barrier()
+    clk = clocks.stop()
+    max_ms = allmax(total_ms)
+    value = world * len(rules) * args.steps / (max_ms / 1e3)
+
+    exact = None
+    if rank == 0 and args.config == "c3":
+        gold = ROOT / "tests" / "golden" / "c3_seed0.npz"
+        if gold.exists():
+            exp = np.load(gold)["expected"]
+            got = np.array([[r.support, r.headSize, r.headSupport, r.bodySize] for r in results], dtype=np.int64)
+            exact = bool((got == exp).all())
+
+    # ---- roofline: algorithmic bytes per launch over the average launch ----
+    alg_bytes = batch.count_bytes()
+    avg_s = total_ms / args.steps / 1e3
+    peaks = measured_peaks()
+    achieved = alg_bytes / avg_s / 1e9
+    traffic = profile_traffic()
+
+    # ---- end to end through the C ABI with host strings ----
+    for _ in range(max(1, args.warmup // 2)):
+        lib.evaluate_rules_batch(rules)
+    barrier()
+    t0 = time.perf_counter()
+    for _ in range(args.steps):
+        lib.evaluate_rules_batch(rules)
+    torch.cuda.synchronize()
+    e2e_s = allmax(time.perf_counter() - t0)
+    e2e = {"value": world * len(rules) * args.steps / e2e_s, "unit": "rules/s",
+           "h2d_bytes_per_step": info["h2d_bytes"], "d2h_bytes_per_step": info["d2h_bytes"],
+           "api": "gpu_evaluate_rules_batch (parse + plan + H2D + kernel + D2H), host wall clock"}
+
+    # ---- the plain per-rule form (one launch per phase per rule) ----
+    per_rule = None
+    if not args.no_per_rule:
+        barrier()
+        t0 = time.perf_counter()
+        dev_ms = 0.0
+        for r in rules:
+            res = lib.evaluate_rule(r)
+            dev_ms += res.supportMs + res.confidenceMs
+        wall = allmax(time.perf_counter() - t0)
+        dev_ms = allmax(dev_ms)
+        per_rule = {"rules_per_s_wall": world * len(rules) / wall,
+                    "rules_per_s_device": world * len(rules) / (dev_ms / 1e3),
+                    "batched_speedup_vs_per_rule_wall": value / (world * len(rules) / wall)}
+
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        cpu = cpu_baseline(d, rules)
+
+    batch.close()
+    lib.close()
+    if rank == 0:
+        line = {
+            "metric": METRIC, "value": value, "unit": "rules/s", "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": max_ms / args.steps, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "int32", "data": "synthetic",
+            "config": {"workload": WORKLOAD, "global_batch": world * len(rules), "rules_per_rank": len(rules),
+                       "parallelism": f"rule sets sharded over {world} GPU(s), no collective",
+                       "l2": "flushed before every step (256 MiB write, outside the timed span)",
+                       "exact_vs_reference_golden": exact, "plans": info["plans"], "tasks": info["tasks"]},
+            "e2e": e2e,
+            "per_rule": per_rule,
+            "roofline": {"bound": "hbm", "achieved": achieved, "peak": peaks["hbm_gbs"], "unit": "GB/s",
+                         "frac": achieved / peaks["hbm_gbs"], "traffic": traffic,
+                         "algorithmic_bytes_per_launch": alg_bytes, "peak_source": peaks["source"] + " (burst copy)"},
+            "cpu_baseline": cpu,
+            "clocks": clk,
+            "gpu_launches": args.steps,
+        }
+        print(json.dumps(line), flush=True)
+    if world > 1:
+        import torch.distributed as dist
+        dist.barrier()
+        dist.destroy_process_group()
+
+
+def main():
+    args = parse_args()
+    if args.impl == "reference":
+        reference_arm(args)
+    else:
+        engine_arm(args)
+
+
+if __name__ == "__main__":
+    main()

@@ -74,6 +74,33 @@ int gpu_query_vram(size_t* freeBytesOut, size_t* totalBytesOut);
 int gpu_evaluate_rules_batch(void* ctx, const char* const* rules, int n, int isJson,
                              GpuRuleResult* out, int* status, double* deviceMs);
 
+/* Prepared batches: parse, plan and upload n rules once, then run the
+ * device work any number of times as one CUDA-graph launch (the batched
+ * persistent form with its inputs resident in device memory).  Returns a
+ * batch handle, or NULL on null arguments or a CUDA error; rules that do not
+ * parse are reported by gpu_batch_run's status array.  A batch belongs to
+ * the context it was prepared on and must be freed before it. */
+void* gpu_batch_prepare(void* ctx, const char* const* rules, int n, int isJson);
+
+/* Runs a prepared batch.  flushBytes > 0 first overwrites a scratch buffer
+ * of that size (outside the timed span) so that the run starts with a cold
+ * L2.  out/status (optional, n entries) receive the results; deviceMs
+ * (optional) the device time between two events around the graph launch.
+ * Returns 0, or -1 on a CUDA error. */
+int gpu_batch_run(void* batch, long long flushBytes, GpuRuleResult* out, int* status, double* deviceMs);
+
+/* Device plans, tasks, bytes copied host->device at preparation and bytes
+ * copied device->host per run. */
+int gpu_batch_info(void* batch, long long* plans, long long* tasks, long long* h2dBytes, long long* d2hBytes);
+
+/* Runs the batch once with the byte-counting variant of the kernel and
+ * returns the global-memory bytes the algorithm requested (the roofline's
+ * algorithmic bytes).  Not timed. */
+int gpu_batch_count_bytes(void* batch, unsigned long long* bytes);
+
+/* Frees a prepared batch (NULL is ignored). */
+void gpu_batch_free(void* batch);
+
 /* Number of entities, predicates and distinct triples of a loaded graph. */
 int gpu_graph_stats(void* ctx, long long* entities, long long* predicates, long long* triples);
 

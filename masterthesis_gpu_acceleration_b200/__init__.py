@@ -28,6 +28,11 @@ API_SYMBOLS = (
     "gpu_free_graph",
     "gpu_query_vram",
     "gpu_evaluate_rules_batch",
+    "gpu_batch_prepare",
+    "gpu_batch_run",
+    "gpu_batch_info",
+    "gpu_batch_count_bytes",
+    "gpu_batch_free",
     "gpu_graph_stats",
     "gpu_last_error",
 )
@@ -82,6 +87,17 @@ def load_library(path: os.PathLike | str | None = None) -> ctypes.CDLL:
     lib.gpu_evaluate_rules_batch.argtypes = [
         ctypes.c_void_p, ctypes.POINTER(ctypes.c_char_p), ctypes.c_int, ctypes.c_int,
         ctypes.POINTER(GpuRuleResult), ctypes.POINTER(ctypes.c_int), ctypes.POINTER(ctypes.c_double)]
+    lib.gpu_batch_prepare.restype = ctypes.c_void_p
+    lib.gpu_batch_prepare.argtypes = [ctypes.c_void_p, ctypes.POINTER(ctypes.c_char_p), ctypes.c_int, ctypes.c_int]
+    lib.gpu_batch_run.restype = ctypes.c_int
+    lib.gpu_batch_run.argtypes = [ctypes.c_void_p, ctypes.c_longlong, ctypes.POINTER(GpuRuleResult),
+                                  ctypes.POINTER(ctypes.c_int), ctypes.POINTER(ctypes.c_double)]
+    lib.gpu_batch_info.restype = ctypes.c_int
+    lib.gpu_batch_info.argtypes = [ctypes.c_void_p] + [ctypes.POINTER(ctypes.c_longlong)] * 4
+    lib.gpu_batch_count_bytes.restype = ctypes.c_int
+    lib.gpu_batch_count_bytes.argtypes = [ctypes.c_void_p, ctypes.POINTER(ctypes.c_ulonglong)]
+    lib.gpu_batch_free.restype = None
+    lib.gpu_batch_free.argtypes = [ctypes.c_void_p]
     lib.gpu_graph_stats.restype = ctypes.c_int
     lib.gpu_graph_stats.argtypes = [ctypes.c_void_p] + [ctypes.POINTER(ctypes.c_longlong)] * 3
     lib.gpu_last_error.restype = ctypes.c_char_p
@@ -142,6 +158,9 @@ class GpuRulesLib:
                                f"({self._lib.gpu_last_error().decode(errors='replace')})")
         return list(out)[:n], list(st)[:n], ms.value
 
+    def prepare_batch(self, rules: Sequence[str], is_json: bool = False) -> "PreparedBatch":
+        return PreparedBatch(self, rules, is_json)
+
     def stats(self) -> dict:
         e, p, t = ctypes.c_longlong(), ctypes.c_longlong(), ctypes.c_longlong()
         self._lib.gpu_graph_stats(self._handle(), ctypes.byref(e), ctypes.byref(p), ctypes.byref(t))
@@ -156,6 +175,62 @@ class GpuRulesLib:
         if self._ctx is None:
             raise RuntimeError("graph already freed")
         return self._ctx
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+class PreparedBatch:
+    """Rules parsed, planned and uploaded once; each run() is one CUDA-graph
+    launch of the persistent kernel over all of them."""
+
+    def __init__(self, lib: GpuRulesLib, rules: Sequence[str], is_json: bool = False):
+        self._owner = lib
+        self._lib = lib._lib
+        self.n = len(rules)
+        arr = (ctypes.c_char_p * max(self.n, 1))(*[r.encode() for r in rules])
+        h = self._lib.gpu_batch_prepare(lib._handle(), arr, self.n, int(is_json))
+        if not h:
+            raise RuntimeError(f"gpu_batch_prepare failed ({self._lib.gpu_last_error().decode(errors='replace')})")
+        self._h = ctypes.c_void_p(h)
+        self._out = (GpuRuleResult * max(self.n, 1))()
+        self._st = (ctypes.c_int * max(self.n, 1))()
+
+    def run(self, flush_bytes: int = 0, fetch: bool = True):
+        """Returns (results or None, statuses or None, device_ms)."""
+        ms = ctypes.c_double()
+        out = self._out if fetch else None
+        st = self._st if fetch else None
+        if self._lib.gpu_batch_run(self._h, flush_bytes, out, st, ctypes.byref(ms)) != 0:
+            raise RuntimeError(f"gpu_batch_run failed ({self._lib.gpu_last_error().decode(errors='replace')})")
+        if not fetch:
+            return None, None, ms.value
+        return list(self._out)[:self.n], list(self._st)[:self.n], ms.value
+
+    def info(self) -> dict:
+        v = [ctypes.c_longlong() for _ in range(4)]
+        self._lib.gpu_batch_info(self._h, *[ctypes.byref(x) for x in v])
+        return dict(zip(("plans", "tasks", "h2d_bytes", "d2h_bytes"), (x.value for x in v)))
+
+    def count_bytes(self) -> int:
+        b = ctypes.c_ulonglong()
+        if self._lib.gpu_batch_count_bytes(self._h, ctypes.byref(b)) != 0:
+            raise RuntimeError("gpu_batch_count_bytes failed")
+        return b.value
+
+    def close(self):
+        if getattr(self, "_h", None) is not None:
+            self._lib.gpu_batch_free(self._h)
+            self._h = None
 
     def __enter__(self):
         return self

@@ -1,4 +1,5 @@
-// context.cu — graph context and the C ABI (include/gpu_rules_api.h).
+// context.cu — graph context, staged launches and the C ABI
+// (include/gpu_rules_api.h).
 //
 // Replaces the reference's GpuContext and entry points
 // (GPU_03/gpu_rules_lib.cu:181-574).  Differences that matter to callers:
@@ -32,7 +33,7 @@ size_t engine_smem_bytes();
 cudaError_t engine_configure();
 cudaError_t engine_launch(const DevIndex& ix, const DevPlan* plans, const DevTask* tasks, int nTasks,
                           int* taskCounter, unsigned long long* results, int* status, int grid,
-                          cudaStream_t stream);
+                          cudaStream_t stream, unsigned long long* bytesOut);
 
 namespace {
 
@@ -56,9 +57,7 @@ struct DevBuf {
     size_t cap = 0;
     void ensure(size_t bytes) {
         if (bytes <= cap) return;
-        if (p) cudaFree(p);
-        p = nullptr;
-        cap = 0;
+        release();
         size_t want = std::max<size_t>(bytes, 4096);
         ck(cudaMalloc(&p, want), "cudaMalloc");
         cap = want;
@@ -68,28 +67,76 @@ struct DevBuf {
         p = nullptr;
         cap = 0;
     }
+    ~DevBuf() { release(); }
 };
 
+struct HostBuf {  // pinned
+    void* p = nullptr;
+    size_t cap = 0;
+    void ensure(size_t bytes) {
+        if (bytes <= cap) return;
+        release();
+        size_t want = std::max<size_t>(bytes, 4096);
+        ck(cudaMallocHost(&p, want), "cudaMallocHost");
+        cap = want;
+    }
+    void release() {
+        if (p) cudaFreeHost(p);
+        p = nullptr;
+        cap = 0;
+    }
+    ~HostBuf() { release(); }
+};
+
+int64_t clamp_int(int64_t v) { return std::min<int64_t>(v, INT_MAX); }
+
 }  // namespace
+
+struct Context;
+
+// A set of plans and their tasks resident on the device, with the buffers
+// one launch over them needs.
+struct Staged {
+    DevBuf dBlob, dResults, dCtl, dBitmap, dBytes;
+    HostBuf hBlob, hResults, hCtl;
+    const DevPlan* dPlans = nullptr;
+    const DevTask* dTasks = nullptr;
+    int nPlans = 0, nTasks = 0;
+    size_t bitmapWords = 0;
+    size_t h2dBytes = 0, d2hBytes = 0;
+
+    void stage(Context& c, std::vector<DevPlan>& plans, const std::vector<const PhasePlan*>& phases,
+               bool sortTasks, cudaStream_t s);
+    void enqueue(Context& c, cudaStream_t s, bool countBytes);
+    void download(cudaStream_t s) {
+        if (!nPlans) return;
+        ck(cudaMemcpyAsync(hResults.p, dResults.p, nPlans * sizeof(unsigned long long), cudaMemcpyDeviceToHost, s), "D2H results");
+        ck(cudaMemcpyAsync(hCtl.p, dCtl.p, 8, cudaMemcpyDeviceToHost, s), "D2H status");
+    }
+    const unsigned long long* counts() const { return static_cast<const unsigned long long*>(hResults.p); }
+    void check_status() const {
+        if (nPlans && static_cast<const int*>(hCtl.p)[1] != 0)
+            throw CudaError("engine reported internal status " + std::to_string(static_cast<const int*>(hCtl.p)[1]));
+    }
+};
 
 struct Context {
     int device = 0;
     TermDict ents, preds;
     std::unordered_map<std::string, std::string> prefixes;
     HostIndex hix;
-    void* indexMem = nullptr;
+    DevBuf indexMem;
     DevIndex dix{};
     cudaStream_t stream = nullptr;
     cudaEvent_t ev[4] = {};
-    DevBuf plans, tasks, results, ctl, gbitmap;
+    Staged one;          // per-rule launches
     int grid = 0;
+    int sms = 0;
     std::unique_ptr<RuleParser> parser;
 
     ~Context() {
         cudaSetDevice(device);
         if (stream) cudaStreamSynchronize(stream);
-        plans.release(); tasks.release(); results.release(); ctl.release(); gbitmap.release();
-        if (indexMem) cudaFree(indexMem);
         for (auto& e : ev) if (e) cudaEventDestroy(e);
         if (stream) cudaStreamDestroy(stream);
     }
@@ -120,8 +167,8 @@ struct Context {
         if (total + (64u << 20) > freeB)
             throw CudaError("not enough device memory: need ~" + std::to_string((total >> 20) + 64) +
                             " MB, " + std::to_string(freeB >> 20) + " MB free");
-        ck(cudaMalloc(&indexMem, std::max<size_t>(total, 256)), "cudaMalloc(index)");
-        char* base = static_cast<char*>(indexMem);
+        indexMem.ensure(std::max<size_t>(total, 256));
+        char* base = static_cast<char*>(indexMem.p);
         for (size_t i = 0; i < parts.size(); ++i)
             if (parts[i].second)
                 ck(cudaMemcpy(base + off[i], parts[i].first, parts[i].second, cudaMemcpyHostToDevice), "cudaMemcpy(index)");
@@ -145,27 +192,110 @@ struct Context {
 
     void init_device() {
         ck(cudaGetDevice(&device), "cudaGetDevice");
-        int sms = 0;
         ck(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device), "cudaDeviceGetAttribute");
         ck(engine_configure(), "cudaFuncSetAttribute");
         grid = sms * 2;
         ck(cudaStreamCreateWithFlags(&stream, cudaStreamNonBlocking), "cudaStreamCreate");
         for (auto& e : ev) ck(cudaEventCreate(&e), "cudaEventCreate");
-        ctl.ensure(256);
     }
+};
 
-    int* counter() { return static_cast<int*>(ctl.p); }
-    int* status() { return static_cast<int*>(ctl.p) + 1; }
+void Staged::stage(Context& c, std::vector<DevPlan>& plans, const std::vector<const PhasePlan*>& phases,
+                   bool sortTasks, cudaStream_t s) {
+    nPlans = (int)plans.size();
+    nTasks = 0;
+    bitmapWords = 0;
+    h2dBytes = d2hBytes = 0;
+    if (!nPlans) return;
+    std::vector<size_t> gOff(nPlans, 0);
+    for (int i = 0; i < nPlans; ++i) {
+        if (!phases[i]->needsGlobalBitmap) continue;
+        size_t rows = (size_t)(phases[i]->rootEnd - phases[i]->rootBeg);
+        gOff[i] = bitmapWords;
+        bitmapWords += (rows * (size_t)plans[i].wo + 31) / 32;
+    }
+    if (bitmapWords) dBitmap.ensure(bitmapWords * 4);
+    std::vector<DevTask> tasks;
+    std::vector<double> cost;
+    for (int i = 0; i < nPlans; ++i) {
+        plans[i].resultSlot = i;
+        plans[i].gBitmap = phases[i]->needsGlobalBitmap ? static_cast<uint32_t*>(dBitmap.p) + gOff[i] : nullptr;
+        plans[i].gRowBase = phases[i]->needsGlobalBitmap ? phases[i]->rootBeg : 0;
+        make_tasks(*phases[i], i, c.hix, tasks, &cost);
+    }
+    if (sortTasks && tasks.size() > 1) {
+        // longest tasks first, so the tail of the persistent launch is short
+        std::vector<size_t> ord(tasks.size());
+        std::iota(ord.begin(), ord.end(), 0);
+        std::stable_sort(ord.begin(), ord.end(), [&](size_t a, size_t b) { return cost[a] > cost[b]; });
+        std::vector<DevTask> t2(tasks.size());
+        for (size_t i = 0; i < ord.size(); ++i) t2[i] = tasks[ord[i]];
+        tasks.swap(t2);
+    }
+    nTasks = (int)tasks.size();
+    size_t planBytes = (size_t)nPlans * sizeof(DevPlan);
+    size_t taskBytes = (size_t)nTasks * sizeof(DevTask);
+    size_t blob = planBytes + taskBytes;
+    hBlob.ensure(blob);
+    std::memcpy(hBlob.p, plans.data(), planBytes);
+    std::memcpy(static_cast<char*>(hBlob.p) + planBytes, tasks.data(), taskBytes);
+    dBlob.ensure(blob);
+    dResults.ensure((size_t)nPlans * sizeof(unsigned long long));
+    dCtl.ensure(64);
+    hResults.ensure((size_t)nPlans * sizeof(unsigned long long));
+    hCtl.ensure(64);
+    ck(cudaMemcpyAsync(dBlob.p, hBlob.p, blob, cudaMemcpyHostToDevice, s), "H2D plans");
+    dPlans = static_cast<const DevPlan*>(dBlob.p);
+    dTasks = reinterpret_cast<const DevTask*>(static_cast<const char*>(dBlob.p) + planBytes);
+    h2dBytes = blob;
+    d2hBytes = (size_t)nPlans * sizeof(unsigned long long) + 8;
+}
+
+void Staged::enqueue(Context& c, cudaStream_t s, bool countBytes) {
+    if (!nPlans) return;
+    ck(cudaMemsetAsync(dResults.p, 0, (size_t)nPlans * sizeof(unsigned long long), s), "memset results");
+    ck(cudaMemsetAsync(dCtl.p, 0, 8, s), "memset ctl");
+    if (bitmapWords) ck(cudaMemsetAsync(dBitmap.p, 0, bitmapWords * 4, s), "memset bitmap");
+    unsigned long long* bytes = nullptr;
+    if (countBytes) {
+        dBytes.ensure(8);
+        ck(cudaMemsetAsync(dBytes.p, 0, 8, s), "memset bytes");
+        bytes = static_cast<unsigned long long*>(dBytes.p);
+    }
+    int grid = std::max(1, std::min(nTasks, c.grid));
+    ck(engine_launch(c.dix, dPlans, dTasks, nTasks, static_cast<int*>(dCtl.p),
+                     static_cast<unsigned long long*>(dResults.p), static_cast<int*>(dCtl.p) + 1, grid, s, bytes),
+       "engine launch");
+}
+
+// A batch prepared once and replayed: parse, plan and upload happen at
+// preparation; a run is one CUDA-graph launch of the device work.
+struct Batch {
+    Context* c = nullptr;
+    int n = 0;
+    std::vector<RulePlan> rps;
+    std::vector<int> parseStatus;
+    std::vector<int> owner;  // plan -> rule * 2 + phase
+    Staged st;
+    cudaStream_t stream = nullptr;
+    cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+    cudaGraph_t graph = nullptr;
+    cudaGraphExec_t exec = nullptr;
+    DevBuf flush;
+    double lastMs = 0.0;
+
+    ~Batch() {
+        if (c) cudaSetDevice(c->device);
+        if (stream) cudaStreamSynchronize(stream);
+        if (exec) cudaGraphExecDestroy(exec);
+        if (graph) cudaGraphDestroy(graph);
+        if (ev0) cudaEventDestroy(ev0);
+        if (ev1) cudaEventDestroy(ev1);
+        if (stream) cudaStreamDestroy(stream);
+    }
 };
 
 namespace {
-
-struct PhaseRun {
-    const PhasePlan* ph;
-    DevPlan plan;
-};
-
-int64_t clamp_int(int64_t v) { return std::min<int64_t>(v, INT_MAX); }
 
 void compose(const RulePlan& rp, int64_t sup, int64_t body, double supMs, double confMs, GpuRuleResult* out) {
     *out = GpuRuleResult{};
@@ -182,86 +312,99 @@ void compose(const RulePlan& rp, int64_t sup, int64_t body, double supMs, double
     out->confidenceMs = confMs;
 }
 
-// Runs the given phases (one plan each) in one launch; results[i] receives
-// plan i's count.  Global bitmaps are carved from the context's arena.
-void run_phases(Context& c, std::vector<DevPlan>& plans, const std::vector<const PhasePlan*>& phases,
-                std::vector<unsigned long long>& counts, float* ms, bool sortTasks) {
-    size_t n = plans.size();
-    counts.assign(n, 0);
-    if (ms) *ms = 0.f;
-    if (!n) return;
-    // global bitmaps
-    size_t gWords = 0;
-    std::vector<size_t> gOff(n, 0);
-    for (size_t i = 0; i < n; ++i) {
-        if (!phases[i]->needsGlobalBitmap) continue;
-        size_t rows = (size_t)(phases[i]->rootEnd - phases[i]->rootBeg);
-        gOff[i] = gWords;
-        gWords += (rows * (size_t)plans[i].wo + 31) / 32;
-    }
-    if (gWords) {
-        c.gbitmap.ensure(gWords * 4);
-        ck(cudaMemsetAsync(c.gbitmap.p, 0, gWords * 4, c.stream), "cudaMemsetAsync(bitmap)");
-    }
-    std::vector<DevTask> tasks;
-    std::vector<double> cost;
-    for (size_t i = 0; i < n; ++i) {
-        plans[i].resultSlot = (int32_t)i;
-        if (phases[i]->needsGlobalBitmap) {
-            plans[i].gBitmap = static_cast<uint32_t*>(c.gbitmap.p) + gOff[i];
-            plans[i].gRowBase = phases[i]->rootBeg;
-        } else {
-            plans[i].gBitmap = nullptr;
-        }
-        make_tasks(*phases[i], (int32_t)i, c.hix, tasks, &cost);
-    }
-    if (sortTasks && tasks.size() > 1) {
-        std::vector<size_t> ord(tasks.size());
-        std::iota(ord.begin(), ord.end(), 0);
-        std::stable_sort(ord.begin(), ord.end(), [&](size_t a, size_t b) { return cost[a] > cost[b]; });
-        std::vector<DevTask> t2(tasks.size());
-        for (size_t i = 0; i < ord.size(); ++i) t2[i] = tasks[ord[i]];
-        tasks.swap(t2);
-    }
-    c.plans.ensure(n * sizeof(DevPlan));
-    c.tasks.ensure(std::max<size_t>(tasks.size(), 1) * sizeof(DevTask));
-    c.results.ensure(n * sizeof(unsigned long long));
-    ck(cudaMemcpyAsync(c.plans.p, plans.data(), n * sizeof(DevPlan), cudaMemcpyHostToDevice, c.stream), "H2D plans");
-    if (!tasks.empty())
-        ck(cudaMemcpyAsync(c.tasks.p, tasks.data(), tasks.size() * sizeof(DevTask), cudaMemcpyHostToDevice, c.stream), "H2D tasks");
-    ck(cudaMemsetAsync(c.results.p, 0, n * sizeof(unsigned long long), c.stream), "memset results");
-    ck(cudaMemsetAsync(c.ctl.p, 0, 8, c.stream), "memset ctl");
+// One phase in its own launch (the plain per-rule form), timed by events.
+int64_t run_one_phase(Context& c, const PhasePlan& ph, float* ms) {
+    std::vector<DevPlan> plans{ph.plan};
+    c.one.stage(c, plans, {&ph}, false, c.stream);
     ck(cudaEventRecord(c.ev[0], c.stream), "event");
-    int grid = std::min<int>((int)tasks.size(), c.grid);
-    ck(engine_launch(c.dix, static_cast<const DevPlan*>(c.plans.p), static_cast<const DevTask*>(c.tasks.p),
-                     (int)tasks.size(), c.counter(), static_cast<unsigned long long*>(c.results.p), c.status(),
-                     std::max(grid, 1), c.stream), "engine launch");
+    c.one.enqueue(c, c.stream, false);
     ck(cudaEventRecord(c.ev[1], c.stream), "event");
-    int st[2] = {0, 0};
-    ck(cudaMemcpyAsync(counts.data(), c.results.p, n * sizeof(unsigned long long), cudaMemcpyDeviceToHost, c.stream), "D2H results");
-    ck(cudaMemcpyAsync(st, c.ctl.p, 8, cudaMemcpyDeviceToHost, c.stream), "D2H status");
-    ck(cudaStreamSynchronize(c.stream), "kernel");
-    if (ms) ck(cudaEventElapsedTime(ms, c.ev[0], c.ev[1]), "elapsed");
-    if (st[1] != 0) throw CudaError("engine reported internal status " + std::to_string(st[1]));
+    c.one.download(c.stream);
+    ck(cudaStreamSynchronize(c.stream), "engine");
+    c.one.check_status();
+    ck(cudaEventElapsedTime(ms, c.ev[0], c.ev[1]), "elapsed");
+    return (int64_t)c.one.counts()[0];
 }
 
 int evaluate_parsed(Context& c, const Rule& rule, GpuRuleResult* out) {
     RulePlan rp = plan_rule(rule, c.hix);
     int64_t sup = rp.support.value, body = rp.body.value;
     float supMs = 0.f, confMs = 0.f;
-    std::vector<unsigned long long> counts;
-    if (rp.status == kRuleOk && rp.support.how == kDevice) {
-        std::vector<DevPlan> plans{rp.support.plan};
-        run_phases(c, plans, {&rp.support}, counts, &supMs, false);
-        sup = (int64_t)counts[0];
-    }
-    if (rp.status == kRuleOk && rp.body.how == kDevice) {
-        std::vector<DevPlan> plans{rp.body.plan};
-        run_phases(c, plans, {&rp.body}, counts, &confMs, false);
-        body = (int64_t)counts[0];
-    }
+    if (rp.status == kRuleOk && rp.support.how == kDevice) sup = run_one_phase(c, rp.support, &supMs);
+    if (rp.status == kRuleOk && rp.body.how == kDevice) body = run_one_phase(c, rp.body, &confMs);
     compose(rp, sup, body, supMs, confMs, out);
     return 0;
+}
+
+// Parses and plans n rules and stages their device phases.
+void prepare(Batch& b, Context& c, const char* const* rules, int n, int isJson) {
+    b.c = &c;
+    b.n = n;
+    b.rps.assign(n, RulePlan{});
+    b.parseStatus.assign(n, 0);
+    std::vector<DevPlan> plans;
+    std::vector<const PhasePlan*> phases;
+    plans.reserve(2 * (size_t)n);
+    for (int i = 0; i < n; ++i) {
+        if (!rules[i]) { b.parseStatus[i] = -1; continue; }
+        try {
+            Rule r = isJson ? c.parser->parse_json(rules[i]) : c.parser->parse_text(rules[i]);
+            b.rps[i] = plan_rule(r, c.hix);
+        } catch (const RuleError&) {
+            b.parseStatus[i] = -1;
+            continue;
+        }
+        RulePlan& rp = b.rps[i];
+        if (rp.status != kRuleOk) continue;
+        if (rp.support.how == kDevice) { plans.push_back(rp.support.plan); phases.push_back(&rp.support); b.owner.push_back(2 * i); }
+        if (rp.body.how == kDevice) { plans.push_back(rp.body.plan); phases.push_back(&rp.body); b.owner.push_back(2 * i + 1); }
+    }
+    if (!b.stream) ck(cudaStreamCreateWithFlags(&b.stream, cudaStreamNonBlocking), "cudaStreamCreate");
+    if (!b.ev0) ck(cudaEventCreate(&b.ev0), "cudaEventCreate");
+    if (!b.ev1) ck(cudaEventCreate(&b.ev1), "cudaEventCreate");
+    b.st.stage(c, plans, phases, true, b.stream);
+}
+
+void collect(const Batch& b, GpuRuleResult* out, int* status) {
+    std::vector<int64_t> sup(b.n), body(b.n);
+    for (int i = 0; i < b.n; ++i) { sup[i] = b.rps[i].support.value; body[i] = b.rps[i].body.value; }
+    const unsigned long long* cnt = b.st.counts();
+    for (size_t k = 0; k < b.owner.size(); ++k) {
+        int i = b.owner[k] / 2;
+        if (b.owner[k] % 2 == 0) sup[i] = (int64_t)cnt[k];
+        else body[i] = (int64_t)cnt[k];
+    }
+    for (int i = 0; i < b.n; ++i) {
+        if (status) status[i] = b.parseStatus[i];
+        if (b.parseStatus[i] != 0) { out[i] = GpuRuleResult{}; continue; }
+        compose(b.rps[i], sup[i], body[i], 0.0, 0.0, &out[i]);
+    }
+}
+
+// Runs a prepared batch: optional L2 flush (untimed), then the device work
+// between two events, then the result download.
+void run_batch(Batch& b, bool useGraph, size_t flushBytes) {
+    Context& c = *b.c;
+    if (flushBytes) {
+        b.flush.ensure(flushBytes);
+        ck(cudaMemsetAsync(b.flush.p, (int)(b.lastMs * 7) & 0xff, flushBytes, b.stream), "flush");
+    }
+    if (useGraph && !b.exec && b.st.nPlans) {
+        ck(cudaStreamBeginCapture(b.stream, cudaStreamCaptureModeThreadLocal), "capture");
+        b.st.enqueue(c, b.stream, false);
+        ck(cudaStreamEndCapture(b.stream, &b.graph), "capture end");
+        ck(cudaGraphInstantiate(&b.exec, b.graph, 0), "graph instantiate");
+    }
+    ck(cudaEventRecord(b.ev0, b.stream), "event");
+    if (useGraph && b.exec) ck(cudaGraphLaunch(b.exec, b.stream), "graph launch");
+    else b.st.enqueue(c, b.stream, false);
+    ck(cudaEventRecord(b.ev1, b.stream), "event");
+    b.st.download(b.stream);
+    ck(cudaStreamSynchronize(b.stream), "engine");
+    b.st.check_status();
+    float ms = 0.f;
+    ck(cudaEventElapsedTime(&ms, b.ev0, b.ev1), "elapsed");
+    b.lastMs = ms;
 }
 
 Context* as_ctx(void* p) { return static_cast<Context*>(p); }
@@ -349,60 +492,84 @@ int gpu_evaluate_rule_json(void* ctx, const char* ruleJson, GpuRuleResult* out) 
 
 int gpu_evaluate_rules_batch(void* ctx, const char* const* rules, int n, int isJson,
                              GpuRuleResult* out, int* status, double* deviceMs) {
-    if (!ctx || (!rules && n > 0) || (!out && n > 0) || n < 0) return -1;
+    if (!ctx || n < 0 || (n > 0 && (!rules || !out))) return -1;
     Context& c = *as_ctx(ctx);
     if (deviceMs) *deviceMs = 0.0;
     try {
         cudaSetDevice(c.device);
-        std::vector<RulePlan> rps(n);
-        std::vector<DevPlan> plans;
-        std::vector<const PhasePlan*> phases;
-        std::vector<int> owner;  // plan -> rule*2 + phase
-        plans.reserve(2 * (size_t)n);
-        for (int i = 0; i < n; ++i) {
-            out[i] = GpuRuleResult{};
-            if (status) status[i] = 0;
-            if (!rules[i]) { if (status) status[i] = -1; rps[i].status = -1; continue; }
-            try {
-                Rule r = isJson ? c.parser->parse_json(rules[i]) : c.parser->parse_text(rules[i]);
-                rps[i] = plan_rule(r, c.hix);
-            } catch (const RuleError& e) {
-                if (status) status[i] = -1;
-                rps[i].status = -1;
-                continue;
-            }
-            if (rps[i].status != kRuleOk) continue;
-            if (rps[i].support.how == kDevice) {
-                plans.push_back(rps[i].support.plan);
-                phases.push_back(&rps[i].support);
-                owner.push_back(2 * i);
-            }
-            if (rps[i].body.how == kDevice) {
-                plans.push_back(rps[i].body.plan);
-                phases.push_back(&rps[i].body);
-                owner.push_back(2 * i + 1);
-            }
-        }
-        std::vector<unsigned long long> counts;
-        float ms = 0.f;
-        run_phases(c, plans, phases, counts, &ms, true);
-        std::vector<int64_t> sup(n), body(n);
-        for (int i = 0; i < n; ++i) { sup[i] = rps[i].support.value; body[i] = rps[i].body.value; }
-        for (size_t k = 0; k < owner.size(); ++k) {
-            int i = owner[k] / 2;
-            if (owner[k] % 2 == 0) sup[i] = (int64_t)counts[k];
-            else body[i] = (int64_t)counts[k];
-        }
-        for (int i = 0; i < n; ++i) {
-            if (rps[i].status == -1) continue;
-            compose(rps[i], sup[i], body[i], 0.0, 0.0, &out[i]);
-        }
-        if (deviceMs) *deviceMs = ms;
+        Batch b;
+        prepare(b, c, rules, n, isJson);
+        run_batch(b, false, 0);
+        collect(b, out, status);
+        if (deviceMs) *deviceMs = b.lastMs;
         return 0;
     } catch (const std::exception& e) {
         set_error(std::string("gpu_evaluate_rules_batch error: ") + e.what());
         return -1;
     }
+}
+
+void* gpu_batch_prepare(void* ctx, const char* const* rules, int n, int isJson) {
+    if (!ctx || n < 0 || (n > 0 && !rules)) return nullptr;
+    Context& c = *as_ctx(ctx);
+    Batch* b = nullptr;
+    try {
+        cudaSetDevice(c.device);
+        b = new Batch();
+        prepare(*b, c, rules, n, isJson);
+        ck(cudaStreamSynchronize(b->stream), "stage");
+        return b;
+    } catch (const std::exception& e) {
+        set_error(std::string("gpu_batch_prepare error: ") + e.what());
+        delete b;
+        return nullptr;
+    }
+}
+
+int gpu_batch_run(void* batch, long long flushBytes, GpuRuleResult* out, int* status, double* deviceMs) {
+    if (!batch) return -1;
+    Batch& b = *static_cast<Batch*>(batch);
+    try {
+        cudaSetDevice(b.c->device);
+        run_batch(b, true, flushBytes > 0 ? (size_t)flushBytes : 0);
+        if (out) collect(b, out, status);
+        if (deviceMs) *deviceMs = b.lastMs;
+        return 0;
+    } catch (const std::exception& e) {
+        set_error(std::string("gpu_batch_run error: ") + e.what());
+        return -1;
+    }
+}
+
+int gpu_batch_info(void* batch, long long* plans, long long* tasks, long long* h2dBytes, long long* d2hBytes) {
+    if (!batch) return -1;
+    Batch& b = *static_cast<Batch*>(batch);
+    if (plans) *plans = b.st.nPlans;
+    if (tasks) *tasks = b.st.nTasks;
+    if (h2dBytes) *h2dBytes = (long long)b.st.h2dBytes;
+    if (d2hBytes) *d2hBytes = (long long)b.st.d2hBytes;
+    return 0;
+}
+
+int gpu_batch_count_bytes(void* batch, unsigned long long* bytes) {
+    if (!batch || !bytes) return -1;
+    Batch& b = *static_cast<Batch*>(batch);
+    try {
+        cudaSetDevice(b.c->device);
+        *bytes = 0;
+        if (!b.st.nPlans) return 0;
+        b.st.enqueue(*b.c, b.stream, true);
+        ck(cudaMemcpyAsync(bytes, b.st.dBytes.p, 8, cudaMemcpyDeviceToHost, b.stream), "D2H bytes");
+        ck(cudaStreamSynchronize(b.stream), "count");
+        return 0;
+    } catch (const std::exception& e) {
+        set_error(std::string("gpu_batch_count_bytes error: ") + e.what());
+        return -1;
+    }
+}
+
+void gpu_batch_free(void* batch) {
+    delete static_cast<Batch*>(batch);
 }
 
 int gpu_graph_stats(void* ctx, long long* entities, long long* predicates, long long* triples) {

@@ -37,6 +37,16 @@
 namespace gr {
 
 constexpr int kWarps = kBlock / 32;
+
+// Counts the global-memory bytes the algorithm requests (the roofline's
+// algorithmic bytes).  Compiled out of the timed kernel.
+template <bool kOn>
+struct Meter {
+    unsigned long long bytes = 0;
+    __device__ __forceinline__ void add(unsigned long long n) {
+        if constexpr (kOn) bytes += n;
+    }
+};
 constexpr int kLeafChunk = 4 * kBlock;
 
 struct BlockState {
@@ -60,12 +70,14 @@ struct Smem {
     uint32_t bitmap[kBitmapWords];
 };
 
-__device__ __forceinline__ int2 row_lookup(const DevIndex& ix, int pred, int dir, int key) {
+template <bool kC>
+__device__ __forceinline__ int2 row_lookup(const DevIndex& ix, int pred, int dir, int key, Meter<kC>& mt) {
     if (key < 0) return make_int2(0, 0);
     const uint32_t tag = (uint32_t)pred * 2u + (uint32_t)dir;
     uint32_t i = slot_hash(tag, (uint32_t)key) & ix.hashMask;
     for (uint32_t probe = 0; probe <= ix.hashMask; ++probe) {
         const uint4 s = __ldg(reinterpret_cast<const uint4*>(ix.hash) + i);
+        mt.add(16);
         if (s.x == kEmptyTag) break;
         if (s.x == tag && s.y == (uint32_t)key) return make_int2((int)s.z, (int)s.w);
         i = (i + 1) & ix.hashMask;
@@ -73,24 +85,27 @@ __device__ __forceinline__ int2 row_lookup(const DevIndex& ix, int pred, int dir
     return make_int2(0, 0);
 }
 
-__device__ __forceinline__ bool has_edge(const DevIndex& ix, int pred, int dir, int key, int target) {
-    const int2 r = row_lookup(ix, pred, dir, key);
+template <bool kC>
+__device__ __forceinline__ bool has_edge(const DevIndex& ix, int pred, int dir, int key, int target, Meter<kC>& mt) {
+    const int2 r = row_lookup(ix, pred, dir, key, mt);
     int lo = r.x, hi = r.y;
     const int* v = ix.val[dir];
     while (lo < hi) {
         const int mid = (lo + hi) >> 1;
+        mt.add(4);
         if (__ldg(v + mid) < target) lo = mid + 1; else hi = mid;
     }
+    if (lo < r.y) mt.add(4);
     return lo < r.y && __ldg(v + lo) == target;
 }
 
-template <class Val>
-__device__ __forceinline__ bool pass_filters(const DevPlan& P, const DevIndex& ix, int lvl, Val val) {
+template <bool kC, class Val>
+__device__ __forceinline__ bool pass_filters(const DevPlan& P, const DevIndex& ix, int lvl, Meter<kC>& mt, Val val) {
     const int cb = P.chkBeg[lvl], cn = P.chkN[lvl];
     for (int c = 0; c < cn; ++c) {
         const DevCheck& C = P.checks[cb + c];
         const int s = val(C.s), o = val(C.o);
-        if (!has_edge(ix, C.pred, C.dir, C.dir == 0 ? s : o, C.dir == 0 ? o : s)) return false;
+        if (!has_edge(ix, C.pred, C.dir, C.dir == 0 ? s : o, C.dir == 0 ? o : s, mt)) return false;
     }
     const int ub = P.usedBeg[lvl], un = P.usedN[lvl];
     for (int u = 0; u < un; ++u) {
@@ -135,8 +150,9 @@ __device__ __forceinline__ unsigned long long block_sum(unsigned long long x, Bl
     return t;  // valid in thread 0
 }
 
+template <bool kC>
 __device__ __forceinline__ void run_task(Smem& sm, const DevIndex& ix, const DevTask& task,
-                                         unsigned long long* results, int* status) {
+                                         unsigned long long* results, int* status, Meter<kC>& mt) {
     const DevPlan& P = sm.plan;
     BlockState& S = sm.st;
     const int tid = threadIdx.x;
@@ -174,7 +190,9 @@ __device__ __forceinline__ void run_task(Smem& sm, const DevIndex& ix, const Dev
             bool ok = true;
             if (P.rootKind == kRootRows) {
                 tv[nv++] = __ldg(ix.rowKey[P.rootDir] + r);
+                mt.add(4);
             } else {
+                mt.add(8);
                 const int key = __ldg(ix.src[P.rootDir] + r);
                 const int v = __ldg(ix.val[P.rootDir] + r);
                 if (P.rootKeyEqVal && key != v) ok = false;
@@ -185,7 +203,7 @@ __device__ __forceinline__ void run_task(Smem& sm, const DevIndex& ix, const Dev
             }
             if (ok && nv != len0) { ok = false; atomicOr(status, 2); }
             if (ok) {
-                ok = pass_filters(P, ix, 0, [&](TermRef ref) -> int {
+                ok = pass_filters(P, ix, 0, mt, [&](TermRef ref) -> int {
                     return ref < 0 ? P.consts[-1 - ref] : tv[ref < nv ? ref : 0];
                 });
             }
@@ -238,16 +256,18 @@ __device__ __forceinline__ void run_task(Smem& sm, const DevIndex& ix, const Dev
                 } else if (itemHasRank) {
                     const long long bit = (rowBase + it[0]) * (long long)P.wo + it[1];
                     pruned = (bm[bit >> 5] >> (bit & 31)) & 1u;
+                    if (!shared) mt.add(4);
                 }
                 if (!pruned) {
                     if (stp.kind == kExpand) {
                         const int key = stp.keyRef < 0 ? P.consts[-1 - stp.keyRef] : it[stp.keyRef];
-                        const int2 r = row_lookup(ix, stp.pred, stp.dir, key);
+                        const int2 r = row_lookup(ix, stp.pred, stp.dir, key, mt);
                         myBeg = r.x;
                         myLen = r.y - r.x;
                     } else {
                         myBeg = __ldg(ix.predEdge[0] + stp.pred);
                         myLen = __ldg(ix.predEdge[0] + stp.pred + 1) - myBeg;
+                        mt.add(8);
                     }
                     if (tid == 0) {
                         const long long off = S.curOff[k];
@@ -281,9 +301,11 @@ __device__ __forceinline__ void run_task(Smem& sm, const DevIndex& ix, const Dev
                 int n0, n1 = 0;
                 if (stp.kind == kExpand) {
                     n0 = __ldg(ix.val[stp.dir] + e);
+                    mt.add(4);
                 } else {
                     n0 = __ldg(ix.src[0] + e);
                     n1 = __ldg(ix.val[0] + e);
+                    mt.add(8);
                     if (stp.sameVar ? (n0 != n1) : (n0 == n1)) continue;
                 }
                 bool ok = true;
@@ -292,7 +314,7 @@ __device__ __forceinline__ void run_task(Smem& sm, const DevIndex& ix, const Dev
                     if (x == n0 || (stp.nNew == 2 && x == n1)) { ok = false; break; }
                 }
                 if (!ok) continue;
-                ok = pass_filters(P, ix, k + 1, [&](TermRef ref) -> int {
+                ok = pass_filters(P, ix, k + 1, mt, [&](TermRef ref) -> int {
                     if (ref < 0) return P.consts[-1 - ref];
                     if (ref < lenK) return par[ref];
                     return ref == lenK ? n0 : n1;
@@ -302,8 +324,10 @@ __device__ __forceinline__ void run_task(Smem& sm, const DevIndex& ix, const Dev
                 if (pairs && stp.hoWhich) {
                     if (stp.kind == kExpand) rank = __ldg(ix.valRank[stp.dir] + e);
                     else rank = stp.hoWhich == 1 ? __ldg(ix.srcRank[0] + e) : __ldg(ix.valRank[0] + e);
+                    mt.add(4);
                     if (!leaf) {
                         const long long bit = (rowBase + root) * (long long)P.wo + rank;
+                        if (!shared) mt.add(4);
                         if ((bm[bit >> 5] >> (bit & 31)) & 1u) continue;
                     }
                 }
@@ -314,6 +338,7 @@ __device__ __forceinline__ void run_task(Smem& sm, const DevIndex& ix, const Dev
                         const long long bit = (rowBase + root) * (long long)P.wo + rank;
                         const uint32_t mask = 1u << (bit & 31);
                         const uint32_t old = atomicOr(&bm[bit >> 5], mask);
+                        if (!shared) mt.add(8);
                         myNew += (old & mask) ? 0ull : 1ull;
                     }
                 } else {
@@ -362,39 +387,57 @@ __device__ __forceinline__ void run_task(Smem& sm, const DevIndex& ix, const Dev
     }
     const unsigned long long tot = block_sum(mine, S);
     if (tid == 0 && tot) atomicAdd(results + P.resultSlot, tot);
+    if (tid == 0) mt.add(8);
 }
 
+template <bool kC>
 __global__ void __launch_bounds__(kBlock, 2)
 engine_kernel(DevIndex ix, const DevPlan* __restrict__ plans, const DevTask* __restrict__ tasks,
-              int nTasks, int* taskCounter, unsigned long long* results, int* status) {
+              int nTasks, int* taskCounter, unsigned long long* results, int* status,
+              unsigned long long* bytesOut) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     Smem& sm = *reinterpret_cast<Smem*>(smem_raw);
+    Meter<kC> mt;
     for (;;) {
         if (threadIdx.x == 0) sm.st.task = atomicAdd(taskCounter, 1);
         __syncthreads();
         const int t = sm.st.task;
-        if (t >= nTasks) return;
+        if (t >= nTasks) break;
         const DevTask task = tasks[t];
+        if (threadIdx.x == 0) mt.add(sizeof(DevTask) + sizeof(DevPlan) + 8);
         const int* src = reinterpret_cast<const int*>(plans + task.plan);
         int* dst = reinterpret_cast<int*>(&sm.plan);
         for (int i = threadIdx.x; i < (int)(sizeof(DevPlan) / 4); i += kBlock) dst[i] = src[i];
         __syncthreads();
-        run_task(sm, ix, task, results, status);
+        run_task(sm, ix, task, results, status, mt);
         __syncthreads();
+    }
+    if constexpr (kC) {
+        unsigned long long b = mt.bytes;
+        for (int d = 16; d; d >>= 1) b += __shfl_down_sync(0xffffffffu, b, d);
+        if ((threadIdx.x & 31) == 0 && b) atomicAdd(bytesOut, b);
     }
 }
 
 size_t engine_smem_bytes() { return sizeof(Smem); }
 
 cudaError_t engine_configure() {
-    return cudaFuncSetAttribute(engine_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sizeof(Smem));
+    cudaError_t e = cudaFuncSetAttribute(engine_kernel<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sizeof(Smem));
+    if (e != cudaSuccess) return e;
+    return cudaFuncSetAttribute(engine_kernel<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sizeof(Smem));
 }
 
+// bytesOut != null selects the byte-counting variant.
 cudaError_t engine_launch(const DevIndex& ix, const DevPlan* plans, const DevTask* tasks, int nTasks,
                           int* taskCounter, unsigned long long* results, int* status, int grid,
-                          cudaStream_t stream) {
+                          cudaStream_t stream, unsigned long long* bytesOut) {
     if (nTasks <= 0) return cudaSuccess;
-    engine_kernel<<<grid, kBlock, sizeof(Smem), stream>>>(ix, plans, tasks, nTasks, taskCounter, results, status);
+    if (bytesOut)
+        engine_kernel<true><<<grid, kBlock, sizeof(Smem), stream>>>(ix, plans, tasks, nTasks, taskCounter, results,
+                                                                    status, bytesOut);
+    else
+        engine_kernel<false><<<grid, kBlock, sizeof(Smem), stream>>>(ix, plans, tasks, nTasks, taskCounter, results,
+                                                                     status, nullptr);
     return cudaGetLastError();
 }
 

@@ -190,7 +190,8 @@ struct RuleSpec {
 };
 
 static bool write_all(const std::string& dir, const Graph& g, const std::vector<RuleIR>& rules,
-                      const std::vector<std::string>& texts, const std::string& cfg, uint64_t seed) {
+                      const std::vector<std::string>& texts, const std::string& cfg, uint64_t seed,
+                      uint64_t ruleSeed = ~0ull) {
     {
         FILE* f = std::fopen((dir + "/triples.bin").c_str(), "wb");
         if (!f) return false;
@@ -227,6 +228,7 @@ static bool write_all(const std::string& dir, const Graph& g, const std::vector<
         if (!f) return false;
         std::fprintf(f, "config=%s\nseed=%llu\nentities=%d\npredicates=%d\ntriples=%zu\nrules=%zu\n",
                      cfg.c_str(), (unsigned long long)seed, g.N, g.P, g.t.size(), rules.size());
+        if (ruleSeed != ~0ull) std::fprintf(f, "rule_seed=%llu\n", (unsigned long long)ruleSeed);
         std::fclose(f);
     }
     return true;
@@ -257,10 +259,13 @@ static void make_rules(const Graph& g, const RuleSpec& rs, Rng& r,
 
 extern "C" {
 
-// Writes configuration `cfg` (c1, c2, c2s, c3, c4) for `seed` into `outDir`.
-// nRules < 0 keeps the configuration's rule count.  Returns the triple count,
-// or -1 on an unknown configuration or an I/O error.
-long long kg_synth_write(const char* cfg, unsigned long long seed, int nRules, const char* outDir) {
+// Writes configuration `cfg` (c1, c2, c2s, c3, c4) for graph seed `seed`
+// into `outDir`; the rules continue the graph's random stream, or, when
+// ruleSeed != ~0, come from their own stream seeded with ruleSeed (the graph
+// is the same either way).  nRules < 0 keeps the configuration's rule count.
+// Returns the triple count, or -1 on an unknown configuration or I/O error.
+long long kg_synth_write2(const char* cfg, unsigned long long seed, unsigned long long ruleSeed, int nRules,
+                          const char* outDir) {
     std::string c(cfg);
     Rng r(seed);
     Graph g;
@@ -327,11 +332,16 @@ long long kg_synth_write(const char* cfg, unsigned long long seed, int nRules, c
         return -1;
     }
     if (nRules >= 0) rs.n = nRules;
+    if (ruleSeed != ~0ull) r = Rng(ruleSeed ^ 0xA5A5A5A5DEADBEEFull);
     std::vector<RuleIR> rules;
     std::vector<std::string> texts;
     make_rules(g, rs, r, rules, texts);
-    if (!write_all(outDir, g, rules, texts, c, seed)) return -1;
+    if (!write_all(outDir, g, rules, texts, c, seed, ruleSeed)) return -1;
     return (long long)g.t.size();
+}
+
+long long kg_synth_write(const char* cfg, unsigned long long seed, int nRules, const char* outDir) {
+    return kg_synth_write2(cfg, seed, ~0ull, nRules, outDir);
 }
 
 // Request stream for the serving configuration: n closed chain rules over a

@@ -34,22 +34,31 @@ def _load():
         _lib = ctypes.CDLL(str(so))
         _lib.kg_synth_write.restype = ctypes.c_longlong
         _lib.kg_synth_write.argtypes = [ctypes.c_char_p, ctypes.c_ulonglong, ctypes.c_int, ctypes.c_char_p]
+        _lib.kg_synth_write2.restype = ctypes.c_longlong
+        _lib.kg_synth_write2.argtypes = [ctypes.c_char_p, ctypes.c_ulonglong, ctypes.c_ulonglong, ctypes.c_int,
+                                         ctypes.c_char_p]
         _lib.kg_synth_rule_stream.restype = ctypes.c_int
         _lib.kg_synth_rule_stream.argtypes = [ctypes.POINTER(ctypes.c_longlong), ctypes.c_int, ctypes.c_int,
                                               ctypes.c_double, ctypes.c_int, ctypes.c_ulonglong, ctypes.c_char_p]
     return _lib
 
 
-def generate(cfg: str, out_dir: Path | str, seed: int = 0, n_rules: int = -1) -> Path:
-    """Writes graph.ttl, triples.bin, rules.txt, rules.ir and meta.txt (cached)."""
+def generate(cfg: str, out_dir: Path | str, seed: int = 0, n_rules: int = -1, rule_seed: int | None = None) -> Path:
+    """Writes graph.ttl, triples.bin, rules.txt, rules.ir and meta.txt (cached).
+
+    rule_seed=None continues the graph's random stream (the configuration's
+    standard rule set); an integer draws the rules from their own stream."""
     out = Path(out_dir)
     out.mkdir(parents=True, exist_ok=True)
     meta = out / "meta.txt"
     want = f"config={cfg}\nseed={seed}\n"
     if meta.exists() and meta.read_text().startswith(want) and (out / "graph.ttl").exists():
-        if n_rules < 0 or read_meta(out).get("rules") == str(n_rules):
+        m = read_meta(out)
+        if (n_rules < 0 or m.get("rules") == str(n_rules)) and m.get("rule_seed") == (
+                None if rule_seed is None else str(rule_seed)):
             return out
-    n = _load().kg_synth_write(cfg.encode(), seed, n_rules, str(out).encode())
+    rs = (1 << 64) - 1 if rule_seed is None else int(rule_seed)
+    n = _load().kg_synth_write2(cfg.encode(), seed, rs, n_rules, str(out).encode())
     if n < 0:
         raise RuntimeError(f"generator failed for {cfg}")
     return out

@@ -144,3 +144,18 @@ def test_oracle_agrees_on_c2_skew_batch(data_dir):
         res, _, _ = lib.evaluate_rules_batch(rules)
     got = np.array([[r.support, r.headSize, r.headSupport, r.bodySize] for r in res], dtype=np.int64)
     assert (got == counts).all()
+
+
+def test_prepared_batch_replays_exactly(tmp_path):
+    fx = load_fixture("fuzz_4.json")
+    p = tmp_path / "graph.ttl"
+    p.write_text(fx["ttl"])
+    with eng.GpuRulesLib(p) as lib:
+        with lib.prepare_batch(fx["rules"]) as b:
+            info = b.info()
+            assert info["h2d_bytes"] > 0 and info["d2h_bytes"] > 0
+            for flush in (0, 1 << 20, 0):
+                res, st, ms = b.run(flush)
+                assert ms >= 0
+                _check(res, fx["expected"], f"prepared run flush={flush}")
+            assert b.count_bytes() > 0
