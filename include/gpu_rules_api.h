@@ -101,6 +101,19 @@ int gpu_batch_count_bytes(void* batch, unsigned long long* bytes);
 /* Frees a prepared batch (NULL is ignored). */
 void gpu_batch_free(void* batch);
 
+/* No counterpart in the reference.  Same as gpu_evaluate_rule, for callers
+ * that cannot allocate device memory while they evaluate: a host framework
+ * that owns a fixed device-memory budget and forbids allocation per request,
+ * or a serving loop that must not call cudaMalloc/cudaFree because they can
+ * synchronise the whole device.  The per-call device buffers (plan, tasks,
+ * counters, status and, for very large hO domains, the pair bitmap) come from
+ * one 8 MiB array built into the library (held on every GPU that loads it
+ * until the process exits); a rule that needs more returns -1 with the size
+ * in gpu_last_error().  The first call on a device looks up the array's
+ * device address (make it before any stream capture).  Calls share the array:
+ * calls that overlap on the same GPU race and must be serialised. */
+int gpu_evaluate_rule_noalloc(void* ctx, const char* ruleText, GpuRuleResult* out);
+
 /* Number of entities, predicates and distinct triples of a loaded graph. */
 int gpu_graph_stats(void* ctx, long long* entities, long long* predicates, long long* triples);
 

@@ -33,6 +33,7 @@ API_SYMBOLS = (
     "gpu_batch_info",
     "gpu_batch_count_bytes",
     "gpu_batch_free",
+    "gpu_evaluate_rule_noalloc",
     "gpu_graph_stats",
     "gpu_last_error",
 )
@@ -98,6 +99,8 @@ def load_library(path: os.PathLike | str | None = None) -> ctypes.CDLL:
     lib.gpu_batch_count_bytes.argtypes = [ctypes.c_void_p, ctypes.POINTER(ctypes.c_ulonglong)]
     lib.gpu_batch_free.restype = None
     lib.gpu_batch_free.argtypes = [ctypes.c_void_p]
+    lib.gpu_evaluate_rule_noalloc.restype = ctypes.c_int
+    lib.gpu_evaluate_rule_noalloc.argtypes = [ctypes.c_void_p, ctypes.c_char_p, ctypes.POINTER(GpuRuleResult)]
     lib.gpu_graph_stats.restype = ctypes.c_int
     lib.gpu_graph_stats.argtypes = [ctypes.c_void_p] + [ctypes.POINTER(ctypes.c_longlong)] * 3
     lib.gpu_last_error.restype = ctypes.c_char_p
@@ -157,6 +160,16 @@ class GpuRulesLib:
             raise RuntimeError(f"gpu_evaluate_rules_batch failed "
                                f"({self._lib.gpu_last_error().decode(errors='replace')})")
         return list(out)[:n], list(st)[:n], ms.value
+
+    def evaluate_rule_noalloc(self, rule_text: str) -> GpuRuleResult:
+        """gpu_evaluate_rule without any device allocation (fixed in-library
+        scratch; for callers that may not call cudaMalloc per request)."""
+        res = GpuRuleResult()
+        rc = self._lib.gpu_evaluate_rule_noalloc(self._handle(), rule_text.encode(), ctypes.byref(res))
+        if rc != 0:
+            raise RuntimeError(f"gpu_evaluate_rule_noalloc error code {rc} for: {rule_text} "
+                               f"({self._lib.gpu_last_error().decode(errors='replace')})")
+        return res
 
     def prepare_batch(self, rules: Sequence[str], is_json: bool = False) -> "PreparedBatch":
         return PreparedBatch(self, rules, is_json)

@@ -16,6 +16,7 @@
 #include <cstdio>
 #include <cstring>
 #include <memory>
+#include <mutex>
 #include <numeric>
 #include <string>
 #include <vector>
@@ -582,3 +583,122 @@ int gpu_graph_stats(void* ctx, long long* entities, long long* predicates, long 
 }
 
 }  // extern "C"
+
+// ---------------------------------------------------------------------------
+// Evaluation without device allocation.
+//
+// Some callers cannot call cudaMalloc while they evaluate rules: a host
+// framework that owns a fixed device-memory budget and forbids allocation at
+// request time, a serving loop that must not hit cudaMalloc/cudaFree (both can
+// synchronise the whole device and stall concurrent work), or code that runs
+// between other libraries' stream-ordered work and must not change the
+// device's memory map.  gpu_evaluate_rule_noalloc serves them: it evaluates a
+// rule exactly like gpu_evaluate_rule (one launch per phase, same results)
+// but takes every per-call device buffer (plan, tasks, task counter, status
+// word, result counter and, for very large hO domains, the pair bitmap) from
+// the fixed array below instead of allocating.
+//
+// The array is a file-scope __device__ object of kNoAllocScratchBytes; every
+// GPU that loads this library holds it until the process exits.  Host code
+// cannot use the array's name as a device address, so the first call on each
+// device (with that device current) looks the address up with
+// cudaGetSymbolAddress and caches it; make that first call before any stream
+// capture.  All calls share the array and it keeps the previous call's
+// contents, so each call clears the parts that must start at zero.  Calls
+// that overlap on the GPU (from several threads, contexts or streams of the
+// same device) race on the array and must be serialised by the caller.
+namespace gr {
+namespace {
+constexpr size_t kNoAllocScratchBytes = 8u << 20;   // 8 MiB
+constexpr size_t kNoAllocHeader = 256;               // [0,8) counter+status, [64,72) result
+constexpr int kNoAllocMaxDevices = 64;
+}  // namespace
+}  // namespace gr
+
+static __device__ __align__(256) unsigned char g_noallocScratch[gr::kNoAllocScratchBytes];
+
+namespace gr {
+namespace {
+
+std::mutex g_noallocMu;
+void* g_noallocAddr[kNoAllocMaxDevices] = {};
+
+// Device address of the scratch array on `dev` (which must be current).
+void* noalloc_scratch(int dev) {
+    if (dev < 0 || dev >= kNoAllocMaxDevices) throw CudaError("device ordinal out of range");
+    std::lock_guard<std::mutex> lk(g_noallocMu);
+    if (!g_noallocAddr[dev]) {
+        void* p = nullptr;
+        ck(cudaGetSymbolAddress(&p, g_noallocScratch), "cudaGetSymbolAddress(scratch)");
+        g_noallocAddr[dev] = p;
+    }
+    return g_noallocAddr[dev];
+}
+
+size_t align256(size_t x) { return (x + 255) & ~size_t(255); }
+
+int64_t run_phase_noalloc(Context& c, const PhasePlan& ph, char* scratch, float* ms) {
+    DevPlan plan = ph.plan;
+    std::vector<DevTask> tasks;
+    make_tasks(ph, 0, c.hix, tasks, nullptr);
+    const size_t planOff = kNoAllocHeader;
+    const size_t taskOff = align256(planOff + sizeof(DevPlan));
+    const size_t bitmapOff = align256(taskOff + tasks.size() * sizeof(DevTask));
+    size_t bitmapWords = 0;
+    if (ph.needsGlobalBitmap)
+        bitmapWords = ((size_t)(ph.rootEnd - ph.rootBeg) * (size_t)plan.wo + 31) / 32;
+    const size_t need = bitmapOff + bitmapWords * 4;
+    if (need > kNoAllocScratchBytes)
+        throw CudaError("rule needs " + std::to_string(need) + " bytes of scratch; the no-allocation limit is " +
+                        std::to_string(kNoAllocScratchBytes) + " bytes");
+    plan.resultSlot = 0;
+    plan.gBitmap = bitmapWords ? reinterpret_cast<uint32_t*>(scratch + bitmapOff) : nullptr;
+    plan.gRowBase = bitmapWords ? ph.rootBeg : 0;
+    int* ctl = reinterpret_cast<int*>(scratch);
+    unsigned long long* result = reinterpret_cast<unsigned long long*>(scratch + 64);
+    ck(cudaMemcpyAsync(scratch + planOff, &plan, sizeof(DevPlan), cudaMemcpyHostToDevice, c.stream), "H2D plan");
+    if (!tasks.empty())
+        ck(cudaMemcpyAsync(scratch + taskOff, tasks.data(), tasks.size() * sizeof(DevTask), cudaMemcpyHostToDevice,
+                           c.stream), "H2D tasks");
+    ck(cudaMemsetAsync(scratch, 0, kNoAllocHeader, c.stream), "clear header");
+    if (bitmapWords) ck(cudaMemsetAsync(scratch + bitmapOff, 0, bitmapWords * 4, c.stream), "clear bitmap");
+    ck(cudaEventRecord(c.ev[2], c.stream), "event");
+    int grid = std::max(1, std::min((int)tasks.size(), c.grid));
+    ck(engine_launch(c.dix, reinterpret_cast<const DevPlan*>(scratch + planOff),
+                     reinterpret_cast<const DevTask*>(scratch + taskOff), (int)tasks.size(), ctl, result, ctl + 1,
+                     grid, c.stream, nullptr), "engine launch");
+    ck(cudaEventRecord(c.ev[3], c.stream), "event");
+    unsigned long long count = 0;
+    int st[2] = {0, 0};
+    ck(cudaMemcpyAsync(&count, result, sizeof(count), cudaMemcpyDeviceToHost, c.stream), "D2H result");
+    ck(cudaMemcpyAsync(st, ctl, sizeof(st), cudaMemcpyDeviceToHost, c.stream), "D2H status");
+    ck(cudaStreamSynchronize(c.stream), "engine");
+    if (st[1] != 0) throw CudaError("engine reported internal status " + std::to_string(st[1]));
+    ck(cudaEventElapsedTime(ms, c.ev[2], c.ev[3]), "elapsed");
+    return (int64_t)count;
+}
+
+}  // namespace
+}  // namespace gr
+
+extern "C" int gpu_evaluate_rule_noalloc(void* ctx, const char* ruleText, GpuRuleResult* out) {
+    if (!ctx || !ruleText || !out) return -1;
+    *out = GpuRuleResult{};
+    Context& c = *as_ctx(ctx);
+    try {
+        ck(cudaSetDevice(c.device), "cudaSetDevice");
+        char* scratch = static_cast<char*>(noalloc_scratch(c.device));
+        Rule r = c.parser->parse_text(ruleText);
+        RulePlan rp = plan_rule(r, c.hix);
+        int64_t sup = rp.support.value, body = rp.body.value;
+        float supMs = 0.f, confMs = 0.f;
+        if (rp.status == kRuleOk && rp.support.how == kDevice) sup = run_phase_noalloc(c, rp.support, scratch, &supMs);
+        if (rp.status == kRuleOk && rp.body.how == kDevice) body = run_phase_noalloc(c, rp.body, scratch, &confMs);
+        compose(rp, sup, body, supMs, confMs, out);
+        return 0;
+    } catch (const std::exception& e) {
+        set_error(std::string("gpu_evaluate_rule_noalloc error: ") + e.what());
+        *out = GpuRuleResult{};
+        return -1;
+    }
+}
