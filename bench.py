@@ -58,6 +58,7 @@ def parse_args():
     ap.add_argument("--config", default="c3")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-per-rule", action="store_true")
+    ap.add_argument("--max-rules", type=int, default=0, help="use only the first N rules (profiling case)")
     ap.add_argument("--data", default=os.environ.get("KG_DATA_DIR", str(Path(tempfile.gettempdir()) / "kg_synth_data")))
     return ap.parse_args()
 
@@ -239,8 +240,11 @@ def engine_arm(args):
     from masterthesis_gpu_acceleration_b200 import synth
     d = data_for(args, rank)
     rules = synth.read_rules(d)
+    if args.max_rules > 0:
+        rules = rules[:args.max_rules]
     lib = eng.GpuRulesLib(d / "graph.ttl")
     batch = lib.prepare_batch(rules)
+    batch.autotune(2)   # feedback-directed task balancing (untimed, learnt per plan signature)
     info = batch.info()
 
     # ---- device-resident batched form ----
@@ -261,7 +265,7 @@ def engine_arm(args):
     value = world * len(rules) * args.steps / (max_ms / 1e3)
 
     exact = None
-    if rank == 0 and args.config == "c3":
+    if rank == 0 and args.config == "c3" and not args.max_rules:
         gold = ROOT / "tests" / "golden" / "c3_seed0.npz"
         if gold.exists():
             exp = np.load(gold)["expected"]

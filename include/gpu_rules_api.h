@@ -98,6 +98,24 @@ int gpu_batch_info(void* batch, long long* plans, long long* tasks, long long* h
  * algorithmic bytes).  Not timed. */
 int gpu_batch_count_bytes(void* batch, unsigned long long* bytes);
 
+/* Runs the batch once with the instrumented kernel variant.  bytes
+ * (optional) receives the algorithmic bytes as gpu_batch_count_bytes does;
+ * for the first maxTasks device tasks, taskNs (optional, 2 per task)
+ * receives the start and end time (device global timer, ns) and taskInfo
+ * (optional, 3 per task) the owner (rule * 2 + phase, phase 0 = support,
+ * 1 = body size) and the root range.  Not timed. */
+int gpu_batch_profile(void* batch, unsigned long long* bytes, unsigned long long* taskNs, int* taskInfo,
+                      long long maxTasks);
+
+/* Feedback-directed task balancing: runs the instrumented kernel `rounds`
+ * times; after each run the context's task builder learns, per plan
+ * signature, the device time per unit of estimated work, marks the phases
+ * whose slowest task held up the launch for an exact per-root measurement,
+ * and the batch's tasks are rebuilt and re-uploaded.  What is learnt stays
+ * with the context and also balances later batches and per-rule calls with
+ * the same plans.  Returns 0, or -1 on a CUDA error. */
+int gpu_batch_autotune(void* batch, int rounds);
+
 /* Frees a prepared batch (NULL is ignored). */
 void gpu_batch_free(void* batch);
 
@@ -113,6 +131,15 @@ void gpu_batch_free(void* batch);
  * device address (make it before any stream capture).  Calls share the array:
  * calls that overlap on the same GPU race and must be serialised. */
 int gpu_evaluate_rule_noalloc(void* ctx, const char* ruleText, GpuRuleResult* out);
+
+/* Engine option for later calls on this context.  "block": threads per
+ * block of the engine kernel, 128, 256 or 512 (default 256; the environment
+ * variable GPU_RULES_BLOCK sets it at load).  "task_target": fixed work per
+ * task in candidate bindings (0 = automatic balancing).  "walk_threshold":
+ * estimated work above which a phase's roots are measured one by one before
+ * splitting (default 200000).  Returns 0, or -1 for an unknown name or
+ * value. */
+int gpu_set_option(void* ctx, const char* name, long long value);
 
 /* Number of entities, predicates and distinct triples of a loaded graph. */
 int gpu_graph_stats(void* ctx, long long* entities, long long* predicates, long long* triples);

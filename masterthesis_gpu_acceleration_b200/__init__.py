@@ -34,6 +34,9 @@ API_SYMBOLS = (
     "gpu_batch_count_bytes",
     "gpu_batch_free",
     "gpu_evaluate_rule_noalloc",
+    "gpu_batch_profile",
+    "gpu_batch_autotune",
+    "gpu_set_option",
     "gpu_graph_stats",
     "gpu_last_error",
 )
@@ -101,6 +104,13 @@ def load_library(path: os.PathLike | str | None = None) -> ctypes.CDLL:
     lib.gpu_batch_free.argtypes = [ctypes.c_void_p]
     lib.gpu_evaluate_rule_noalloc.restype = ctypes.c_int
     lib.gpu_evaluate_rule_noalloc.argtypes = [ctypes.c_void_p, ctypes.c_char_p, ctypes.POINTER(GpuRuleResult)]
+    lib.gpu_batch_profile.restype = ctypes.c_int
+    lib.gpu_batch_profile.argtypes = [ctypes.c_void_p, ctypes.POINTER(ctypes.c_ulonglong), ctypes.c_void_p,
+                                      ctypes.c_void_p, ctypes.c_longlong]
+    lib.gpu_batch_autotune.restype = ctypes.c_int
+    lib.gpu_batch_autotune.argtypes = [ctypes.c_void_p, ctypes.c_int]
+    lib.gpu_set_option.restype = ctypes.c_int
+    lib.gpu_set_option.argtypes = [ctypes.c_void_p, ctypes.c_char_p, ctypes.c_longlong]
     lib.gpu_graph_stats.restype = ctypes.c_int
     lib.gpu_graph_stats.argtypes = [ctypes.c_void_p] + [ctypes.POINTER(ctypes.c_longlong)] * 3
     lib.gpu_last_error.restype = ctypes.c_char_p
@@ -174,6 +184,10 @@ class GpuRulesLib:
     def prepare_batch(self, rules: Sequence[str], is_json: bool = False) -> "PreparedBatch":
         return PreparedBatch(self, rules, is_json)
 
+    def set_option(self, name: str, value: int) -> None:
+        if self._lib.gpu_set_option(self._handle(), name.encode(), int(value)) != 0:
+            raise ValueError(f"bad option {name}={value}")
+
     def stats(self) -> dict:
         e, p, t = ctypes.c_longlong(), ctypes.c_longlong(), ctypes.c_longlong()
         self._lib.gpu_graph_stats(self._handle(), ctypes.byref(e), ctypes.byref(p), ctypes.byref(t))
@@ -234,11 +248,33 @@ class PreparedBatch:
         self._lib.gpu_batch_info(self._h, *[ctypes.byref(x) for x in v])
         return dict(zip(("plans", "tasks", "h2d_bytes", "d2h_bytes"), (x.value for x in v)))
 
+    def autotune(self, rounds: int = 1) -> None:
+        """Measure task times and rebalance the batch's tasks (see gpu_batch_autotune)."""
+        if self._lib.gpu_batch_autotune(self._h, rounds) != 0:
+            raise RuntimeError(f"gpu_batch_autotune failed ({self._lib.gpu_last_error().decode(errors='replace')})")
+
     def count_bytes(self) -> int:
         b = ctypes.c_ulonglong()
         if self._lib.gpu_batch_count_bytes(self._h, ctypes.byref(b)) != 0:
             raise RuntimeError("gpu_batch_count_bytes failed")
         return b.value
+
+    def profile(self):
+        """Instrumented run: (algorithmic bytes, task table) where each task row is
+        (rule, phase, root_begin, root_end, start_ns, end_ns)."""
+        import numpy as np
+        n = self.info()["tasks"]
+        ns = np.zeros((max(n, 1), 2), dtype=np.uint64)
+        ti = np.zeros((max(n, 1), 3), dtype=np.int32)
+        b = ctypes.c_ulonglong()
+        if self._lib.gpu_batch_profile(self._h, ctypes.byref(b), ns.ctypes.data, ti.ctypes.data, n) != 0:
+            raise RuntimeError("gpu_batch_profile failed")
+        tab = np.zeros((n, 6), dtype=np.int64)
+        tab[:, 0] = ti[:n, 0] // 2
+        tab[:, 1] = ti[:n, 0] % 2
+        tab[:, 2:4] = ti[:n, 1:3]
+        tab[:, 4:6] = ns[:n].astype(np.int64)
+        return b.value, tab
 
     def close(self):
         if getattr(self, "_h", None) is not None:

@@ -120,17 +120,41 @@ struct DevPlan {
     DevUsed used[kMaxUsed];
     uint32_t* gBitmap;            // kPairs with a global bitmap (null: shared memory)
     int64_t gRowBase;             // first root of the plan, for global bitmap rows
+    uint32_t* gHeavy;             // global dedup rows of split heavy roots
+    int32_t rowWords;             // words per heavy row (kPairs: ceil(wo / 32); kExist: 1)
+    int32_t pad1;
 };
 
+// A unit of device work: the roots [beg, end) of one plan.  A heavy root is
+// split over several tasks (gRow >= 0, end == beg + 1): each takes the slice
+// [sub0, sub1) of the root's first neighbour segment and deduplicates into
+// the plan's global row gRow, so the slices together count each pair (or
+// the root) once.
 struct DevTask {
     int32_t plan;
     int32_t beg, end;        // root range
-    int32_t pad;
+    int32_t sub0, sub1;      // heavy root: slice of the first segment
+    int32_t gRow;            // heavy root: global dedup row, else -1
 };
 
-// Engine launch geometry and shared-memory budget.
-constexpr int kBlock = 512;
-constexpr int kItemInts = 8192;        // frontier storage per block (ints)
-constexpr int kBitmapWords = 16384;    // per-block dedup bitmap (u32 words) = 64 KiB
+// Engine launch geometry: block size B (128, 256 or 512 threads) with a
+// shared-memory budget that scales with it, so 1024 / B blocks stay
+// resident per SM.  Frontier storage: 16 ints per thread; dedup bitmap:
+// 32 words (1024 bits) per thread.
+struct Geom {
+    int block = 256;
+    static constexpr int items_for(int b) { return 16 * b; }
+    static constexpr int words_for(int b) { return 32 * b; }
+    int itemInts() const { return items_for(block); }
+    int bitmapWords() const { return words_for(block); }
+};
+
+// Profiling outputs of the instrumented kernel variant (null members are
+// skipped): requested global-memory bytes, and per task its start and end
+// time (globaltimer ns).
+struct EngineProfile {
+    unsigned long long* bytes = nullptr;
+    unsigned long long* taskNs = nullptr;
+};
 
 }  // namespace gr

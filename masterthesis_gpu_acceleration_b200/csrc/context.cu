@@ -14,6 +14,7 @@
 #include <algorithm>
 #include <climits>
 #include <cstdio>
+#include <cstdlib>
 #include <cstring>
 #include <memory>
 #include <mutex>
@@ -26,15 +27,16 @@
 #include "index.hpp"
 #include "planner.hpp"
 #include "rules.hpp"
+#include "tasks.hpp"
 #include "turtle.hpp"
 
 namespace gr {
 
-size_t engine_smem_bytes();
+size_t engine_smem_bytes(int block);
 cudaError_t engine_configure();
 cudaError_t engine_launch(const DevIndex& ix, const DevPlan* plans, const DevTask* tasks, int nTasks,
-                          int* taskCounter, unsigned long long* results, int* status, int grid,
-                          cudaStream_t stream, unsigned long long* bytesOut);
+                          int* taskCounter, unsigned long long* results, int* status, int grid, int block,
+                          cudaStream_t stream, const EngineProfile* prof);
 
 namespace {
 
@@ -98,17 +100,19 @@ struct Context;
 // A set of plans and their tasks resident on the device, with the buffers
 // one launch over them needs.
 struct Staged {
-    DevBuf dBlob, dResults, dCtl, dBitmap, dBytes;
+    DevBuf dBlob, dResults, dCtl, dBitmap, dHeavy, dBytes, dTaskNs;
+    std::vector<DevTask> hTasks;  // task list as uploaded (for profiles)
+    std::vector<double> hCost;    // estimated work per uploaded task
     HostBuf hBlob, hResults, hCtl;
     const DevPlan* dPlans = nullptr;
     const DevTask* dTasks = nullptr;
     int nPlans = 0, nTasks = 0;
-    size_t bitmapWords = 0;
+    size_t bitmapWords = 0, heavyWords = 0;
     size_t h2dBytes = 0, d2hBytes = 0;
 
     void stage(Context& c, std::vector<DevPlan>& plans, const std::vector<const PhasePlan*>& phases,
                bool sortTasks, cudaStream_t s);
-    void enqueue(Context& c, cudaStream_t s, bool countBytes);
+    void enqueue(Context& c, cudaStream_t s, bool profile);
     void download(cudaStream_t s) {
         if (!nPlans) return;
         ck(cudaMemcpyAsync(hResults.p, dResults.p, nPlans * sizeof(unsigned long long), cudaMemcpyDeviceToHost, s), "D2H results");
@@ -131,6 +135,8 @@ struct Context {
     cudaStream_t stream = nullptr;
     cudaEvent_t ev[4] = {};
     Staged one;          // per-rule launches
+    std::unique_ptr<TaskBuilder> tasks;
+    Geom geom;
     int grid = 0;
     int sms = 0;
     std::unique_ptr<RuleParser> parser;
@@ -191,11 +197,19 @@ struct Context {
         dix.nTriples = h.nTriples;
     }
 
+    bool set_block(int b) {
+        if (b != 128 && b != 256 && b != 512) return false;
+        geom.block = b;
+        grid = sms * (1024 / b);
+        return true;
+    }
+
     void init_device() {
         ck(cudaGetDevice(&device), "cudaGetDevice");
         ck(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device), "cudaDeviceGetAttribute");
         ck(engine_configure(), "cudaFuncSetAttribute");
-        grid = sms * 2;
+        if (const char* b = std::getenv("GPU_RULES_BLOCK")) set_block(std::atoi(b));
+        else set_block(geom.block);
         ck(cudaStreamCreateWithFlags(&stream, cudaStreamNonBlocking), "cudaStreamCreate");
         for (auto& e : ev) ck(cudaEventCreate(&e), "cudaEventCreate");
     }
@@ -216,24 +230,42 @@ void Staged::stage(Context& c, std::vector<DevPlan>& plans, const std::vector<co
         bitmapWords += (rows * (size_t)plans[i].wo + 31) / 32;
     }
     if (bitmapWords) dBitmap.ensure(bitmapWords * 4);
+    std::vector<PhaseTasks> pts;
+    c.tasks->build(phases, c.grid, true, pts);
+    std::vector<size_t> hOff(nPlans, 0);
+    heavyWords = 0;
+    for (int i = 0; i < nPlans; ++i) {
+        plans[i].rowWords = plans[i].mode == kPairs ? (plans[i].wo + 31) / 32 : 1;
+        hOff[i] = heavyWords;
+        heavyWords += (size_t)pts[i].heavyRows * plans[i].rowWords;
+    }
+    if (heavyWords) dHeavy.ensure(heavyWords * 4);
     std::vector<DevTask> tasks;
     std::vector<double> cost;
     for (int i = 0; i < nPlans; ++i) {
         plans[i].resultSlot = i;
         plans[i].gBitmap = phases[i]->needsGlobalBitmap ? static_cast<uint32_t*>(dBitmap.p) + gOff[i] : nullptr;
         plans[i].gRowBase = phases[i]->needsGlobalBitmap ? phases[i]->rootBeg : 0;
-        make_tasks(*phases[i], i, c.hix, tasks, &cost);
+        plans[i].gHeavy = pts[i].heavyRows ? static_cast<uint32_t*>(dHeavy.p) + hOff[i] : nullptr;
+        tasks.insert(tasks.end(), pts[i].tasks.begin(), pts[i].tasks.end());
+        cost.insert(cost.end(), pts[i].cost.begin(), pts[i].cost.end());
     }
     if (sortTasks && tasks.size() > 1) {
-        // longest tasks first, so the tail of the persistent launch is short
+        // longest (estimated device time) first, so the tail of the launch is short
+        std::vector<double> t(tasks.size());
+        for (size_t i = 0; i < tasks.size(); ++i) t[i] = cost[i] * pts[tasks[i].plan].scale;
         std::vector<size_t> ord(tasks.size());
         std::iota(ord.begin(), ord.end(), 0);
-        std::stable_sort(ord.begin(), ord.end(), [&](size_t a, size_t b) { return cost[a] > cost[b]; });
+        std::stable_sort(ord.begin(), ord.end(), [&](size_t a, size_t b) { return t[a] > t[b]; });
         std::vector<DevTask> t2(tasks.size());
-        for (size_t i = 0; i < ord.size(); ++i) t2[i] = tasks[ord[i]];
+        std::vector<double> c2(tasks.size());
+        for (size_t i = 0; i < ord.size(); ++i) { t2[i] = tasks[ord[i]]; c2[i] = cost[ord[i]]; }
         tasks.swap(t2);
+        cost.swap(c2);
     }
     nTasks = (int)tasks.size();
+    hTasks = tasks;
+    hCost = cost;
     size_t planBytes = (size_t)nPlans * sizeof(DevPlan);
     size_t taskBytes = (size_t)nTasks * sizeof(DevTask);
     size_t blob = planBytes + taskBytes;
@@ -252,20 +284,24 @@ void Staged::stage(Context& c, std::vector<DevPlan>& plans, const std::vector<co
     d2hBytes = (size_t)nPlans * sizeof(unsigned long long) + 8;
 }
 
-void Staged::enqueue(Context& c, cudaStream_t s, bool countBytes) {
+void Staged::enqueue(Context& c, cudaStream_t s, bool profile) {
     if (!nPlans) return;
     ck(cudaMemsetAsync(dResults.p, 0, (size_t)nPlans * sizeof(unsigned long long), s), "memset results");
     ck(cudaMemsetAsync(dCtl.p, 0, 8, s), "memset ctl");
     if (bitmapWords) ck(cudaMemsetAsync(dBitmap.p, 0, bitmapWords * 4, s), "memset bitmap");
-    unsigned long long* bytes = nullptr;
-    if (countBytes) {
+    if (heavyWords) ck(cudaMemsetAsync(dHeavy.p, 0, heavyWords * 4, s), "memset heavy rows");
+    EngineProfile prof;
+    if (profile) {
         dBytes.ensure(8);
+        dTaskNs.ensure((size_t)std::max(nTasks, 1) * 16);
         ck(cudaMemsetAsync(dBytes.p, 0, 8, s), "memset bytes");
-        bytes = static_cast<unsigned long long*>(dBytes.p);
+        prof.bytes = static_cast<unsigned long long*>(dBytes.p);
+        prof.taskNs = static_cast<unsigned long long*>(dTaskNs.p);
     }
     int grid = std::max(1, std::min(nTasks, c.grid));
     ck(engine_launch(c.dix, dPlans, dTasks, nTasks, static_cast<int*>(dCtl.p),
-                     static_cast<unsigned long long*>(dResults.p), static_cast<int*>(dCtl.p) + 1, grid, s, bytes),
+                     static_cast<unsigned long long*>(dResults.p), static_cast<int*>(dCtl.p) + 1, grid,
+                     c.geom.block, s, profile ? &prof : nullptr),
        "engine launch");
 }
 
@@ -277,6 +313,8 @@ struct Batch {
     std::vector<RulePlan> rps;
     std::vector<int> parseStatus;
     std::vector<int> owner;  // plan -> rule * 2 + phase
+    std::vector<DevPlan> plans0;
+    std::vector<const PhasePlan*> phases;
     Staged st;
     cudaStream_t stream = nullptr;
     cudaEvent_t ev0 = nullptr, ev1 = nullptr;
@@ -328,7 +366,7 @@ int64_t run_one_phase(Context& c, const PhasePlan& ph, float* ms) {
 }
 
 int evaluate_parsed(Context& c, const Rule& rule, GpuRuleResult* out) {
-    RulePlan rp = plan_rule(rule, c.hix);
+    RulePlan rp = plan_rule(rule, c.hix, c.geom);
     int64_t sup = rp.support.value, body = rp.body.value;
     float supMs = 0.f, confMs = 0.f;
     if (rp.status == kRuleOk && rp.support.how == kDevice) sup = run_one_phase(c, rp.support, &supMs);
@@ -350,7 +388,7 @@ void prepare(Batch& b, Context& c, const char* const* rules, int n, int isJson) 
         if (!rules[i]) { b.parseStatus[i] = -1; continue; }
         try {
             Rule r = isJson ? c.parser->parse_json(rules[i]) : c.parser->parse_text(rules[i]);
-            b.rps[i] = plan_rule(r, c.hix);
+            b.rps[i] = plan_rule(r, c.hix, c.geom);
         } catch (const RuleError&) {
             b.parseStatus[i] = -1;
             continue;
@@ -363,6 +401,8 @@ void prepare(Batch& b, Context& c, const char* const* rules, int n, int isJson) 
     if (!b.stream) ck(cudaStreamCreateWithFlags(&b.stream, cudaStreamNonBlocking), "cudaStreamCreate");
     if (!b.ev0) ck(cudaEventCreate(&b.ev0), "cudaEventCreate");
     if (!b.ev1) ck(cudaEventCreate(&b.ev1), "cudaEventCreate");
+    b.plans0 = plans;
+    b.phases = phases;
     b.st.stage(c, plans, phases, true, b.stream);
 }
 
@@ -444,6 +484,7 @@ void* gpu_load_graph(const char* ttlPath) {
         }
         c->prefixes = scan_rule_prefixes(ttlPath);
         c->hix = build_index(spo, (int32_t)c->ents.size(), (int32_t)c->preds.size());
+        c->tasks.reset(new TaskBuilder(c->hix));
         c->parser.reset(new RuleParser(c->ents, c->preds, c->prefixes));
         c->init_device();
         c->upload_index();
@@ -553,20 +594,72 @@ int gpu_batch_info(void* batch, long long* plans, long long* tasks, long long* h
 }
 
 int gpu_batch_count_bytes(void* batch, unsigned long long* bytes) {
-    if (!batch || !bytes) return -1;
+    return gpu_batch_profile(batch, bytes, nullptr, nullptr, 0);
+}
+
+int gpu_batch_profile(void* batch, unsigned long long* bytes, unsigned long long* taskNs, int* taskInfo,
+                      long long maxTasks) {
+    if (!batch) return -1;
     Batch& b = *static_cast<Batch*>(batch);
     try {
         cudaSetDevice(b.c->device);
-        *bytes = 0;
+        if (bytes) *bytes = 0;
         if (!b.st.nPlans) return 0;
         b.st.enqueue(*b.c, b.stream, true);
-        ck(cudaMemcpyAsync(bytes, b.st.dBytes.p, 8, cudaMemcpyDeviceToHost, b.stream), "D2H bytes");
-        ck(cudaStreamSynchronize(b.stream), "count");
+        unsigned long long by = 0;
+        ck(cudaMemcpyAsync(&by, b.st.dBytes.p, 8, cudaMemcpyDeviceToHost, b.stream), "D2H bytes");
+        long long n = std::min<long long>(maxTasks, b.st.nTasks);
+        if (taskNs && n > 0)
+            ck(cudaMemcpyAsync(taskNs, b.st.dTaskNs.p, (size_t)n * 16, cudaMemcpyDeviceToHost, b.stream), "D2H task times");
+        ck(cudaStreamSynchronize(b.stream), "profile");
+        if (bytes) *bytes = by;
+        if (taskInfo)
+            for (long long t = 0; t < n; ++t) {
+                const DevTask& tk = b.st.hTasks[t];
+                taskInfo[3 * t] = b.owner[tk.plan];
+                taskInfo[3 * t + 1] = tk.beg;
+                taskInfo[3 * t + 2] = tk.end;
+            }
         return 0;
     } catch (const std::exception& e) {
-        set_error(std::string("gpu_batch_count_bytes error: ") + e.what());
+        set_error(std::string("gpu_batch_profile error: ") + e.what());
         return -1;
     }
+}
+
+int gpu_batch_autotune(void* batch, int rounds) {
+    if (!batch || rounds < 0) return -1;
+    Batch& b = *static_cast<Batch*>(batch);
+    try {
+        Context& c = *b.c;
+        cudaSetDevice(c.device);
+        for (int r = 0; r < rounds && b.st.nPlans; ++r) {
+            b.st.enqueue(c, b.stream, true);
+            std::vector<unsigned long long> ns(2 * (size_t)b.st.nTasks);
+            ck(cudaMemcpyAsync(ns.data(), b.st.dTaskNs.p, ns.size() * 8, cudaMemcpyDeviceToHost, b.stream), "D2H task times");
+            ck(cudaStreamSynchronize(b.stream), "autotune");
+            c.tasks->learn(b.phases, b.st.hTasks, b.st.hCost, ns.data(), c.grid);
+            if (b.exec) { cudaGraphExecDestroy(b.exec); b.exec = nullptr; }
+            if (b.graph) { cudaGraphDestroy(b.graph); b.graph = nullptr; }
+            std::vector<DevPlan> pl = b.plans0;
+            b.st.stage(c, pl, b.phases, true, b.stream);
+            ck(cudaStreamSynchronize(b.stream), "restage");
+        }
+        return 0;
+    } catch (const std::exception& e) {
+        set_error(std::string("gpu_batch_autotune error: ") + e.what());
+        return -1;
+    }
+}
+
+int gpu_set_option(void* ctx, const char* name, long long value) {
+    if (!ctx || !name) return -1;
+    Context& c = *as_ctx(ctx);
+    std::string n(name);
+    if (n == "block") return c.set_block((int)value) ? 0 : -1;
+    if (n == "task_target" && value >= 0) { c.tasks->forceTarget = (double)value; return 0; }
+    if (n == "walk_threshold" && value >= 0) { c.tasks->walkThreshold = (double)value; return 0; }
+    return -1;
 }
 
 void gpu_batch_free(void* batch) {
@@ -639,8 +732,9 @@ size_t align256(size_t x) { return (x + 255) & ~size_t(255); }
 
 int64_t run_phase_noalloc(Context& c, const PhasePlan& ph, char* scratch, float* ms) {
     DevPlan plan = ph.plan;
-    std::vector<DevTask> tasks;
-    make_tasks(ph, 0, c.hix, tasks, nullptr);
+    std::vector<PhaseTasks> pts;
+    c.tasks->build({&ph}, c.grid, false, pts);
+    std::vector<DevTask>& tasks = pts[0].tasks;
     const size_t planOff = kNoAllocHeader;
     const size_t taskOff = align256(planOff + sizeof(DevPlan));
     const size_t bitmapOff = align256(taskOff + tasks.size() * sizeof(DevTask));
@@ -666,7 +760,7 @@ int64_t run_phase_noalloc(Context& c, const PhasePlan& ph, char* scratch, float*
     int grid = std::max(1, std::min((int)tasks.size(), c.grid));
     ck(engine_launch(c.dix, reinterpret_cast<const DevPlan*>(scratch + planOff),
                      reinterpret_cast<const DevTask*>(scratch + taskOff), (int)tasks.size(), ctl, result, ctl + 1,
-                     grid, c.stream, nullptr), "engine launch");
+                     grid, c.geom.block, c.stream, nullptr), "engine launch");
     ck(cudaEventRecord(c.ev[3], c.stream), "event");
     unsigned long long count = 0;
     int st[2] = {0, 0};
@@ -689,7 +783,7 @@ extern "C" int gpu_evaluate_rule_noalloc(void* ctx, const char* ruleText, GpuRul
         ck(cudaSetDevice(c.device), "cudaSetDevice");
         char* scratch = static_cast<char*>(noalloc_scratch(c.device));
         Rule r = c.parser->parse_text(ruleText);
-        RulePlan rp = plan_rule(r, c.hix);
+        RulePlan rp = plan_rule(r, c.hix, c.geom);
         int64_t sup = rp.support.value, body = rp.body.value;
         float supMs = 0.f, confMs = 0.f;
         if (rp.status == kRuleOk && rp.support.how == kDevice) sup = run_phase_noalloc(c, rp.support, scratch, &supMs);

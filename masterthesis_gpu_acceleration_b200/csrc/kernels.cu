@@ -4,13 +4,14 @@
 // tasks (a plan and a range of roots) from a device queue.  A task is
 // evaluated as a depth-first search over *chunks*: the block keeps, for each
 // plan level, a bounded frontier of partial bindings in shared memory and
-// always extends the deepest level that still has work.  Extending a level
-// lays the neighbour lists of up to kBlock frontier items end to end (one
-// hash lookup per item, a block-wide prefix sum) and hands the resulting
-// candidates to threads one per slot, so a hub with 50,000 neighbours is
-// spread over the whole block instead of serialising one thread.  Frontier
-// memory is bounded by construction (each round produces at most `cap`
-// items), so any fan-out fits.
+// always extends the deepest level that still has work.  Each frontier item
+// carries the neighbour segment of its next step (looked up once, when the
+// item is created).  Extending a level lays the segments of up to B items end
+// to end (a block-wide prefix sum) and hands the resulting candidates to
+// threads one per slot, so a hub with 50,000 neighbours is spread over the
+// whole block instead of serialising one thread.  Frontier memory is bounded
+// by construction (each round produces at most `cap` items), so any fan-out
+// fits.
 //
 // Outputs:
 //  * kExist: roots with at least one complete grounding (a bit per root);
@@ -25,6 +26,10 @@
 //    is dropped, which is the reference's early prune
 //    (CPU_01_nonparallel/SupportCounting.cpp:284-290).
 //
+// Block sizes 128, 256 and 512 are instantiated; shared memory scales with
+// the block (16 ints of frontier and 32 bitmap words per thread), so 8, 4 or
+// 2 blocks stay resident per SM.
+//
 // The reference's kernels (GPU_03/gpu_kernels.cuh:34-443) run one thread
 // per head triple or per first-atom triple with template-unrolled
 // recursion; this engine replaces them as a whole.
@@ -36,8 +41,6 @@
 
 namespace gr {
 
-constexpr int kWarps = kBlock / 32;
-
 // Counts the global-memory bytes the algorithm requests (the roofline's
 // algorithmic bytes).  Compiled out of the timed kernel.
 template <bool kOn>
@@ -47,9 +50,10 @@ struct Meter {
         if constexpr (kOn) bytes += n;
     }
 };
-constexpr int kLeafChunk = 4 * kBlock;
 
+template <int B>
 struct BlockState {
+    static constexpr int kWarps = B / 32;
     int task;
     int k;
     int curItem[kMaxBody + 1];
@@ -60,14 +64,15 @@ struct BlockState {
     unsigned long long red[kWarps];
 };
 
+template <int B>
 struct Smem {
     DevPlan plan;
-    BlockState st;
-    int wBeg[kBlock];
-    long long wLen[kBlock];
-    long long wPre[kBlock];
-    int items[kItemInts];
-    uint32_t bitmap[kBitmapWords];
+    BlockState<B> st;
+    int wBeg[B];
+    long long wLen[B];
+    long long wPre[B];
+    int items[Geom::items_for(B)];
+    uint32_t bitmap[Geom::words_for(B)];
 };
 
 template <bool kC>
@@ -115,8 +120,19 @@ __device__ __forceinline__ bool pass_filters(const DevPlan& P, const DevIndex& i
     return true;
 }
 
+// Edge range of step `s` (0-based) for a binding resolved by `val`.
+template <bool kC, class Val>
+__device__ __forceinline__ int2 step_segment(const DevPlan& P, const DevIndex& ix, int s, Meter<kC>& mt, Val val) {
+    const DevStep& st = P.steps[s];
+    if (st.kind == kExpand) return row_lookup(ix, st.pred, st.dir, val(st.keyRef), mt);
+    mt.add(8);
+    return make_int2(__ldg(ix.predEdge[0] + st.pred), __ldg(ix.predEdge[0] + st.pred + 1));
+}
+
 // Inclusive block scan of one 64-bit value per thread.
-__device__ __forceinline__ long long block_scan(long long x, BlockState& st) {
+template <int B>
+__device__ __forceinline__ long long block_scan(long long x, BlockState<B>& st) {
+    constexpr int kWarps = B / 32;
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
 #pragma unroll
     for (int d = 1; d < 32; d <<= 1) {
@@ -138,7 +154,9 @@ __device__ __forceinline__ long long block_scan(long long x, BlockState& st) {
     return warp ? x + st.warpSum[warp - 1] : x;
 }
 
-__device__ __forceinline__ unsigned long long block_sum(unsigned long long x, BlockState& st) {
+template <int B>
+__device__ __forceinline__ unsigned long long block_sum(unsigned long long x, BlockState<B>& st) {
+    constexpr int kWarps = B / 32;
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
 #pragma unroll
     for (int d = 16; d; d >>= 1) x += __shfl_down_sync(0xffffffffu, x, d);
@@ -150,21 +168,28 @@ __device__ __forceinline__ unsigned long long block_sum(unsigned long long x, Bl
     return t;  // valid in thread 0
 }
 
-template <bool kC>
-__device__ __forceinline__ void run_task(Smem& sm, const DevIndex& ix, const DevTask& task,
+template <int B, bool kC>
+__device__ __forceinline__ void run_task(Smem<B>& sm, const DevIndex& ix, const DevTask& task,
                                          unsigned long long* results, int* status, Meter<kC>& mt) {
+    constexpr int kLeafChunk = 8 * B;
     const DevPlan& P = sm.plan;
-    BlockState& S = sm.st;
+    BlockState<B>& S = sm.st;
     const int tid = threadIdx.x;
     const int G = task.end - task.beg;
     const bool pairs = P.mode == kPairs;
-    const bool shared = !(pairs && P.gBitmap);
-    uint32_t* bm = shared ? sm.bitmap : P.gBitmap;
-    const long long rowBase = shared ? 0 : (long long)task.beg - P.gRowBase;
+    // Dedup targets.  A split heavy root (one root, G == 1) uses its global
+    // row for both the pair bits and the found bit; counting happens on
+    // insertion so that the slices of one root count each result once.
+    const bool heavy = task.gRow >= 0;
+    const bool shared = !heavy && !(pairs && P.gBitmap);
+    uint32_t* bm = heavy ? P.gHeavy + (long long)task.gRow * P.rowWords : (shared ? sm.bitmap : P.gBitmap);
+    uint32_t* fb = heavy ? bm : sm.bitmap;   // kExist found bits
+    const long long rowBase = (heavy || shared) ? 0 : (long long)task.beg - P.gRowBase;
 
-    // clear the task's dedup bits
-    const int nWords = shared ? (int)(pairs ? (((long long)G * P.wo + 31) >> 5) : ((G + 31) >> 5)) : 0;
-    for (int i = tid; i < nWords; i += kBlock) sm.bitmap[i] = 0u;
+    // clear the task's shared dedup bits
+    const int nWords = heavy ? 0 : (shared ? (int)(pairs ? (((long long)G * P.wo + 31) >> 5) : ((G + 31) >> 5))
+                                           : (pairs ? 0 : ((G + 31) >> 5)));
+    for (int i = tid; i < nWords; i += B) sm.bitmap[i] = 0u;
     if (tid == 0) {
         S.k = 0;
         int off = 0;
@@ -173,15 +198,17 @@ __device__ __forceinline__ void run_task(Smem& sm, const DevIndex& ix, const Dev
             S.curOff[l] = 0;
             S.count[l] = 0;
             S.levelOff[l] = off;
-            if (l < P.m || (P.m == 0 && l == 0)) off += P.cap * P.tupleLen[l];
+            if (l < P.m) off += P.cap * (P.tupleLen[l] + 2);
+            else if (P.m == 0 && l == 0) off += P.cap * P.tupleLen[0];
         }
     }
     __syncthreads();
 
-    // ---- level 0: roots ----
+    // ---- level 0: roots (tuple, then the segment of step 1) ----
     {
         const int len0 = P.tupleLen[0];
-        for (int i = tid; i < G; i += kBlock) {
+        const int stride0 = P.m > 0 ? len0 + 2 : len0;
+        for (int i = tid; i < G; i += B) {
             const int r = task.beg + i;
             int tv[kTupleHead + 2];
             tv[0] = i;
@@ -202,16 +229,24 @@ __device__ __forceinline__ void run_task(Smem& sm, const DevIndex& ix, const Dev
                 if (P.rootAppendVal) tv[nv++] = v;
             }
             if (ok && nv != len0) { ok = false; atomicOr(status, 2); }
-            if (ok) {
-                ok = pass_filters(P, ix, 0, mt, [&](TermRef ref) -> int {
-                    return ref < 0 ? P.consts[-1 - ref] : tv[ref < nv ? ref : 0];
-                });
+            auto val0 = [&](TermRef ref) -> int { return ref < 0 ? P.consts[-1 - ref] : tv[ref < nv ? ref : 0]; };
+            if (ok) ok = pass_filters(P, ix, 0, mt, val0);
+            int2 seg = make_int2(0, 0);
+            if (ok && P.m > 0) {
+                seg = step_segment(P, ix, 0, mt, val0);
+                if (heavy) {
+                    const int b0 = seg.x;
+                    seg.x = min(seg.y, b0 + task.sub0);
+                    seg.y = min(seg.y, b0 + task.sub1);
+                }
+                ok = seg.y > seg.x;
             }
             if (ok) {
                 const int slot = atomicAdd(&S.count[0], 1);
                 if (slot < P.cap) {
-                    int* dst = sm.items + S.levelOff[0] + slot * len0;
+                    int* dst = sm.items + S.levelOff[0] + slot * stride0;
                     for (int q = 0; q < len0; ++q) dst[q] = tv[q];
+                    if (P.m > 0) { dst[len0] = seg.x; dst[len0 + 1] = seg.y - seg.x; }
                 } else {
                     atomicOr(status, 4);
                 }
@@ -222,9 +257,10 @@ __device__ __forceinline__ void run_task(Smem& sm, const DevIndex& ix, const Dev
 
     unsigned long long myNew = 0;
     if (P.m == 0) {
-        for (int i = tid; i < S.count[0] && i < P.cap; i += kBlock) {
+        for (int i = tid; i < S.count[0] && i < P.cap; i += B) {
             const int root = sm.items[S.levelOff[0] + i * P.tupleLen[0]];
-            atomicOr(&sm.bitmap[root >> 5], 1u << (root & 31));
+            const uint32_t old = atomicOr(&fb[root >> 5], 1u << (root & 31));
+            if (heavy && !(old & (1u << (root & 31)))) myNew++;
         }
     } else {
         for (;;) {
@@ -238,37 +274,31 @@ __device__ __forceinline__ void run_task(Smem& sm, const DevIndex& ix, const Dev
                 if (tid == 0) S.k = k - 1;
                 continue;
             }
-            const int nw = min(kBlock, cnt - w0);
+            const int nw = min(B, cnt - w0);
             const int lenK = P.tupleLen[k];
+            const int strideK = lenK + 2;
             const int* baseK = sm.items + S.levelOff[k];
             const DevStep& stp = P.steps[k];
             const bool leaf = (k + 1 == P.m);
             const bool itemHasRank = pairs && P.hoLevel >= 1 && k >= P.hoLevel;
 
-            // window: the neighbour segment of each item
+            // window: the stored neighbour segment of each item
             int myBeg = 0;
             long long myLen = 0;
             if (tid < nw) {
-                const int* it = baseK + (w0 + tid) * lenK;
+                const int* it = baseK + (w0 + tid) * strideK;
                 bool pruned = false;
                 if (!pairs) {
-                    pruned = (sm.bitmap[it[0] >> 5] >> (it[0] & 31)) & 1u;
+                    pruned = (fb[it[0] >> 5] >> (it[0] & 31)) & 1u;
+                    if (heavy) mt.add(4);
                 } else if (itemHasRank) {
                     const long long bit = (rowBase + it[0]) * (long long)P.wo + it[1];
                     pruned = (bm[bit >> 5] >> (bit & 31)) & 1u;
                     if (!shared) mt.add(4);
                 }
                 if (!pruned) {
-                    if (stp.kind == kExpand) {
-                        const int key = stp.keyRef < 0 ? P.consts[-1 - stp.keyRef] : it[stp.keyRef];
-                        const int2 r = row_lookup(ix, stp.pred, stp.dir, key, mt);
-                        myBeg = r.x;
-                        myLen = r.y - r.x;
-                    } else {
-                        myBeg = __ldg(ix.predEdge[0] + stp.pred);
-                        myLen = __ldg(ix.predEdge[0] + stp.pred + 1) - myBeg;
-                        mt.add(8);
-                    }
+                    myBeg = it[lenK];
+                    myLen = it[lenK + 1];
                     if (tid == 0) {
                         const long long off = S.curOff[k];
                         myBeg += (int)off;
@@ -279,15 +309,16 @@ __device__ __forceinline__ void run_task(Smem& sm, const DevIndex& ix, const Dev
             sm.wBeg[tid] = myBeg;
             sm.wLen[tid] = myLen;
             if (tid == 0 && !leaf) S.count[k + 1] = 0;
-            const long long pre = block_scan(myLen, S);
+            const long long pre = block_scan<B>(myLen, S);
             sm.wPre[tid] = pre;
             __syncthreads();
             const long long total = sm.wPre[nw - 1];
             const long long take = min(total, (long long)(leaf ? kLeafChunk : P.cap));
             const int lenN = leaf ? 0 : P.tupleLen[k + 1];
+            const int strideN = lenN + 2;
             int* baseN = leaf ? nullptr : sm.items + S.levelOff[k + 1];
 
-            for (long long j = tid; j < take; j += kBlock) {
+            for (long long j = tid; j < take; j += B) {
                 int lo = 0, hi = nw - 1;
                 while (lo < hi) {
                     const int mid = (lo + hi) >> 1;
@@ -295,9 +326,9 @@ __device__ __forceinline__ void run_task(Smem& sm, const DevIndex& ix, const Dev
                 }
                 const long long start = sm.wPre[lo] - sm.wLen[lo];
                 const int e = sm.wBeg[lo] + (int)(j - start);
-                const int* par = baseK + (w0 + lo) * lenK;
+                const int* par = baseK + (w0 + lo) * strideK;
                 const int root = par[0];
-                if (!pairs && ((sm.bitmap[root >> 5] >> (root & 31)) & 1u)) continue;
+                if (!pairs && ((fb[root >> 5] >> (root & 31)) & 1u)) continue;
                 int n0, n1 = 0;
                 if (stp.kind == kExpand) {
                     n0 = __ldg(ix.val[stp.dir] + e);
@@ -314,12 +345,12 @@ __device__ __forceinline__ void run_task(Smem& sm, const DevIndex& ix, const Dev
                     if (x == n0 || (stp.nNew == 2 && x == n1)) { ok = false; break; }
                 }
                 if (!ok) continue;
-                ok = pass_filters(P, ix, k + 1, mt, [&](TermRef ref) -> int {
+                auto valN = [&](TermRef ref) -> int {
                     if (ref < 0) return P.consts[-1 - ref];
                     if (ref < lenK) return par[ref];
                     return ref == lenK ? n0 : n1;
-                });
-                if (!ok) continue;
+                };
+                if (!pass_filters(P, ix, k + 1, mt, valN)) continue;
                 int rank = par[1];
                 if (pairs && stp.hoWhich) {
                     if (stp.kind == kExpand) rank = __ldg(ix.valRank[stp.dir] + e);
@@ -333,7 +364,9 @@ __device__ __forceinline__ void run_task(Smem& sm, const DevIndex& ix, const Dev
                 }
                 if (leaf) {
                     if (!pairs) {
-                        atomicOr(&sm.bitmap[root >> 5], 1u << (root & 31));
+                        const uint32_t mask = 1u << (root & 31);
+                        const uint32_t old = atomicOr(&fb[root >> 5], mask);
+                        if (heavy) { mt.add(8); myNew += (old & mask) ? 0ull : 1ull; }
                     } else {
                         const long long bit = (rowBase + root) * (long long)P.wo + rank;
                         const uint32_t mask = 1u << (bit & 31);
@@ -342,14 +375,18 @@ __device__ __forceinline__ void run_task(Smem& sm, const DevIndex& ix, const Dev
                         myNew += (old & mask) ? 0ull : 1ull;
                     }
                 } else {
+                    const int2 seg = step_segment(P, ix, k + 1, mt, valN);
+                    if (seg.y <= seg.x) continue;
                     const int slot = atomicAdd(&S.count[k + 1], 1);
                     if (slot >= P.cap) { atomicOr(status, 8); continue; }
-                    int* dst = baseN + slot * lenN;
+                    int* dst = baseN + slot * strideN;
                     dst[0] = root;
                     dst[1] = rank;
                     for (int q = kTupleHead; q < lenK; ++q) dst[q] = par[q];
                     dst[lenK] = n0;
                     if (stp.nNew == 2) dst[lenK + 1] = n1;
+                    dst[lenN] = seg.x;
+                    dst[lenN + 1] = seg.y - seg.x;
                 }
             }
             __syncthreads();
@@ -380,23 +417,28 @@ __device__ __forceinline__ void run_task(Smem& sm, const DevIndex& ix, const Dev
 
     // ---- result ----
     unsigned long long mine = 0;
-    if (!pairs) {
-        for (int i = tid; i < ((G + 31) >> 5); i += kBlock) mine += __popc(sm.bitmap[i]);
+    if (!pairs && !heavy) {
+        for (int i = tid; i < ((G + 31) >> 5); i += B) mine += __popc(sm.bitmap[i]);
     } else {
         mine = myNew;
     }
-    const unsigned long long tot = block_sum(mine, S);
+    const unsigned long long tot = block_sum<B>(mine, S);
     if (tid == 0 && tot) atomicAdd(results + P.resultSlot, tot);
     if (tid == 0) mt.add(8);
 }
 
-template <bool kC>
-__global__ void __launch_bounds__(kBlock, 2)
+__device__ __forceinline__ unsigned long long global_ns() {
+    unsigned long long t;
+    asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+    return t;
+}
+
+template <int B, bool kC>
+__global__ void __launch_bounds__(B, 1024 / B)
 engine_kernel(DevIndex ix, const DevPlan* __restrict__ plans, const DevTask* __restrict__ tasks,
-              int nTasks, int* taskCounter, unsigned long long* results, int* status,
-              unsigned long long* bytesOut) {
+              int nTasks, int* taskCounter, unsigned long long* results, int* status, EngineProfile prof) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
-    Smem& sm = *reinterpret_cast<Smem*>(smem_raw);
+    Smem<B>& sm = *reinterpret_cast<Smem<B>*>(smem_raw);
     Meter<kC> mt;
     for (;;) {
         if (threadIdx.x == 0) sm.st.task = atomicAdd(taskCounter, 1);
@@ -404,40 +446,80 @@ engine_kernel(DevIndex ix, const DevPlan* __restrict__ plans, const DevTask* __r
         const int t = sm.st.task;
         if (t >= nTasks) break;
         const DevTask task = tasks[t];
-        if (threadIdx.x == 0) mt.add(sizeof(DevTask) + sizeof(DevPlan) + 8);
+        unsigned long long t0 = 0;
+        if constexpr (kC) {
+            if (threadIdx.x == 0) {
+                mt.add(sizeof(DevTask) + sizeof(DevPlan) + 8);
+                t0 = global_ns();
+            }
+        }
         const int* src = reinterpret_cast<const int*>(plans + task.plan);
         int* dst = reinterpret_cast<int*>(&sm.plan);
-        for (int i = threadIdx.x; i < (int)(sizeof(DevPlan) / 4); i += kBlock) dst[i] = src[i];
+        for (int i = threadIdx.x; i < (int)(sizeof(DevPlan) / 4); i += B) dst[i] = src[i];
         __syncthreads();
-        run_task(sm, ix, task, results, status, mt);
+        run_task<B, kC>(sm, ix, task, results, status, mt);
         __syncthreads();
+        if constexpr (kC) {
+            if (threadIdx.x == 0 && prof.taskNs) {
+                prof.taskNs[2 * t] = t0;
+                prof.taskNs[2 * t + 1] = global_ns();
+            }
+        }
     }
     if constexpr (kC) {
         unsigned long long b = mt.bytes;
         for (int d = 16; d; d >>= 1) b += __shfl_down_sync(0xffffffffu, b, d);
-        if ((threadIdx.x & 31) == 0 && b) atomicAdd(bytesOut, b);
+        if ((threadIdx.x & 31) == 0 && b && prof.bytes) atomicAdd(prof.bytes, b);
     }
 }
 
-size_t engine_smem_bytes() { return sizeof(Smem); }
-
-cudaError_t engine_configure() {
-    cudaError_t e = cudaFuncSetAttribute(engine_kernel<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sizeof(Smem));
+template <int B>
+static cudaError_t configure_b() {
+    cudaError_t e = cudaFuncSetAttribute(engine_kernel<B, false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                         (int)sizeof(Smem<B>));
     if (e != cudaSuccess) return e;
-    return cudaFuncSetAttribute(engine_kernel<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sizeof(Smem));
+    return cudaFuncSetAttribute(engine_kernel<B, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                (int)sizeof(Smem<B>));
 }
 
-// bytesOut != null selects the byte-counting variant.
-cudaError_t engine_launch(const DevIndex& ix, const DevPlan* plans, const DevTask* tasks, int nTasks,
-                          int* taskCounter, unsigned long long* results, int* status, int grid,
-                          cudaStream_t stream, unsigned long long* bytesOut) {
-    if (nTasks <= 0) return cudaSuccess;
-    if (bytesOut)
-        engine_kernel<true><<<grid, kBlock, sizeof(Smem), stream>>>(ix, plans, tasks, nTasks, taskCounter, results,
-                                                                    status, bytesOut);
+size_t engine_smem_bytes(int block) {
+    switch (block) {
+        case 128: return sizeof(Smem<128>);
+        case 256: return sizeof(Smem<256>);
+        default: return sizeof(Smem<512>);
+    }
+}
+
+cudaError_t engine_configure() {
+    cudaError_t e = configure_b<128>();
+    if (e == cudaSuccess) e = configure_b<256>();
+    if (e == cudaSuccess) e = configure_b<512>();
+    return e;
+}
+
+template <int B>
+static void launch_b(const DevIndex& ix, const DevPlan* plans, const DevTask* tasks, int nTasks, int* taskCounter,
+                     unsigned long long* results, int* status, int grid, cudaStream_t stream,
+                     const EngineProfile* prof) {
+    if (prof)
+        engine_kernel<B, true><<<grid, B, sizeof(Smem<B>), stream>>>(ix, plans, tasks, nTasks, taskCounter, results,
+                                                                     status, *prof);
     else
-        engine_kernel<false><<<grid, kBlock, sizeof(Smem), stream>>>(ix, plans, tasks, nTasks, taskCounter, results,
-                                                                     status, nullptr);
+        engine_kernel<B, false><<<grid, B, sizeof(Smem<B>), stream>>>(ix, plans, tasks, nTasks, taskCounter, results,
+                                                                      status, EngineProfile{});
+}
+
+// prof != null selects the profiling variant (byte counts, task times).
+cudaError_t engine_launch(const DevIndex& ix, const DevPlan* plans, const DevTask* tasks, int nTasks,
+                          int* taskCounter, unsigned long long* results, int* status, int grid, int block,
+                          cudaStream_t stream, const EngineProfile* prof) {
+    if (nTasks <= 0) return cudaSuccess;
+    switch (block) {
+        case 128: launch_b<128>(ix, plans, tasks, nTasks, taskCounter, results, status, grid, stream, prof); break;
+        case 256: launch_b<256>(ix, plans, tasks, nTasks, taskCounter, results, status, grid, stream, prof); break;
+        case 512: launch_b<512>(ix, plans, tasks, nTasks, taskCounter, results, status, grid, stream, prof); break;
+        default: return cudaErrorInvalidValue;
+    }
     return cudaGetLastError();
 }
 

@@ -188,22 +188,25 @@ bool build_steps(Builder& b, const std::vector<Atom>& body, const Atom* head, in
     return true;
 }
 
-void finish_capacity(DevPlan& P) {
+// Frontier capacity per level: levels 0..m-1 each hold `cap` items of
+// (tuple + stored segment) ints; the roots of one task must fit level 0 and,
+// for kPairs, their bitmap rows must fit the block's bitmap.
+void finish_capacity(DevPlan& P, const Geom& geom) {
     int sum = 0;
     if (P.m == 0) sum = P.tupleLen[0];
-    for (int l = 0; l < P.m; ++l) sum += P.tupleLen[l];
-    int cap = (kItemInts / std::max(sum, 1)) & ~31;
+    for (int l = 0; l < P.m; ++l) sum += P.tupleLen[l] + 2;
+    int cap = (geom.itemInts() / std::max(sum, 1)) & ~31;
     P.cap = std::max(cap, 32);
     P.groupMax = P.cap;
     if (P.mode == kPairs && P.wo > 0) {
-        int64_t g = (int64_t)kBitmapWords * 32 / P.wo;
+        int64_t g = (int64_t)geom.bitmapWords() * 32 / P.wo;
         P.groupMax = (int32_t)std::min<int64_t>(P.groupMax, g);
     }
 }
 
 }  // namespace
 
-RulePlan plan_rule(const Rule& rule, const HostIndex& ix) {
+RulePlan plan_rule(const Rule& rule, const HostIndex& ix, const Geom& geom) {
     RulePlan rp;
     const Atom& h = rule.head;
     int nb = (int)rule.body.size();
@@ -277,7 +280,7 @@ RulePlan plan_rule(const Rule& rule, const HostIndex& ix) {
                 P.rootValConst = b.ref(h.o);
             }
             if (build_steps(b, rule.body, &h, -1, false) && b.ok) {
-                finish_capacity(P);
+                finish_capacity(P, geom);
                 S.how = kDevice;
                 S.rootBeg = range.first;
                 S.rootEnd = range.second;
@@ -324,11 +327,11 @@ RulePlan plan_rule(const Rule& rule, const HostIndex& ix) {
                         else P.wo = (int32_t)ix.pred_rows(st.pred, st.hoWhich == 1 ? 0 : 1);
                     }
                 }
-                finish_capacity(P);
+                finish_capacity(P, geom);
                 B.how = kDevice;
                 B.rootBeg = ix.predRow[seedDir][seedPred];
                 B.rootEnd = ix.predRow[seedDir][seedPred + 1];
-                B.needsGlobalBitmap = pairs && (int64_t)P.wo > (int64_t)kBitmapWords * 32;
+                B.needsGlobalBitmap = pairs && (int64_t)P.wo > (int64_t)geom.bitmapWords() * 32;
                 B.estCost = (double)(ix.predEdge[seedDir][seedPred + 1] - ix.predEdge[seedDir][seedPred]);
             } else if (!b.ok) {
                 rp.status = kRuleUnsupported;
@@ -341,34 +344,6 @@ RulePlan plan_rule(const Rule& rule, const HostIndex& ix) {
         rp.headSupport = rp.headSize;
     }
     return rp;
-}
-
-void make_tasks(const PhasePlan& ph, int32_t planIdx, const HostIndex& ix,
-                std::vector<DevTask>& out, std::vector<double>* cost) {
-    const DevPlan& P = ph.plan;
-    int32_t g = std::max(P.groupMax, 1);
-    if (ph.needsGlobalBitmap) g = std::min(P.cap, 512);
-    const int64_t kMaxRowWork = 1 << 14;
-    int32_t r = ph.rootBeg;
-    while (r < ph.rootEnd) {
-        int32_t e = r;
-        int64_t work = 0;
-        if (P.rootKind == kRootRows) {
-            const auto& rb = ix.rowBeg[P.rootDir];
-            while (e < ph.rootEnd && e - r < g) {
-                int64_t w = 1 + (rb[e + 1] - rb[e]);
-                if (e > r && work + w > kMaxRowWork) break;
-                work += w;
-                ++e;
-            }
-        } else {
-            e = std::min<int32_t>(ph.rootEnd, r + g);
-            work = e - r;
-        }
-        out.push_back(DevTask{planIdx, r, e, 0});
-        if (cost) cost->push_back((double)work);
-        r = e;
-    }
 }
 
 }  // namespace gr

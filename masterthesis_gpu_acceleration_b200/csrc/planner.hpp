@@ -38,10 +38,6 @@ struct RulePlan {
 // Plans both phases.  Semantics follow CPU_01_nonparallel/SupportCounting.cpp:
 // support (474-552) with the head triple counted as used, body size
 // (563-631) with the seed atom's keys as headS candidates.
-RulePlan plan_rule(const Rule& rule, const HostIndex& ix);
-
-// Splits a device phase into root-range tasks for plan number `planIdx`.
-void make_tasks(const PhasePlan& ph, int32_t planIdx, const HostIndex& ix,
-                std::vector<DevTask>& out, std::vector<double>* cost = nullptr);
+RulePlan plan_rule(const Rule& rule, const HostIndex& ix, const Geom& geom);
 
 }  // namespace gr

@@ -1,0 +1,283 @@
+// tasks.cpp — balanced task construction (see tasks.hpp).
+#include "tasks.hpp"
+
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+#include <numeric>
+
+namespace gr {
+namespace {
+
+constexpr double kMinTarget = 4096.0;
+constexpr double kWalkBudget = 4.0e7;     // first-segment edges walked per batch
+constexpr size_t kCacheLimit = 256u << 20;
+
+int64_t pd_key(int32_t pred, int dir) { return (int64_t)pred * 2 + dir; }
+
+std::string signature(const PhasePlan& ph) {
+    DevPlan p = ph.plan;
+    p.resultSlot = 0;
+    p.gBitmap = nullptr;
+    p.gRowBase = 0;
+    p.gHeavy = nullptr;
+    p.rowWords = 0;
+    std::string s(reinterpret_cast<const char*>(&p), sizeof(p));
+    s.append(reinterpret_cast<const char*>(&ph.rootBeg), sizeof(ph.rootBeg));
+    s.append(reinterpret_cast<const char*>(&ph.rootEnd), sizeof(ph.rootEnd));
+    return s;
+}
+
+}  // namespace
+
+const int32_t* TaskBuilder::degrees(int32_t pred, int dir) {
+    auto it = deg_.find(pd_key(pred, dir));
+    if (it != deg_.end()) return it->second.data();
+    std::vector<int32_t> d((size_t)std::max(ix_.nEnt, 1), 0);
+    for (int32_t r = ix_.predRow[dir][pred]; r < ix_.predRow[dir][pred + 1]; ++r)
+        d[ix_.rowKey[dir][r]] = ix_.rowBeg[dir][r + 1] - ix_.rowBeg[dir][r];
+    cacheBytes_ += d.size() * 4;
+    return deg_.emplace(pd_key(pred, dir), std::move(d)).first->second.data();
+}
+
+double TaskBuilder::sb_fan(int32_t pred, int dir) {
+    auto it = sbFan_.find(pd_key(pred, dir));
+    if (it != sbFan_.end()) return it->second;
+    double s1 = 0, s2 = 0;
+    for (int32_t r = ix_.predRow[dir][pred]; r < ix_.predRow[dir][pred + 1]; ++r) {
+        double d = ix_.rowBeg[dir][r + 1] - ix_.rowBeg[dir][r];
+        s1 += d;
+        s2 += d * d;
+    }
+    double v = s1 > 0 ? s2 / s1 : 0.0;
+    sbFan_[pd_key(pred, dir)] = v;
+    return v;
+}
+
+double TaskBuilder::avg_fan(const DevStep& st) const {
+    if (st.kind == kScan) return (double)ix_.pred_size(st.pred);
+    return std::max(1.0, ix_.avg_degree(st.pred, st.dir));
+}
+
+double TaskBuilder::estimate(const PhasePlan& ph, bool hubAware) {
+    const DevPlan& P = ph.plan;
+    double w = std::max(1, ph.rootEnd - ph.rootBeg);
+    for (int s = 0; s < P.m; ++s) {
+        const DevStep& st = P.steps[s];
+        double f = avg_fan(st);
+        if (hubAware && st.kind == kExpand) f = std::max(f, sb_fan(st.pred, st.dir));
+        w *= std::max(1.0, f);
+        if (w > 1e18) return 1e18;
+    }
+    return w;
+}
+
+int TaskBuilder::root_vals(const DevPlan& P, int32_t r, int32_t* vals) const {
+    int nv = 0;
+    if (P.rootKind == kRootRows) {
+        vals[nv++] = ix_.rowKey[P.rootDir][r];
+    } else {
+        if (P.rootAppendKey) vals[nv++] = ix_.src[P.rootDir][r];
+        if (P.rootAppendVal) vals[nv++] = ix_.val[P.rootDir][r];
+    }
+    return nv;
+}
+
+static int32_t resolve(const DevPlan& P, TermRef ref, const int32_t* vals, int32_t n0, int32_t n1) {
+    if (ref < 0) return P.consts[-1 - ref];
+    if (ref < kTupleHead) return -1;
+    if (ref < P.tupleLen[0]) return vals[ref - kTupleHead];
+    return ref == P.tupleLen[0] ? n0 : n1;
+}
+
+std::pair<int32_t, int32_t> TaskBuilder::first_segment(const DevPlan& P, const int32_t* vals) const {
+    const DevStep& st = P.steps[0];
+    if (st.kind == kScan) return {ix_.predEdge[0][st.pred], ix_.predEdge[0][st.pred + 1]};
+    return ix_.row_range(st.pred, st.dir, resolve(P, st.keyRef, vals, -1, -1));
+}
+
+double TaskBuilder::child_work(const DevPlan& P, const int32_t* vals, int32_t e, const int32_t* deg2,
+                               double tail) const {
+    if (P.m < 2) return 1.0;
+    const DevStep& s0 = P.steps[0];
+    int32_t n0, n1 = -1;
+    if (s0.kind == kExpand) n0 = ix_.val[s0.dir][e];
+    else { n0 = ix_.src[0][e]; n1 = ix_.val[0][e]; }
+    const DevStep& s1 = P.steps[1];
+    double d2;
+    if (s1.kind == kScan) d2 = (double)ix_.pred_size(s1.pred);
+    else {
+        int32_t k = resolve(P, s1.keyRef, vals, n0, n1);
+        d2 = (k >= 0 && k < ix_.nEnt) ? deg2[k] : 0.0;
+    }
+    return 1.0 + d2 * tail;
+}
+
+const std::vector<float>& TaskBuilder::walk(const PhasePlan& ph) {
+    std::string sig = signature(ph);
+    auto it = walks_.find(sig);
+    if (it != walks_.end()) return it->second;
+    const DevPlan& P = ph.plan;
+    double tail = 1.0;
+    for (int s = 2; s < P.m; ++s) tail *= std::max(1.0, avg_fan(P.steps[s]));
+    const int32_t* deg2 = (P.m >= 2 && P.steps[1].kind == kExpand) ? degrees(P.steps[1].pred, P.steps[1].dir) : nullptr;
+    std::vector<float> w((size_t)(ph.rootEnd - ph.rootBeg));
+    int32_t vals[2];
+    for (int32_t r = ph.rootBeg; r < ph.rootEnd; ++r) {
+        root_vals(P, r, vals);
+        auto seg = first_segment(P, vals);
+        double acc = 1.0;
+        if (P.m < 2) acc += seg.second - seg.first;
+        else
+            for (int32_t e = seg.first; e < seg.second; ++e) acc += child_work(P, vals, e, deg2, tail);
+        w[r - ph.rootBeg] = (float)acc;
+    }
+    cacheBytes_ += w.size() * sizeof(float) + sig.size();
+    return walks_.emplace(std::move(sig), std::move(w)).first->second;
+}
+
+void TaskBuilder::build(const std::vector<const PhasePlan*>& phases, int blocks, bool split,
+                        std::vector<PhaseTasks>& out) {
+    size_t n = phases.size();
+    out.assign(n, PhaseTasks{});
+    if (cacheBytes_ > kCacheLimit) {  // only here: walks hand out references into the cache
+        walks_.clear();
+        deg_.clear();
+        cacheBytes_ = 0;
+    }
+    std::vector<double> estAvg(n), estHub(n), scale(n, defaultCalib_);
+    std::vector<const std::vector<float>*> walked(n, nullptr);
+    std::vector<char> forced(n, 0);
+    for (size_t i = 0; i < n; ++i) {
+        estAvg[i] = estimate(*phases[i], false);
+        estHub[i] = split ? estimate(*phases[i], true) : estAvg[i];
+        out[i].work = estAvg[i];
+        if (!calib_.empty() || !mustWalk_.empty()) {
+            std::string sig = signature(*phases[i]);
+            auto c = calib_.find(sig);
+            if (c != calib_.end()) scale[i] = c->second;
+            forced[i] = mustWalk_.count(sig) ? 1 : 0;
+        }
+    }
+    if (split) {
+        std::vector<size_t> ord(n);
+        std::iota(ord.begin(), ord.end(), 0);
+        // phases that ran slow before come first, then the hub-aware ranking
+        std::sort(ord.begin(), ord.end(), [&](size_t a, size_t b) {
+            if (forced[a] != forced[b]) return forced[a] > forced[b];
+            return estHub[a] > estHub[b];
+        });
+        double used = 0;
+        for (size_t i : ord) {
+            if (!forced[i] && estHub[i] < walkThreshold) break;
+            const PhasePlan& ph = *phases[i];
+            const DevStep& s0 = ph.plan.steps[0];
+            double edges = (double)(ph.rootEnd - ph.rootBeg) *
+                           (s0.kind == kExpand ? std::max(1.0, ix_.avg_degree(s0.pred, s0.dir)) : (double)ix_.pred_size(s0.pred));
+            if (!forced[i] && used + edges > kWalkBudget) continue;
+            used += edges;
+            walked[i] = &walk(ph);
+            double s = 0;
+            for (float x : *walked[i]) s += x;
+            out[i].work = s;
+        }
+    }
+    // work in device-time units (learned ns per unit, where known)
+    double total = 0;
+    for (size_t i = 0; i < n; ++i) total += out[i].work * scale[i];
+    const double target = forceTarget > 0 ? forceTarget
+                                          : std::max(kMinTarget * defaultCalib_, total / (std::max(blocks, 1) * 8.0));
+
+    for (size_t i = 0; i < n; ++i) {
+        const PhasePlan& ph = *phases[i];
+        const DevPlan& P = ph.plan;
+        PhaseTasks& pt = out[i];
+        const double sc = forceTarget > 0 ? 1.0 : scale[i];
+        pt.scale = scale[i];
+        int32_t g = std::max(P.groupMax, 1);
+        if (ph.needsGlobalBitmap) g = std::min(P.cap, 512);
+        const int32_t R = ph.rootEnd - ph.rootBeg;
+        const double uniform = R > 0 ? std::max(1.0, pt.work / R) : 1.0;
+        const std::vector<float>* w = walked[i];
+        int32_t gb = ph.rootBeg;
+        double acc = 0, accUnits = 0;
+        auto flush = [&](int32_t end) {
+            if (end > gb) {
+                pt.tasks.push_back(DevTask{(int32_t)i, gb, end, 0, 0, -1});
+                pt.cost.push_back(accUnits);
+            }
+            gb = end;
+            acc = 0;
+            accUnits = 0;
+        };
+        for (int32_t r = ph.rootBeg; r < ph.rootEnd; ++r) {
+            const double wu = w ? (double)(*w)[r - ph.rootBeg] : uniform;
+            const double wr = wu * sc;
+            if (split && w && wr > target && P.m >= 1) {
+                // a heavy root: slices of its first segment, one task each
+                flush(r);
+                int32_t vals[2];
+                root_vals(P, r, vals);
+                auto seg = first_segment(P, vals);
+                double tail = 1.0;
+                for (int s = 2; s < P.m; ++s) tail *= std::max(1.0, avg_fan(P.steps[s]));
+                const int32_t* deg2 =
+                    (P.m >= 2 && P.steps[1].kind == kExpand) ? degrees(P.steps[1].pred, P.steps[1].dir) : nullptr;
+                size_t first = pt.tasks.size();
+                int32_t s0 = 0;
+                double sa = 0;
+                for (int32_t e = seg.first; e < seg.second; ++e) {
+                    sa += child_work(P, vals, e, deg2, tail);
+                    if (sa * sc >= target || e + 1 == seg.second) {
+                        int32_t s1 = e + 1 - seg.first;
+                        pt.tasks.push_back(DevTask{(int32_t)i, r, r + 1, s0, s1, pt.heavyRows});
+                        pt.cost.push_back(sa);
+                        s0 = s1;
+                        sa = 0;
+                    }
+                }
+                if (pt.tasks.size() - first <= 1) {
+                    // not worth a global row: keep the root as a plain task
+                    if (pt.tasks.size() > first) { pt.tasks.pop_back(); pt.cost.pop_back(); }
+                    pt.tasks.push_back(DevTask{(int32_t)i, r, r + 1, 0, 0, -1});
+                    pt.cost.push_back(wu);
+                } else {
+                    pt.heavyRows++;
+                }
+                gb = r + 1;
+                continue;
+            }
+            if (r > gb && (r - gb >= g || acc + wr > target)) flush(r);
+            acc += wr;
+            accUnits += wu;
+        }
+        flush(ph.rootEnd);
+    }
+}
+
+void TaskBuilder::learn(const std::vector<const PhasePlan*>& phases, const std::vector<DevTask>& tasks,
+                        const std::vector<double>& cost, const unsigned long long* taskNs, int blocks) {
+    size_t n = phases.size();
+    std::vector<double> ns(n, 0.0), units(n, 0.0), worst(n, 0.0);
+    double totNs = 0, totUnits = 0;
+    for (size_t t = 0; t < tasks.size(); ++t) {
+        int p = tasks[t].plan;
+        if (p < 0 || (size_t)p >= n) continue;
+        double d = (double)(taskNs[2 * t + 1] - taskNs[2 * t]);
+        ns[p] += d;
+        units[p] += std::max(cost[t], 1.0);
+        worst[p] = std::max(worst[p], d);
+        totNs += d;
+        totUnits += std::max(cost[t], 1.0);
+    }
+    if (totUnits > 0) defaultCalib_ = totNs / totUnits;
+    const double limit = totNs / (std::max(blocks, 1) * 8.0);
+    for (size_t p = 0; p < n; ++p) {
+        if (units[p] <= 0) continue;
+        std::string sig = signature(*phases[p]);
+        calib_[sig] = ns[p] / units[p];
+        if (worst[p] > limit) mustWalk_[sig] = true;
+    }
+}
+
+}  // namespace gr

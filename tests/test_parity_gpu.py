@@ -159,3 +159,20 @@ def test_prepared_batch_replays_exactly(tmp_path):
                 assert ms >= 0
                 _check(res, fx["expected"], f"prepared run flush={flush}")
             assert b.count_bytes() > 0
+
+
+@pytest.mark.parametrize("name", ["fuzz_0.json", "fuzz_2.json", "fuzz_5.json"])
+@pytest.mark.parametrize("block", [128, 512])
+def test_fuzz_forced_splitting(name, block, tmp_path):
+    """Every root is measured and every root with more than a few candidates
+    is split into first-segment slices deduplicated in global rows."""
+    fx = load_fixture(name)
+    p = tmp_path / "graph.ttl"
+    p.write_text(fx["ttl"])
+    with eng.GpuRulesLib(p) as lib:
+        lib.set_option("block", block)
+        lib.set_option("walk_threshold", 0)
+        lib.set_option("task_target", 3)
+        res, st, _ = lib.evaluate_rules_batch(fx["rules"])
+        _check(res, fx["expected"], f"batch split block={block}")
+        _check([lib.evaluate_rule(t) for t in fx["rules"][:60]], fx["expected"][:60], "per-rule split")
