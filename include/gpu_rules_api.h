@@ -133,7 +133,7 @@ void gpu_batch_free(void* batch);
 int gpu_evaluate_rule_noalloc(void* ctx, const char* ruleText, GpuRuleResult* out);
 
 /* Engine option for later calls on this context.  "block": threads per
- * block of the engine kernel, 128, 256 or 512 (default 256; the environment
+ * block of the engine kernel, 128, 256 or 512 (default 512; the environment
  * variable GPU_RULES_BLOCK sets it at load).  "task_target": fixed work per
  * task in candidate bindings (0 = automatic balancing).  "walk_threshold":
  * estimated work above which a phase's roots are measured one by one before

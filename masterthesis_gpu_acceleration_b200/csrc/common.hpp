@@ -110,6 +110,7 @@ struct DevPlan {
     int8_t chkBeg[kMaxBody + 1], chkN[kMaxBody + 1];
     int8_t usedBeg[kMaxBody + 1], usedN[kMaxBody + 1];
     int32_t wo;              // kPairs: bitmap row width (size of hO's value domain)
+    int32_t bitmapOff;       // where the dedup bitmap starts in the block's shared pool (ints)
     int32_t hoLevel;         // kPairs: level whose step binds hO (1..m)
     int32_t cap;             // frontier capacity per level (items)
     int32_t groupMax;        // max roots per task
@@ -138,15 +139,13 @@ struct DevTask {
 };
 
 // Engine launch geometry: block size B (128, 256 or 512 threads) with a
-// shared-memory budget that scales with it, so 1024 / B blocks stay
-// resident per SM.  Frontier storage: 16 ints per thread; dedup bitmap:
-// 32 words (1024 bits) per thread.
+// shared-memory pool of 48 ints per thread that each plan splits between
+// its frontier levels and its dedup bitmap, so 1024 / B blocks stay
+// resident per SM.
 struct Geom {
-    int block = 256;
-    static constexpr int items_for(int b) { return 16 * b; }
-    static constexpr int words_for(int b) { return 32 * b; }
-    int itemInts() const { return items_for(block); }
-    int bitmapWords() const { return words_for(block); }
+    int block = 512;
+    static constexpr int pool_for(int b) { return 48 * b; }
+    int poolInts() const { return pool_for(block); }
 };
 
 // Profiling outputs of the instrumented kernel variant (null members are

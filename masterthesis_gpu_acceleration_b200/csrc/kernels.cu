@@ -71,8 +71,7 @@ struct Smem {
     int wBeg[B];
     long long wLen[B];
     long long wPre[B];
-    int items[Geom::items_for(B)];
-    uint32_t bitmap[Geom::words_for(B)];
+    int pool[Geom::pool_for(B)];   // frontier levels, then the dedup bitmap at plan.bitmapOff
 };
 
 template <bool kC>
@@ -171,7 +170,8 @@ __device__ __forceinline__ unsigned long long block_sum(unsigned long long x, Bl
 template <int B, bool kC>
 __device__ __forceinline__ void run_task(Smem<B>& sm, const DevIndex& ix, const DevTask& task,
                                          unsigned long long* results, int* status, Meter<kC>& mt) {
-    constexpr int kLeafChunk = 8 * B;
+    constexpr int kLeafChunk = 16 * B;
+    constexpr int kU = 4;
     const DevPlan& P = sm.plan;
     BlockState<B>& S = sm.st;
     const int tid = threadIdx.x;
@@ -182,14 +182,16 @@ __device__ __forceinline__ void run_task(Smem<B>& sm, const DevIndex& ix, const 
     // insertion so that the slices of one root count each result once.
     const bool heavy = task.gRow >= 0;
     const bool shared = !heavy && !(pairs && P.gBitmap);
-    uint32_t* bm = heavy ? P.gHeavy + (long long)task.gRow * P.rowWords : (shared ? sm.bitmap : P.gBitmap);
-    uint32_t* fb = heavy ? bm : sm.bitmap;   // kExist found bits
+    uint32_t* sbits = reinterpret_cast<uint32_t*>(sm.pool + P.bitmapOff);
+    int* const items = sm.pool;
+    uint32_t* bm = heavy ? P.gHeavy + (long long)task.gRow * P.rowWords : (shared ? sbits : P.gBitmap);
+    uint32_t* fb = heavy ? bm : sbits;   // kExist found bits
     const long long rowBase = (heavy || shared) ? 0 : (long long)task.beg - P.gRowBase;
 
     // clear the task's shared dedup bits
     const int nWords = heavy ? 0 : (shared ? (int)(pairs ? (((long long)G * P.wo + 31) >> 5) : ((G + 31) >> 5))
                                            : (pairs ? 0 : ((G + 31) >> 5)));
-    for (int i = tid; i < nWords; i += B) sm.bitmap[i] = 0u;
+    for (int i = tid; i < nWords; i += B) sbits[i] = 0u;
     if (tid == 0) {
         S.k = 0;
         int off = 0;
@@ -244,7 +246,7 @@ __device__ __forceinline__ void run_task(Smem<B>& sm, const DevIndex& ix, const 
             if (ok) {
                 const int slot = atomicAdd(&S.count[0], 1);
                 if (slot < P.cap) {
-                    int* dst = sm.items + S.levelOff[0] + slot * stride0;
+                    int* dst = items + S.levelOff[0] + slot * stride0;
                     for (int q = 0; q < len0; ++q) dst[q] = tv[q];
                     if (P.m > 0) { dst[len0] = seg.x; dst[len0 + 1] = seg.y - seg.x; }
                 } else {
@@ -258,7 +260,7 @@ __device__ __forceinline__ void run_task(Smem<B>& sm, const DevIndex& ix, const 
     unsigned long long myNew = 0;
     if (P.m == 0) {
         for (int i = tid; i < S.count[0] && i < P.cap; i += B) {
-            const int root = sm.items[S.levelOff[0] + i * P.tupleLen[0]];
+            const int root = items[S.levelOff[0] + i * P.tupleLen[0]];
             const uint32_t old = atomicOr(&fb[root >> 5], 1u << (root & 31));
             if (heavy && !(old & (1u << (root & 31)))) myNew++;
         }
@@ -277,9 +279,11 @@ __device__ __forceinline__ void run_task(Smem<B>& sm, const DevIndex& ix, const 
             const int nw = min(B, cnt - w0);
             const int lenK = P.tupleLen[k];
             const int strideK = lenK + 2;
-            const int* baseK = sm.items + S.levelOff[k];
-            const DevStep& stp = P.steps[k];
+            const int* baseK = items + S.levelOff[k];
+            const DevStep stp = P.steps[k];   // uniform for the round: keep it in registers
             const bool leaf = (k + 1 == P.m);
+            const bool hasFilters = (P.chkN[k + 1] | P.usedN[k + 1]) != 0;
+            const int wo = P.wo;
             const bool itemHasRank = pairs && P.hoLevel >= 1 && k >= P.hoLevel;
 
             // window: the stored neighbour segment of each item
@@ -316,50 +320,32 @@ __device__ __forceinline__ void run_task(Smem<B>& sm, const DevIndex& ix, const 
             const long long take = min(total, (long long)(leaf ? kLeafChunk : P.cap));
             const int lenN = leaf ? 0 : P.tupleLen[k + 1];
             const int strideN = lenN + 2;
-            int* baseN = leaf ? nullptr : sm.items + S.levelOff[k + 1];
+            int* baseN = leaf ? nullptr : items + S.levelOff[k + 1];
 
-            for (long long j = tid; j < take; j += B) {
-                int lo = 0, hi = nw - 1;
-                while (lo < hi) {
-                    const int mid = (lo + hi) >> 1;
-                    if (sm.wPre[mid] > j) hi = mid; else lo = mid + 1;
-                }
-                const long long start = sm.wPre[lo] - sm.wLen[lo];
-                const int e = sm.wBeg[lo] + (int)(j - start);
+            // One candidate: its parent item `lo`, edge `e`, new value(s)
+            // n0/n1 and (when this step binds hO) the loaded rank.
+            auto eval = [&](int lo, int e, int n0, int n1, int rankLoaded) {
                 const int* par = baseK + (w0 + lo) * strideK;
                 const int root = par[0];
-                if (!pairs && ((fb[root >> 5] >> (root & 31)) & 1u)) continue;
-                int n0, n1 = 0;
-                if (stp.kind == kExpand) {
-                    n0 = __ldg(ix.val[stp.dir] + e);
-                    mt.add(4);
-                } else {
-                    n0 = __ldg(ix.src[0] + e);
-                    n1 = __ldg(ix.val[0] + e);
-                    mt.add(8);
-                    if (stp.sameVar ? (n0 != n1) : (n0 == n1)) continue;
-                }
-                bool ok = true;
+                if (!pairs && ((fb[root >> 5] >> (root & 31)) & 1u)) return;
+                if (stp.kind == kScan && (stp.sameVar ? (n0 != n1) : (n0 == n1))) return;
                 for (int q = kTupleHead; q < lenK; ++q) {
                     const int x = par[q];
-                    if (x == n0 || (stp.nNew == 2 && x == n1)) { ok = false; break; }
+                    if (x == n0 || (stp.nNew == 2 && x == n1)) return;
                 }
-                if (!ok) continue;
                 auto valN = [&](TermRef ref) -> int {
                     if (ref < 0) return P.consts[-1 - ref];
                     if (ref < lenK) return par[ref];
                     return ref == lenK ? n0 : n1;
                 };
-                if (!pass_filters(P, ix, k + 1, mt, valN)) continue;
+                if (hasFilters && !pass_filters(P, ix, k + 1, mt, valN)) return;
                 int rank = par[1];
                 if (pairs && stp.hoWhich) {
-                    if (stp.kind == kExpand) rank = __ldg(ix.valRank[stp.dir] + e);
-                    else rank = stp.hoWhich == 1 ? __ldg(ix.srcRank[0] + e) : __ldg(ix.valRank[0] + e);
-                    mt.add(4);
+                    rank = rankLoaded;
                     if (!leaf) {
-                        const long long bit = (rowBase + root) * (long long)P.wo + rank;
+                        const long long bit = (rowBase + root) * (long long)wo + rank;
                         if (!shared) mt.add(4);
-                        if ((bm[bit >> 5] >> (bit & 31)) & 1u) continue;
+                        if ((bm[bit >> 5] >> (bit & 31)) & 1u) return;
                     }
                 }
                 if (leaf) {
@@ -368,7 +354,7 @@ __device__ __forceinline__ void run_task(Smem<B>& sm, const DevIndex& ix, const 
                         const uint32_t old = atomicOr(&fb[root >> 5], mask);
                         if (heavy) { mt.add(8); myNew += (old & mask) ? 0ull : 1ull; }
                     } else {
-                        const long long bit = (rowBase + root) * (long long)P.wo + rank;
+                        const long long bit = (rowBase + root) * (long long)wo + rank;
                         const uint32_t mask = 1u << (bit & 31);
                         const uint32_t old = atomicOr(&bm[bit >> 5], mask);
                         if (!shared) mt.add(8);
@@ -376,9 +362,9 @@ __device__ __forceinline__ void run_task(Smem<B>& sm, const DevIndex& ix, const 
                     }
                 } else {
                     const int2 seg = step_segment(P, ix, k + 1, mt, valN);
-                    if (seg.y <= seg.x) continue;
+                    if (seg.y <= seg.x) return;
                     const int slot = atomicAdd(&S.count[k + 1], 1);
-                    if (slot >= P.cap) { atomicOr(status, 8); continue; }
+                    if (slot >= P.cap) { atomicOr(status, 8); return; }
                     int* dst = baseN + slot * strideN;
                     dst[0] = root;
                     dst[1] = rank;
@@ -388,6 +374,45 @@ __device__ __forceinline__ void run_task(Smem<B>& sm, const DevIndex& ix, const 
                     dst[lenN] = seg.x;
                     dst[lenN + 1] = seg.y - seg.x;
                 }
+            };
+
+            // Candidates j = tid, tid + B, ... in groups of kU per thread: all
+            // group members are located first, then their loads are issued
+            // together, then they are evaluated (memory-level parallelism).
+            const int* vbase = stp.kind == kExpand ? ix.val[stp.dir] : ix.src[0];
+            const int* rbase = stp.kind == kExpand ? ix.valRank[stp.dir]
+                                                   : (stp.hoWhich == 1 ? ix.srcRank[0] : ix.valRank[0]);
+            const bool wantRank = pairs && stp.hoWhich;
+            int hint = 0;
+            for (long long jb = tid; jb < take; jb += (long long)B * kU) {
+                int lo_[kU], e_[kU], n0_[kU], n1_[kU], rk_[kU];
+#pragma unroll
+                for (int u = 0; u < kU; ++u) {
+                    const long long j = jb + (long long)u * B;
+                    lo_[u] = -1;
+                    e_[u] = 0;
+                    if (j < take) {
+                        int lo = hint, hi = nw - 1;
+                        while (lo < hi) {
+                            const int mid = (lo + hi) >> 1;
+                            if (sm.wPre[mid] > j) hi = mid; else lo = mid + 1;
+                        }
+                        hint = lo;
+                        lo_[u] = lo;
+                        e_[u] = sm.wBeg[lo] + (int)(j - (sm.wPre[lo] - sm.wLen[lo]));
+                    }
+                }
+#pragma unroll
+                for (int u = 0; u < kU; ++u) {
+                    n0_[u] = n1_[u] = rk_[u] = 0;
+                    if (lo_[u] < 0) continue;
+                    n0_[u] = __ldg(vbase + e_[u]);
+                    if (stp.kind == kScan) { n1_[u] = __ldg(ix.val[0] + e_[u]); mt.add(8); } else mt.add(4);
+                    if (wantRank) { rk_[u] = __ldg(rbase + e_[u]); mt.add(4); }
+                }
+#pragma unroll
+                for (int u = 0; u < kU; ++u)
+                    if (lo_[u] >= 0) eval(lo_[u], e_[u], n0_[u], n1_[u], rk_[u]);
             }
             __syncthreads();
             if (tid == 0) {
@@ -418,7 +443,7 @@ __device__ __forceinline__ void run_task(Smem<B>& sm, const DevIndex& ix, const 
     // ---- result ----
     unsigned long long mine = 0;
     if (!pairs && !heavy) {
-        for (int i = tid; i < ((G + 31) >> 5); i += B) mine += __popc(sm.bitmap[i]);
+        for (int i = tid; i < ((G + 31) >> 5); i += B) mine += __popc(sbits[i]);
     } else {
         mine = myNew;
     }

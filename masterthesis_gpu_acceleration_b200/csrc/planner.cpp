@@ -188,20 +188,39 @@ bool build_steps(Builder& b, const std::vector<Atom>& body, const Atom* head, in
     return true;
 }
 
-// Frontier capacity per level: levels 0..m-1 each hold `cap` items of
-// (tuple + stored segment) ints; the roots of one task must fit level 0 and,
-// for kPairs, their bitmap rows must fit the block's bitmap.
-void finish_capacity(DevPlan& P, const Geom& geom) {
+// Splits the block's shared pool between the frontier (levels 0..m-1, each
+// `cap` items of tuple + stored segment) and the dedup bitmap: kExist keeps
+// one bit per root of the task (at most 1024 roots); kPairs gives its bitmap
+// rows up to half the pool (ceil(wo / 32) words per root), or none when one
+// row does not fit next to a minimal frontier (the plan then deduplicates in
+// a global bitmap).  Returns false in that last case.
+bool finish_capacity(DevPlan& P, const Geom& geom) {
     int sum = 0;
     if (P.m == 0) sum = P.tupleLen[0];
     for (int l = 0; l < P.m; ++l) sum += P.tupleLen[l] + 2;
-    int cap = (geom.itemInts() / std::max(sum, 1)) & ~31;
-    P.cap = std::max(cap, 32);
-    P.groupMax = P.cap;
-    if (P.mode == kPairs && P.wo > 0) {
-        int64_t g = (int64_t)geom.bitmapWords() * 32 / P.wo;
-        P.groupMax = (int32_t)std::min<int64_t>(P.groupMax, g);
+    sum = std::max(sum, 1);
+    const int pool = geom.poolInts();
+    bool local = true;
+    int bitmapInts = 0, groupMax = 0;
+    if (P.mode == kPairs) {
+        const int rowWords = std::max(1, (P.wo + 31) / 32);
+        if ((int64_t)rowWords + 32LL * sum > pool) {
+            local = false;
+            groupMax = 512;
+        } else {
+            int g = std::max(1, std::min(1024, (pool / 2) / rowWords));
+            while (g > 1 && pool - g * rowWords < 32 * sum) --g;
+            bitmapInts = g * rowWords;
+            groupMax = g;
+        }
+    } else {
+        bitmapInts = 32;  // 1024 found bits
+        groupMax = 1024;
     }
+    P.cap = std::max(((pool - bitmapInts) / sum) & ~31, 32);
+    P.bitmapOff = pool - bitmapInts;
+    P.groupMax = std::min(groupMax, P.cap);
+    return local;
 }
 
 }  // namespace
@@ -327,11 +346,11 @@ RulePlan plan_rule(const Rule& rule, const HostIndex& ix, const Geom& geom) {
                         else P.wo = (int32_t)ix.pred_rows(st.pred, st.hoWhich == 1 ? 0 : 1);
                     }
                 }
-                finish_capacity(P, geom);
+                const bool local = finish_capacity(P, geom);
                 B.how = kDevice;
                 B.rootBeg = ix.predRow[seedDir][seedPred];
                 B.rootEnd = ix.predRow[seedDir][seedPred + 1];
-                B.needsGlobalBitmap = pairs && (int64_t)P.wo > (int64_t)geom.bitmapWords() * 32;
+                B.needsGlobalBitmap = pairs && !local;
                 B.estCost = (double)(ix.predEdge[seedDir][seedPred + 1] - ix.predEdge[seedDir][seedPred]);
             } else if (!b.ok) {
                 rp.status = kRuleUnsupported;
