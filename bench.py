@@ -71,9 +71,9 @@ def dist_env():
 
 
 def data_for(args, rank: int) -> Path:
-    from masterthesis_gpu_acceleration_b200 import synth
+    from masterthesis_gpu_acceleration_b200 import shard, synth
     d = Path(args.data) / (f"{args.config}" if rank == 0 else f"{args.config}_r{rank}")
-    return synth.generate(args.config, d, seed=0, rule_seed=None if rank == 0 else rank)
+    return synth.generate(args.config, d, seed=0, rule_seed=shard.rule_seed(rank))
 
 
 class ClockSampler:
@@ -228,13 +228,10 @@ def engine_arm(args):
             dist.barrier()
         torch.cuda.synchronize()
 
+    from masterthesis_gpu_acceleration_b200 import shard
+
     def allmax(x: float) -> float:
-        if world == 1:
-            return x
-        import torch.distributed as dist
-        t = torch.tensor([x], dtype=torch.float64, device="cuda")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        return float(t.item())
+        return shard.max_over_ranks(x, device="cuda")
 
     import masterthesis_gpu_acceleration_b200 as eng
     from masterthesis_gpu_acceleration_b200 import synth
@@ -262,7 +259,7 @@ def engine_arm(args):
     barrier()
     clk = clocks.stop()
     max_ms = allmax(total_ms)
-    value = world * len(rules) * args.steps / (max_ms / 1e3)
+    value = shard.weak_value(len(rules), world, args.steps, max_ms)
 
     exact = None
     if rank == 0 and args.config == "c3" and not args.max_rules:

@@ -141,6 +141,46 @@ int gpu_evaluate_rule_noalloc(void* ctx, const char* ruleText, GpuRuleResult* ou
  * value. */
 int gpu_set_option(void* ctx, const char* name, long long value);
 
+/* ---- serving: continuous batching on a resident graph ---- */
+
+/* One completed request.  status: 0 ok, -1 the rule does not parse, -2 the
+ * rule's device-memory estimate exceeds the server's whole budget, -3 a CUDA
+ * or engine error.  latencyMs: from gpu_serve_submit to completion. */
+typedef struct {
+    long long     requestId;
+    int           status;
+    GpuRuleResult result;
+    double        latencyMs;
+} GpuServeResult;
+
+/* Starts a request loop on a loaded graph: a worker thread with `slots`
+ * launch slots (streams, 1..16), at most maxBatch rules per launch, and at
+ * most memBudgetBytes of estimated device memory (plans, tasks, dedup
+ * buffers) held by launches in flight.  Whenever a slot is free, the waiting
+ * requests are admitted in arrival order while their memory fits and are
+ * launched together without waiting for the other slots, so requests that
+ * arrive while others run are batched onto the GPU as slots and memory free
+ * up.  While a server runs, its context must not be used by other calls.
+ * Returns a server handle or NULL. */
+void* gpu_serve_start(void* ctx, int slots, int maxBatch, long long memBudgetBytes);
+
+/* Queues one rule (text syntax).  Thread-safe.  Returns 0, or -1 when the
+ * server is stopping or an argument is null. */
+int gpu_serve_submit(void* server, long long requestId, const char* ruleText);
+
+/* Copies up to max completed results into out, waiting up to waitMs for the
+ * first one.  Thread-safe.  Returns the number copied, or -1. */
+int gpu_serve_poll(void* server, GpuServeResult* out, int max, int waitMs);
+
+/* Requests submitted and completed, launches issued and device memory
+ * currently held by launches in flight. */
+int gpu_serve_stats(void* server, long long* submitted, long long* completed, long long* launches,
+                    long long* memInUse);
+
+/* Finishes every queued request, stops the worker and frees the server
+ * (uncollected results are dropped).  NULL is ignored. */
+void gpu_serve_stop(void* server);
+
 /* Number of entities, predicates and distinct triples of a loaded graph. */
 int gpu_graph_stats(void* ctx, long long* entities, long long* predicates, long long* triples);
 

@@ -37,6 +37,11 @@ API_SYMBOLS = (
     "gpu_batch_profile",
     "gpu_batch_autotune",
     "gpu_set_option",
+    "gpu_serve_start",
+    "gpu_serve_submit",
+    "gpu_serve_poll",
+    "gpu_serve_stats",
+    "gpu_serve_stop",
     "gpu_graph_stats",
     "gpu_last_error",
 )
@@ -63,6 +68,17 @@ class GpuRuleResult(ctypes.Structure):
         return (f"support={self.support}, headSize={self.headSize}, headCoverage={self.headCoverage}, "
                 f"bodySize={self.bodySize}, confidence={self.confidence}, "
                 f"supportMs={self.supportMs} ms, confidenceMs={self.confidenceMs} ms")
+
+
+class GpuServeResult(ctypes.Structure):
+    """Same layout as GpuServeResult in include/gpu_rules_api.h."""
+
+    _fields_ = [
+        ("requestId", ctypes.c_longlong),
+        ("status", ctypes.c_int),
+        ("result", GpuRuleResult),
+        ("latencyMs", ctypes.c_double),
+    ]
 
 
 _lib = None
@@ -111,6 +127,16 @@ def load_library(path: os.PathLike | str | None = None) -> ctypes.CDLL:
     lib.gpu_batch_autotune.argtypes = [ctypes.c_void_p, ctypes.c_int]
     lib.gpu_set_option.restype = ctypes.c_int
     lib.gpu_set_option.argtypes = [ctypes.c_void_p, ctypes.c_char_p, ctypes.c_longlong]
+    lib.gpu_serve_start.restype = ctypes.c_void_p
+    lib.gpu_serve_start.argtypes = [ctypes.c_void_p, ctypes.c_int, ctypes.c_int, ctypes.c_longlong]
+    lib.gpu_serve_submit.restype = ctypes.c_int
+    lib.gpu_serve_submit.argtypes = [ctypes.c_void_p, ctypes.c_longlong, ctypes.c_char_p]
+    lib.gpu_serve_poll.restype = ctypes.c_int
+    lib.gpu_serve_poll.argtypes = [ctypes.c_void_p, ctypes.POINTER(GpuServeResult), ctypes.c_int, ctypes.c_int]
+    lib.gpu_serve_stats.restype = ctypes.c_int
+    lib.gpu_serve_stats.argtypes = [ctypes.c_void_p] + [ctypes.POINTER(ctypes.c_longlong)] * 4
+    lib.gpu_serve_stop.restype = None
+    lib.gpu_serve_stop.argtypes = [ctypes.c_void_p]
     lib.gpu_graph_stats.restype = ctypes.c_int
     lib.gpu_graph_stats.argtypes = [ctypes.c_void_p] + [ctypes.POINTER(ctypes.c_longlong)] * 3
     lib.gpu_last_error.restype = ctypes.c_char_p
@@ -183,6 +209,9 @@ class GpuRulesLib:
 
     def prepare_batch(self, rules: Sequence[str], is_json: bool = False) -> "PreparedBatch":
         return PreparedBatch(self, rules, is_json)
+
+    def serve(self, slots: int = 3, max_batch: int = 4096, mem_budget: int = 1 << 30) -> "GpuServer":
+        return GpuServer(self, slots, max_batch, mem_budget)
 
     def set_option(self, name: str, value: int) -> None:
         if self._lib.gpu_set_option(self._handle(), name.encode(), int(value)) != 0:
@@ -290,5 +319,57 @@ class PreparedBatch:
     def __del__(self):
         try:
             self.close()
+        except Exception:
+            pass
+
+
+class GpuServer:
+    """Continuous-batching request loop on a loaded graph (gpu_serve_*)."""
+
+    def __init__(self, lib: GpuRulesLib, slots: int = 3, max_batch: int = 4096, mem_budget: int = 1 << 30):
+        self._owner = lib
+        self._lib = lib._lib
+        h = self._lib.gpu_serve_start(lib._handle(), slots, max_batch, mem_budget)
+        if not h:
+            raise RuntimeError(f"gpu_serve_start failed ({self._lib.gpu_last_error().decode(errors='replace')})")
+        self._h = ctypes.c_void_p(h)
+        self._buf = (GpuServeResult * 4096)()
+
+    def submit(self, request_id: int, rule_text: str) -> None:
+        if self._lib.gpu_serve_submit(self._h, request_id, rule_text.encode()) != 0:
+            raise RuntimeError("gpu_serve_submit failed")
+
+    def poll(self, wait_ms: int = 0) -> list:
+        """Completed requests as (request_id, status, GpuRuleResult, latency_ms)."""
+        n = self._lib.gpu_serve_poll(self._h, self._buf, len(self._buf), wait_ms)
+        if n < 0:
+            raise RuntimeError("gpu_serve_poll failed")
+        out = []
+        for i in range(n):
+            r = self._buf[i]
+            res = GpuRuleResult()
+            ctypes.pointer(res)[0] = r.result
+            out.append((r.requestId, r.status, res, r.latencyMs))
+        return out
+
+    def stats(self) -> dict:
+        v = [ctypes.c_longlong() for _ in range(4)]
+        self._lib.gpu_serve_stats(self._h, *[ctypes.byref(x) for x in v])
+        return dict(zip(("submitted", "completed", "launches", "mem_in_use"), (x.value for x in v)))
+
+    def stop(self) -> None:
+        if getattr(self, "_h", None) is not None:
+            self._lib.gpu_serve_stop(self._h)
+            self._h = None
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.stop()
+
+    def __del__(self):
+        try:
+            self.stop()
         except Exception:
             pass

@@ -22,198 +22,18 @@
 #include <string>
 #include <vector>
 
-#include "../../include/gpu_rules_api.h"
-#include "common.hpp"
-#include "index.hpp"
-#include "planner.hpp"
-#include "rules.hpp"
-#include "tasks.hpp"
-#include "turtle.hpp"
+#include "engine.hpp"
 
 namespace gr {
 
-size_t engine_smem_bytes(int block);
-cudaError_t engine_configure();
-cudaError_t engine_launch(const DevIndex& ix, const DevPlan* plans, const DevTask* tasks, int nTasks,
-                          int* taskCounter, unsigned long long* results, int* status, int grid, int block,
-                          cudaStream_t stream, const EngineProfile* prof);
-
 namespace {
-
 thread_local std::string g_lastError;
+}  // namespace
 
 void set_error(const std::string& s) {
     g_lastError = s;
     std::fprintf(stderr, "[gpu_rules] %s\n", s.c_str());
 }
-
-struct CudaError : std::runtime_error {
-    using std::runtime_error::runtime_error;
-};
-
-inline void ck(cudaError_t e, const char* what) {
-    if (e != cudaSuccess) throw CudaError(std::string(what) + ": " + cudaGetErrorString(e));
-}
-
-struct DevBuf {
-    void* p = nullptr;
-    size_t cap = 0;
-    void ensure(size_t bytes) {
-        if (bytes <= cap) return;
-        release();
-        size_t want = std::max<size_t>(bytes, 4096);
-        ck(cudaMalloc(&p, want), "cudaMalloc");
-        cap = want;
-    }
-    void release() {
-        if (p) cudaFree(p);
-        p = nullptr;
-        cap = 0;
-    }
-    ~DevBuf() { release(); }
-};
-
-struct HostBuf {  // pinned
-    void* p = nullptr;
-    size_t cap = 0;
-    void ensure(size_t bytes) {
-        if (bytes <= cap) return;
-        release();
-        size_t want = std::max<size_t>(bytes, 4096);
-        ck(cudaMallocHost(&p, want), "cudaMallocHost");
-        cap = want;
-    }
-    void release() {
-        if (p) cudaFreeHost(p);
-        p = nullptr;
-        cap = 0;
-    }
-    ~HostBuf() { release(); }
-};
-
-int64_t clamp_int(int64_t v) { return std::min<int64_t>(v, INT_MAX); }
-
-}  // namespace
-
-struct Context;
-
-// A set of plans and their tasks resident on the device, with the buffers
-// one launch over them needs.
-struct Staged {
-    DevBuf dBlob, dResults, dCtl, dBitmap, dHeavy, dBytes, dTaskNs;
-    std::vector<DevTask> hTasks;  // task list as uploaded (for profiles)
-    std::vector<double> hCost;    // estimated work per uploaded task
-    HostBuf hBlob, hResults, hCtl;
-    const DevPlan* dPlans = nullptr;
-    const DevTask* dTasks = nullptr;
-    int nPlans = 0, nTasks = 0;
-    size_t bitmapWords = 0, heavyWords = 0;
-    size_t h2dBytes = 0, d2hBytes = 0;
-
-    void stage(Context& c, std::vector<DevPlan>& plans, const std::vector<const PhasePlan*>& phases,
-               bool sortTasks, cudaStream_t s);
-    void enqueue(Context& c, cudaStream_t s, bool profile);
-    void download(cudaStream_t s) {
-        if (!nPlans) return;
-        ck(cudaMemcpyAsync(hResults.p, dResults.p, nPlans * sizeof(unsigned long long), cudaMemcpyDeviceToHost, s), "D2H results");
-        ck(cudaMemcpyAsync(hCtl.p, dCtl.p, 8, cudaMemcpyDeviceToHost, s), "D2H status");
-    }
-    const unsigned long long* counts() const { return static_cast<const unsigned long long*>(hResults.p); }
-    void check_status() const {
-        if (nPlans && static_cast<const int*>(hCtl.p)[1] != 0)
-            throw CudaError("engine reported internal status " + std::to_string(static_cast<const int*>(hCtl.p)[1]));
-    }
-};
-
-struct Context {
-    int device = 0;
-    TermDict ents, preds;
-    std::unordered_map<std::string, std::string> prefixes;
-    HostIndex hix;
-    DevBuf indexMem;
-    DevIndex dix{};
-    cudaStream_t stream = nullptr;
-    cudaEvent_t ev[4] = {};
-    Staged one;          // per-rule launches
-    std::unique_ptr<TaskBuilder> tasks;
-    Geom geom;
-    int grid = 0;
-    int sms = 0;
-    std::unique_ptr<RuleParser> parser;
-
-    ~Context() {
-        cudaSetDevice(device);
-        if (stream) cudaStreamSynchronize(stream);
-        for (auto& e : ev) if (e) cudaEventDestroy(e);
-        if (stream) cudaStreamDestroy(stream);
-    }
-
-    void upload_index() {
-        const HostIndex& h = hix;
-        std::vector<std::pair<const void*, size_t>> parts;
-        auto add = [&](const void* p, size_t n) { parts.push_back({p, n}); };
-        for (int d = 0; d < 2; ++d) {
-            add(h.val[d].data(), h.val[d].size() * 4);
-            add(h.valRank[d].data(), h.valRank[d].size() * 4);
-            add(h.src[d].data(), h.src[d].size() * 4);
-            add(h.srcRank[d].data(), h.srcRank[d].size() * 4);
-            add(h.rowKey[d].data(), h.rowKey[d].size() * 4);
-            add(h.rowBeg[d].data(), h.rowBeg[d].size() * 4);
-            add(h.predRow[d].data(), h.predRow[d].size() * 4);
-            add(h.predEdge[d].data(), h.predEdge[d].size() * 4);
-        }
-        add(h.hash.data(), h.hash.size() * sizeof(HashSlot));
-        size_t total = 0;
-        std::vector<size_t> off;
-        for (auto& pp : parts) {
-            off.push_back(total);
-            total += (pp.second + 255) & ~size_t(255);
-        }
-        size_t freeB = 0, totB = 0;
-        ck(cudaMemGetInfo(&freeB, &totB), "cudaMemGetInfo");
-        if (total + (64u << 20) > freeB)
-            throw CudaError("not enough device memory: need ~" + std::to_string((total >> 20) + 64) +
-                            " MB, " + std::to_string(freeB >> 20) + " MB free");
-        indexMem.ensure(std::max<size_t>(total, 256));
-        char* base = static_cast<char*>(indexMem.p);
-        for (size_t i = 0; i < parts.size(); ++i)
-            if (parts[i].second)
-                ck(cudaMemcpy(base + off[i], parts[i].first, parts[i].second, cudaMemcpyHostToDevice), "cudaMemcpy(index)");
-        size_t k = 0;
-        for (int d = 0; d < 2; ++d) {
-            dix.val[d] = reinterpret_cast<const int32_t*>(base + off[k++]);
-            dix.valRank[d] = reinterpret_cast<const int32_t*>(base + off[k++]);
-            dix.src[d] = reinterpret_cast<const int32_t*>(base + off[k++]);
-            dix.srcRank[d] = reinterpret_cast<const int32_t*>(base + off[k++]);
-            dix.rowKey[d] = reinterpret_cast<const int32_t*>(base + off[k++]);
-            dix.rowBeg[d] = reinterpret_cast<const int32_t*>(base + off[k++]);
-            dix.predRow[d] = reinterpret_cast<const int32_t*>(base + off[k++]);
-            dix.predEdge[d] = reinterpret_cast<const int32_t*>(base + off[k++]);
-        }
-        dix.hash = reinterpret_cast<const HashSlot*>(base + off[k++]);
-        dix.hashMask = h.hashMask;
-        dix.nPred = h.nPred;
-        dix.nEnt = h.nEnt;
-        dix.nTriples = h.nTriples;
-    }
-
-    bool set_block(int b) {
-        if (b != 128 && b != 256 && b != 512) return false;
-        geom.block = b;
-        grid = sms * (1024 / b);
-        return true;
-    }
-
-    void init_device() {
-        ck(cudaGetDevice(&device), "cudaGetDevice");
-        ck(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device), "cudaDeviceGetAttribute");
-        ck(engine_configure(), "cudaFuncSetAttribute");
-        if (const char* b = std::getenv("GPU_RULES_BLOCK")) set_block(std::atoi(b));
-        else set_block(geom.block);
-        ck(cudaStreamCreateWithFlags(&stream, cudaStreamNonBlocking), "cudaStreamCreate");
-        for (auto& e : ev) ck(cudaEventCreate(&e), "cudaEventCreate");
-    }
-};
 
 void Staged::stage(Context& c, std::vector<DevPlan>& plans, const std::vector<const PhasePlan*>& phases,
                    bool sortTasks, cudaStream_t s) {
@@ -305,37 +125,6 @@ void Staged::enqueue(Context& c, cudaStream_t s, bool profile) {
        "engine launch");
 }
 
-// A batch prepared once and replayed: parse, plan and upload happen at
-// preparation; a run is one CUDA-graph launch of the device work.
-struct Batch {
-    Context* c = nullptr;
-    int n = 0;
-    std::vector<RulePlan> rps;
-    std::vector<int> parseStatus;
-    std::vector<int> owner;  // plan -> rule * 2 + phase
-    std::vector<DevPlan> plans0;
-    std::vector<const PhasePlan*> phases;
-    Staged st;
-    cudaStream_t stream = nullptr;
-    cudaEvent_t ev0 = nullptr, ev1 = nullptr;
-    cudaGraph_t graph = nullptr;
-    cudaGraphExec_t exec = nullptr;
-    DevBuf flush;
-    double lastMs = 0.0;
-
-    ~Batch() {
-        if (c) cudaSetDevice(c->device);
-        if (stream) cudaStreamSynchronize(stream);
-        if (exec) cudaGraphExecDestroy(exec);
-        if (graph) cudaGraphDestroy(graph);
-        if (ev0) cudaEventDestroy(ev0);
-        if (ev1) cudaEventDestroy(ev1);
-        if (stream) cudaStreamDestroy(stream);
-    }
-};
-
-namespace {
-
 void compose(const RulePlan& rp, int64_t sup, int64_t body, double supMs, double confMs, GpuRuleResult* out) {
     *out = GpuRuleResult{};
     out->headSize = (int)clamp_int(rp.headSize);
@@ -350,6 +139,8 @@ void compose(const RulePlan& rp, int64_t sup, int64_t body, double supMs, double
     out->supportMs = supMs;
     out->confidenceMs = confMs;
 }
+
+namespace {
 
 // One phase in its own launch (the plain per-rule form), timed by events.
 int64_t run_one_phase(Context& c, const PhasePlan& ph, float* ms) {
@@ -379,6 +170,9 @@ int evaluate_parsed(Context& c, const Rule& rule, GpuRuleResult* out) {
 void prepare(Batch& b, Context& c, const char* const* rules, int n, int isJson) {
     b.c = &c;
     b.n = n;
+    b.owner.clear();
+    if (b.exec) { cudaGraphExecDestroy(b.exec); b.exec = nullptr; }
+    if (b.graph) { cudaGraphDestroy(b.graph); b.graph = nullptr; }
     b.rps.assign(n, RulePlan{});
     b.parseStatus.assign(n, 0);
     std::vector<DevPlan> plans;
@@ -539,11 +333,31 @@ int gpu_evaluate_rules_batch(void* ctx, const char* const* rules, int n, int isJ
     if (deviceMs) *deviceMs = 0.0;
     try {
         cudaSetDevice(c.device);
-        Batch b;
-        prepare(b, c, rules, n, isJson);
-        run_batch(b, false, 0);
-        collect(b, out, status);
-        if (deviceMs) *deviceMs = b.lastMs;
+        // Pipelined: chunk k+1 is parsed, planned and staged on the host
+        // while chunk k runs on the device (each chunk on its own stream).
+        const int K = std::max(1, std::min(4, (n + 2499) / 2500));
+        while ((int)c.pipe.size() < K) c.pipe.push_back(new Batch());
+        for (int k = 0; k < K; ++k) {
+            const int lo = (int)((long long)n * k / K), hi = (int)((long long)n * (k + 1) / K);
+            Batch& b = *c.pipe[k];
+            prepare(b, c, rules + lo, hi - lo, isJson);
+            ck(cudaEventRecord(b.ev0, b.stream), "event");
+            b.st.enqueue(c, b.stream, false);
+            ck(cudaEventRecord(b.ev1, b.stream), "event");
+            b.st.download(b.stream);
+        }
+        float span = 0.f;
+        for (int k = 0; k < K; ++k) {
+            Batch& b = *c.pipe[k];
+            ck(cudaStreamSynchronize(b.stream), "engine");
+            b.st.check_status();
+            float ms = 0.f;
+            ck(cudaEventElapsedTime(&ms, c.pipe[0]->ev0, b.ev1), "elapsed");
+            span = std::max(span, ms);
+            const int lo = (int)((long long)n * k / K);
+            collect(b, out + lo, status ? status + lo : nullptr);
+        }
+        if (deviceMs) *deviceMs = span;
         return 0;
     } catch (const std::exception& e) {
         set_error(std::string("gpu_evaluate_rules_batch error: ") + e.what());

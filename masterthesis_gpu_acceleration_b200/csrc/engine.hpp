@@ -1,0 +1,243 @@
+// engine.hpp — host-side engine state shared by the C ABI (context.cu) and
+// the serving loop (serve.cu): device buffers, staged launches, the graph
+// context and prepared batches.
+#pragma once
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <climits>
+#include <cstdio>
+#include <memory>
+#include <stdexcept>
+#include <string>
+#include <unordered_map>
+#include <vector>
+
+#include "../../include/gpu_rules_api.h"
+#include "common.hpp"
+#include "index.hpp"
+#include "planner.hpp"
+#include "rules.hpp"
+#include "tasks.hpp"
+#include "turtle.hpp"
+
+namespace gr {
+
+size_t engine_smem_bytes(int block);
+cudaError_t engine_configure();
+cudaError_t engine_launch(const DevIndex& ix, const DevPlan* plans, const DevTask* tasks, int nTasks,
+                          int* taskCounter, unsigned long long* results, int* status, int grid, int block,
+                          cudaStream_t stream, const EngineProfile* prof);
+
+// Records the calling thread's last error (gpu_last_error) and logs it.
+void set_error(const std::string& s);
+
+struct CudaError : std::runtime_error {
+    using std::runtime_error::runtime_error;
+};
+
+inline void ck(cudaError_t e, const char* what) {
+    if (e != cudaSuccess) throw CudaError(std::string(what) + ": " + cudaGetErrorString(e));
+}
+
+struct DevBuf {
+    void* p = nullptr;
+    size_t cap = 0;
+    void ensure(size_t bytes) {
+        if (bytes <= cap) return;
+        release();
+        size_t want = std::max<size_t>(bytes, 4096);
+        ck(cudaMalloc(&p, want), "cudaMalloc");
+        cap = want;
+    }
+    void release() {
+        if (p) cudaFree(p);
+        p = nullptr;
+        cap = 0;
+    }
+    ~DevBuf() { release(); }
+};
+
+struct HostBuf {  // pinned
+    void* p = nullptr;
+    size_t cap = 0;
+    void ensure(size_t bytes) {
+        if (bytes <= cap) return;
+        release();
+        size_t want = std::max<size_t>(bytes, 4096);
+        ck(cudaMallocHost(&p, want), "cudaMallocHost");
+        cap = want;
+    }
+    void release() {
+        if (p) cudaFreeHost(p);
+        p = nullptr;
+        cap = 0;
+    }
+    ~HostBuf() { release(); }
+};
+
+inline int64_t clamp_int(int64_t v) { return std::min<int64_t>(v, INT_MAX); }
+
+struct Context;
+
+// A set of plans and their tasks resident on the device, with the buffers
+// one launch over them needs.
+struct Staged {
+    DevBuf dBlob, dResults, dCtl, dBitmap, dHeavy, dBytes, dTaskNs;
+    std::vector<DevTask> hTasks;  // task list as uploaded (for profiles)
+    std::vector<double> hCost;    // estimated work per uploaded task
+    HostBuf hBlob, hResults, hCtl;
+    const DevPlan* dPlans = nullptr;
+    const DevTask* dTasks = nullptr;
+    int nPlans = 0, nTasks = 0;
+    size_t bitmapWords = 0, heavyWords = 0;
+    size_t h2dBytes = 0, d2hBytes = 0;
+
+    void stage(Context& c, std::vector<DevPlan>& plans, const std::vector<const PhasePlan*>& phases,
+               bool sortTasks, cudaStream_t s);
+    void enqueue(Context& c, cudaStream_t s, bool profile);
+    void download(cudaStream_t s) {
+        if (!nPlans) return;
+        ck(cudaMemcpyAsync(hResults.p, dResults.p, nPlans * sizeof(unsigned long long), cudaMemcpyDeviceToHost, s), "D2H results");
+        ck(cudaMemcpyAsync(hCtl.p, dCtl.p, 8, cudaMemcpyDeviceToHost, s), "D2H status");
+    }
+    const unsigned long long* counts() const { return static_cast<const unsigned long long*>(hResults.p); }
+    void check_status() const {
+        if (nPlans && static_cast<const int*>(hCtl.p)[1] != 0)
+            throw CudaError("engine reported internal status " + std::to_string(static_cast<const int*>(hCtl.p)[1]));
+    }
+};
+
+struct Context {
+    int device = 0;
+    TermDict ents, preds;
+    std::unordered_map<std::string, std::string> prefixes;
+    HostIndex hix;
+    DevBuf indexMem;
+    DevIndex dix{};
+    cudaStream_t stream = nullptr;
+    cudaEvent_t ev[4] = {};
+    Staged one;          // per-rule launches
+    std::vector<struct Batch*> pipe;  // reusable chunks of one-shot batches
+    std::unique_ptr<TaskBuilder> tasks;
+    Geom geom;
+    int grid = 0;
+    int sms = 0;
+    std::unique_ptr<RuleParser> parser;
+
+    void free_pipe();
+    ~Context() {
+        free_pipe();
+        cudaSetDevice(device);
+        if (stream) cudaStreamSynchronize(stream);
+        for (auto& e : ev) if (e) cudaEventDestroy(e);
+        if (stream) cudaStreamDestroy(stream);
+    }
+
+    void upload_index() {
+        const HostIndex& h = hix;
+        std::vector<std::pair<const void*, size_t>> parts;
+        auto add = [&](const void* p, size_t n) { parts.push_back({p, n}); };
+        for (int d = 0; d < 2; ++d) {
+            add(h.val[d].data(), h.val[d].size() * 4);
+            add(h.valRank[d].data(), h.valRank[d].size() * 4);
+            add(h.src[d].data(), h.src[d].size() * 4);
+            add(h.srcRank[d].data(), h.srcRank[d].size() * 4);
+            add(h.rowKey[d].data(), h.rowKey[d].size() * 4);
+            add(h.rowBeg[d].data(), h.rowBeg[d].size() * 4);
+            add(h.predRow[d].data(), h.predRow[d].size() * 4);
+            add(h.predEdge[d].data(), h.predEdge[d].size() * 4);
+        }
+        add(h.hash.data(), h.hash.size() * sizeof(HashSlot));
+        size_t total = 0;
+        std::vector<size_t> off;
+        for (auto& pp : parts) {
+            off.push_back(total);
+            total += (pp.second + 255) & ~size_t(255);
+        }
+        size_t freeB = 0, totB = 0;
+        ck(cudaMemGetInfo(&freeB, &totB), "cudaMemGetInfo");
+        if (total + (64u << 20) > freeB)
+            throw CudaError("not enough device memory: need ~" + std::to_string((total >> 20) + 64) +
+                            " MB, " + std::to_string(freeB >> 20) + " MB free");
+        indexMem.ensure(std::max<size_t>(total, 256));
+        char* base = static_cast<char*>(indexMem.p);
+        for (size_t i = 0; i < parts.size(); ++i)
+            if (parts[i].second)
+                ck(cudaMemcpy(base + off[i], parts[i].first, parts[i].second, cudaMemcpyHostToDevice), "cudaMemcpy(index)");
+        size_t k = 0;
+        for (int d = 0; d < 2; ++d) {
+            dix.val[d] = reinterpret_cast<const int32_t*>(base + off[k++]);
+            dix.valRank[d] = reinterpret_cast<const int32_t*>(base + off[k++]);
+            dix.src[d] = reinterpret_cast<const int32_t*>(base + off[k++]);
+            dix.srcRank[d] = reinterpret_cast<const int32_t*>(base + off[k++]);
+            dix.rowKey[d] = reinterpret_cast<const int32_t*>(base + off[k++]);
+            dix.rowBeg[d] = reinterpret_cast<const int32_t*>(base + off[k++]);
+            dix.predRow[d] = reinterpret_cast<const int32_t*>(base + off[k++]);
+            dix.predEdge[d] = reinterpret_cast<const int32_t*>(base + off[k++]);
+        }
+        dix.hash = reinterpret_cast<const HashSlot*>(base + off[k++]);
+        dix.hashMask = h.hashMask;
+        dix.nPred = h.nPred;
+        dix.nEnt = h.nEnt;
+        dix.nTriples = h.nTriples;
+    }
+
+    bool set_block(int b) {
+        if (b != 128 && b != 256 && b != 512) return false;
+        geom.block = b;
+        grid = sms * (1024 / b);
+        return true;
+    }
+
+    void init_device() {
+        ck(cudaGetDevice(&device), "cudaGetDevice");
+        ck(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device), "cudaDeviceGetAttribute");
+        ck(engine_configure(), "cudaFuncSetAttribute");
+        if (const char* b = std::getenv("GPU_RULES_BLOCK")) set_block(std::atoi(b));
+        else set_block(geom.block);
+        ck(cudaStreamCreateWithFlags(&stream, cudaStreamNonBlocking), "cudaStreamCreate");
+        for (auto& e : ev) ck(cudaEventCreate(&e), "cudaEventCreate");
+    }
+};
+
+
+// A batch prepared once and replayed: parse, plan and upload happen at
+// preparation; a run is one CUDA-graph launch of the device work.
+struct Batch {
+    Context* c = nullptr;
+    int n = 0;
+    std::vector<RulePlan> rps;
+    std::vector<int> parseStatus;
+    std::vector<int> owner;  // plan -> rule * 2 + phase
+    std::vector<DevPlan> plans0;
+    std::vector<const PhasePlan*> phases;
+    Staged st;
+    cudaStream_t stream = nullptr;
+    cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+    cudaGraph_t graph = nullptr;
+    cudaGraphExec_t exec = nullptr;
+    DevBuf flush;
+    double lastMs = 0.0;
+
+    ~Batch() {
+        if (c) cudaSetDevice(c->device);
+        if (stream) cudaStreamSynchronize(stream);
+        if (exec) cudaGraphExecDestroy(exec);
+        if (graph) cudaGraphDestroy(graph);
+        if (ev0) cudaEventDestroy(ev0);
+        if (ev1) cudaEventDestroy(ev1);
+        if (stream) cudaStreamDestroy(stream);
+    }
+};
+
+
+inline void Context::free_pipe() {
+    for (Batch* b : pipe) delete b;
+    pipe.clear();
+}
+
+// Result fields from counts (FinalRule::setMeasures / setConfidence).
+void compose(const RulePlan& rp, int64_t sup, int64_t body, double supMs, double confMs, GpuRuleResult* out);
+
+}  // namespace gr

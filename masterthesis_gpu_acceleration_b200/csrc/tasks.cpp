@@ -199,6 +199,18 @@ void TaskBuilder::build(const std::vector<const PhasePlan*>& phases, int blocks,
         const int32_t R = ph.rootEnd - ph.rootBeg;
         const double uniform = R > 0 ? std::max(1.0, pt.work / R) : 1.0;
         const std::vector<float>* w = walked[i];
+        if (!w) {
+            // uniform cost per root: fixed-size chunks, no per-root pass
+            const double per = uniform * sc;
+            int32_t chunk = g;
+            if (per > 0 && per * chunk > target) chunk = std::max<int32_t>(1, (int32_t)(target / per));
+            for (int32_t b = ph.rootBeg; b < ph.rootEnd; b += chunk) {
+                const int32_t e = std::min(ph.rootEnd, b + chunk);
+                pt.tasks.push_back(DevTask{(int32_t)i, b, e, 0, 0, -1});
+                pt.cost.push_back(uniform * (e - b));
+            }
+            continue;
+        }
         int32_t gb = ph.rootBeg;
         double acc = 0, accUnits = 0;
         auto flush = [&](int32_t end) {

@@ -1,0 +1,84 @@
+"""Multi-rank host logic with two gloo processes on the CPU.
+
+The engine needs a GPU, but everything the multi-GPU layout adds around it
+runs on the host: each rank's data (same graph, own rule set), the slice of a
+shared rule list, the max-over-ranks timing that the benchmark reports, and
+the gather of per-rank results back into rule order.
+"""
+import hashlib
+import os
+import socket
+import sys
+
+import pytest
+import torch.multiprocessing as mp
+
+from conftest import ROOT
+from masterthesis_gpu_acceleration_b200 import shard
+
+
+def _free_port() -> int:
+    s = socket.socket()
+    s.bind(("127.0.0.1", 0))
+    p = s.getsockname()[1]
+    s.close()
+    return p
+
+
+def _worker(rank, world, port, data_dir, q):
+    sys.path.insert(0, str(ROOT))
+    import torch.distributed as dist
+    from masterthesis_gpu_acceleration_b200 import shard, synth
+    os.environ["MASTER_ADDR"] = "127.0.0.1"
+    os.environ["MASTER_PORT"] = str(port)
+    dist.init_process_group("gloo", rank=rank, world_size=world)
+    try:
+        d = synth.generate("c1", os.path.join(data_dir, f"r{rank}"), seed=0, rule_seed=shard.rule_seed(rank))
+        triples = hashlib.sha256((d / "triples.bin").read_bytes()).hexdigest()
+        rules = synth.read_rules(d)
+        # a per-rank "timed span": the reported value uses the slowest rank
+        span = 100.0 + 50.0 * rank
+        mx = shard.max_over_ranks(span)
+        # strong layout: slice a shared list and gather the slices back
+        shared = [f"rule{i}" for i in range(11)]
+        mine = shard.shard_rules(shared, rank, world)
+        parts = [None] * world
+        dist.all_gather_object(parts, [r.upper() for r in mine])
+        back = shard.gather_results(parts, len(shared), world)
+        q.put((rank, triples, rules, mx, back))
+    finally:
+        dist.destroy_process_group()
+
+
+def test_two_ranks_gloo(tmp_path):
+    world = 2
+    ctx = mp.get_context("spawn")
+    q = ctx.Queue()
+    port = _free_port()
+    procs = [ctx.Process(target=_worker, args=(r, world, port, str(tmp_path), q)) for r in range(world)]
+    for p in procs:
+        p.start()
+    out = {}
+    for _ in range(world):
+        rank, triples, rules, mx, back = q.get(timeout=120)
+        out[rank] = (triples, rules, mx, back)
+    for p in procs:
+        p.join(timeout=60)
+        assert p.exitcode == 0
+    assert out[0][0] == out[1][0], "ranks must share the graph"
+    assert out[0][1] != out[1][1], "ranks must evaluate different rule sets"
+    assert out[0][2] == out[1][2] == 150.0
+    assert out[0][3] == out[1][3] == [f"RULE{i}" for i in range(11)]
+    assert shard.weak_value(10000, 2, 5, 150.0) == pytest.approx(2 * 10000 * 5 / 0.15)
+
+
+def test_shard_bounds_cover_exactly():
+    for n in (0, 1, 7, 10000):
+        for world in (1, 2, 3, 8):
+            covered = []
+            for r in range(world):
+                lo, hi = shard.shard_bounds(n, r, world)
+                covered.extend(range(lo, hi))
+            assert covered == list(range(n))
+    with pytest.raises(ValueError):
+        shard.shard_bounds(10, 2, 2)

@@ -1,0 +1,104 @@
+"""The continuous-batching request loop (gpu_serve_*) on the GPU.
+
+Every served result must equal the reference's expected value and the same
+rule evaluated alone, whatever else was batched with it, however the
+requests arrived, and however tight the device-memory budget was.
+"""
+import threading
+import time
+
+import numpy as np
+import pytest
+
+import masterthesis_gpu_acceleration_b200 as eng
+from conftest import GOLDEN, load_fixture
+from masterthesis_gpu_acceleration_b200 import synth
+
+pytestmark = pytest.mark.gpu
+
+FIELDS = ("support", "headSize", "headSupport", "bodySize", "headCoverage", "confidence")
+
+
+def _collect(server, n, timeout=120.0):
+    got = {}
+    t0 = time.time()
+    while len(got) < n and time.time() - t0 < timeout:
+        for rid, st, res, lat in server.poll(wait_ms=50):
+            got[rid] = (st, res.as_dict(), lat)
+    assert len(got) == n, f"{len(got)} of {n} requests completed"
+    return got
+
+
+def test_serving_matches_reference_fuzz(tmp_path):
+    fx = load_fixture("fuzz_1.json")
+    p = tmp_path / "graph.ttl"
+    p.write_text(fx["ttl"])
+    with eng.GpuRulesLib(p) as lib:
+        with lib.serve(slots=3, max_batch=16) as sv:
+            for i, r in enumerate(fx["rules"]):
+                sv.submit(i, r)
+            got = _collect(sv, len(fx["rules"]))
+            assert sv.stats()["launches"] >= 2
+    for i, e in enumerate(fx["expected"]):
+        st, res, lat = got[i]
+        assert st == 0 and lat >= 0
+        assert {f: res[f] for f in FIELDS} == {f: e[f] for f in FIELDS}, i
+
+
+def test_serving_same_alone_and_in_the_mix(tmp_path):
+    d = synth.generate("c3", tmp_path / "c3", seed=0)
+    rules = synth.read_rules(d)[:3000]
+    exp = np.load(GOLDEN / "c3_seed0.npz")["expected"][:3000]
+    with eng.GpuRulesLib(d / "graph.ttl") as lib:
+        alone = [lib.evaluate_rule(r) for r in rules[::150]]
+        with lib.serve(slots=3, max_batch=512) as sv:
+            # two producers submit interleaved, in bursts, while results drain
+            def produce(ids):
+                for k, i in enumerate(ids):
+                    sv.submit(i, rules[i])
+                    if k % 97 == 0:
+                        time.sleep(0.002)
+            ts = [threading.Thread(target=produce, args=(list(range(j, len(rules), 2)),)) for j in (0, 1)]
+            for t in ts:
+                t.start()
+            got = _collect(sv, len(rules))
+            for t in ts:
+                t.join()
+            stats = sv.stats()
+    assert stats["launches"] > 1
+    for i in range(len(rules)):
+        st, res, _ = got[i]
+        assert st == 0
+        assert [res["support"], res["headSize"], res["headSupport"], res["bodySize"]] == exp[i].tolist(), i
+    for k, a in enumerate(alone):
+        assert {f: getattr(a, f) for f in FIELDS} == {f: got[150 * k][1][f] for f in FIELDS}
+
+
+def test_serving_tight_memory_budget_queues_requests(tmp_path):
+    fx = load_fixture("fuzz_4.json")
+    p = tmp_path / "graph.ttl"
+    p.write_text(fx["ttl"])
+    with eng.GpuRulesLib(p) as lib:
+        with lib.serve(slots=2, max_batch=1024, mem_budget=8192) as sv:
+            for i, r in enumerate(fx["rules"]):
+                sv.submit(i, r)
+            got = _collect(sv, len(fx["rules"]))
+            launches = sv.stats()["launches"]
+    assert launches > 10, "a small budget must split the requests over many launches"
+    for i, e in enumerate(fx["expected"]):
+        st, res, _ = got[i]
+        assert st == 0
+        assert {f: res[f] for f in FIELDS} == {f: e[f] for f in FIELDS}, i
+
+
+def test_serving_reports_bad_rules(tmp_path):
+    fx = load_fixture("edge_cases.json")
+    p = tmp_path / "graph.ttl"
+    p.write_text(fx["ttl"])
+    with eng.GpuRulesLib(p) as lib:
+        with lib.serve() as sv:
+            sv.submit(1, "not a rule")
+            sv.submit(2, fx["cases"][0]["rule"])
+            got = _collect(sv, 2)
+    assert got[1][0] == -1
+    assert got[2][0] == 0 and got[2][1]["bodySize"] == fx["cases"][0]["expected"]["bodySize"]
