@@ -59,6 +59,8 @@ def parse_args():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-per-rule", action="store_true")
     ap.add_argument("--max-rules", type=int, default=0, help="use only the first N rules (profiling case)")
+    ap.add_argument("--serve-seconds", type=float, default=1.5, help="seconds per offered rate in the serving sweep")
+    ap.add_argument("--no-serve", action="store_true")
     ap.add_argument("--data", default=os.environ.get("KG_DATA_DIR", str(Path(tempfile.gettempdir()) / "kg_synth_data")))
     return ap.parse_args()
 
@@ -160,6 +162,67 @@ def cpu_baseline(d: Path, rules: list[str], timeout: float = 300.0) -> dict:
             kind = "port"
     return {"value": len(sample) / secs, "unit": "rules/s", "cores": 1, "kind": kind, "sample": desc,
             "seconds": secs}
+
+
+def _oracle_worker(triples_path, n_pred, irs, q):
+    import numpy as np
+    sys.path.insert(0, str(ROOT))
+    import oracle
+    g = oracle.OracleGraph(np.fromfile(triples_path, dtype=np.int32).reshape(-1, 3), n_pred)
+    for k, ir in enumerate(irs):
+        counts, _ = g.evaluate_ir(np.asarray(ir, dtype=np.int32), 1)
+        q.put((k, counts[0].tolist()))
+
+
+def check_sample(graph_dir: Path, stream_dir: Path, results: dict, n_pred: int, every: int = 100,
+                 timeout: float = 60.0) -> dict:
+    """Bit-exact check of every `every`-th served request against the C oracle
+    (a separate process; rules it cannot finish within `timeout` stay unchecked)."""
+    import multiprocessing as mp
+    import oracle
+    from masterthesis_gpu_acceleration_b200 import synth
+    irs_all = oracle.split_ir(synth.read_rule_ir(stream_dir))
+    ids = sorted(results)[::every]
+    picks = [(rid, results[rid]) for rid in ids if results[rid][1] == 0]
+    irs = [irs_all[ri].tolist() for _, (ri, _, _) in picks]
+    ctx = mp.get_context("spawn")
+    q = ctx.Queue()
+    p = ctx.Process(target=_oracle_worker, args=(str(graph_dir / "triples.bin"), n_pred, irs, q))
+    p.start()
+    got = {}
+    t0 = time.time()
+    while len(got) < len(irs) and time.time() - t0 < timeout:
+        try:
+            k, c = q.get(timeout=max(0.1, timeout - (time.time() - t0)))
+            got[k] = c
+        except Exception:
+            break
+    if p.is_alive():
+        p.kill()
+    p.join()
+    bad = 0
+    for k, c in got.items():
+        res = picks[k][1][2]
+        if [res.support, res.headSize, res.headSupport, res.bodySize] != c:
+            bad += 1
+    return {"sampled": len(picks), "checked": len(got), "mismatches": bad, "exact": bad == 0 and len(got) > 0}
+
+
+def serving_sweep(lib, d: Path, args) -> dict:
+    """C5-shaped requests (chain rules, geometric(0.4) lengths up to 8,
+    predicates by frequency) on the resident c3 graph at swept Poisson rates."""
+    from masterthesis_gpu_acceleration_b200 import serving, synth
+    n_pred = int(synth.read_meta(d)["predicates"])
+    pc = synth.pred_counts(synth.read_triples(d), n_pred)
+    sd = synth.rule_stream(pc, 20000, Path(args.data) / "c5_stream", p=0.4, max_len=8, seed=1)
+    rules = synth.read_rules(sd)
+    rates = [1000, 5000, 20000, 50000]
+    rows, res = serving.sweep(lib, rules, rates, duration=args.serve_seconds, seed=11)
+    check = check_sample(d, sd, res, n_pred)
+    return {"workload": "c5-shaped stream on the c3 graph: 20,000 chain rules, lengths geometric(0.4) in 1..8, "
+                        "predicates by frequency, open-loop Poisson arrivals",
+            "seconds_per_rate": args.serve_seconds, "slots": "4 (3 light + 1 heavy lane)", "rates": rows,
+            "oracle_check_1pct": check}
 
 
 def reference_arm(args):
@@ -308,6 +371,10 @@ def engine_arm(args):
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         cpu = cpu_baseline(d, rules)
 
+    serving = None
+    if rank == 0 and world == 1 and not args.no_serve:
+        serving = serving_sweep(lib, d, args)
+
     batch.close()
     lib.close()
     if rank == 0:
@@ -321,6 +388,7 @@ def engine_arm(args):
                        "exact_vs_reference_golden": exact, "plans": info["plans"], "tasks": info["tasks"]},
             "e2e": e2e,
             "per_rule": per_rule,
+            "serving": serving,
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": peaks["hbm_gbs"], "unit": "GB/s",
                          "frac": achieved / peaks["hbm_gbs"], "traffic": traffic,
                          "algorithmic_bytes_per_launch": alg_bytes, "peak_source": peaks["source"] + " (burst copy)"},

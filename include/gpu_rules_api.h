@@ -137,7 +137,11 @@ int gpu_evaluate_rule_noalloc(void* ctx, const char* ruleText, GpuRuleResult* ou
  * variable GPU_RULES_BLOCK sets it at load).  "task_target": fixed work per
  * task in candidate bindings (0 = automatic balancing).  "walk_threshold":
  * estimated work above which a phase's roots are measured one by one before
- * splitting (default 200000).  Returns 0, or -1 for an unknown name or
+ * splitting (default 200000).  Servers started afterwards: "serve_lanes"
+ * (1: keep a heavy lane, default; 0: all slots alike), "serve_heavy_share"
+ * (the heavy lane launches on 1/share of the blocks, default 2) and
+ * "serve_heavy_us" (expected device time in microseconds above which a
+ * request is heavy, default 5000).  Returns 0, or -1 for an unknown name or
  * value. */
 int gpu_set_option(void* ctx, const char* name, long long value);
 
@@ -156,11 +160,18 @@ typedef struct {
 /* Starts a request loop on a loaded graph: a worker thread with `slots`
  * launch slots (streams, 1..16), at most maxBatch rules per launch, and at
  * most memBudgetBytes of estimated device memory (plans, tasks, dedup
- * buffers) held by launches in flight.  Whenever a slot is free, the waiting
- * requests are admitted in arrival order while their memory fits and are
- * launched together without waiting for the other slots, so requests that
- * arrive while others run are batched onto the GPU as slots and memory free
- * up.  While a server runs, its context must not be used by other calls.
+ * buffers) held by launches in flight.  The worker plans requests as they
+ * arrive.  Whenever a slot is free, the waiting requests are admitted in
+ * arrival order while their memory fits and are launched together without
+ * waiting for the other slots, so requests that arrive while others run are
+ * batched onto the GPU as slots and memory free up.  With two or more slots
+ * the last one serves requests whose expected device time is long (heavy
+ * lane), launched on half of the SMs so that they never hold the whole
+ * GPU; when heavy work piles up and no light request waits, the other
+ * slots take heavy requests too.  Every launch records its task times, from
+ * which the context learns each plan shape's cost (later launches, and
+ * later batches on the same context, split slow shapes finer).  While a
+ * server runs, its context must not be used by other calls.
  * Returns a server handle or NULL. */
 void* gpu_serve_start(void* ctx, int slots, int maxBatch, long long memBudgetBytes);
 
@@ -172,10 +183,11 @@ int gpu_serve_submit(void* server, long long requestId, const char* ruleText);
  * first one.  Thread-safe.  Returns the number copied, or -1. */
 int gpu_serve_poll(void* server, GpuServeResult* out, int max, int waitMs);
 
-/* Requests submitted and completed, launches issued and device memory
- * currently held by launches in flight. */
+/* Requests submitted and completed, launches issued, device memory
+ * currently held by launches in flight, the summed device span of the
+ * completed launches and the worker's summed host preparation time. */
 int gpu_serve_stats(void* server, long long* submitted, long long* completed, long long* launches,
-                    long long* memInUse);
+                    long long* memInUse, double* deviceMs, double* hostMs);
 
 /* Finishes every queued request, stops the worker and frees the server
  * (uncollected results are dropped).  NULL is ignored. */

@@ -134,7 +134,8 @@ def load_library(path: os.PathLike | str | None = None) -> ctypes.CDLL:
     lib.gpu_serve_poll.restype = ctypes.c_int
     lib.gpu_serve_poll.argtypes = [ctypes.c_void_p, ctypes.POINTER(GpuServeResult), ctypes.c_int, ctypes.c_int]
     lib.gpu_serve_stats.restype = ctypes.c_int
-    lib.gpu_serve_stats.argtypes = [ctypes.c_void_p] + [ctypes.POINTER(ctypes.c_longlong)] * 4
+    lib.gpu_serve_stats.argtypes = [ctypes.c_void_p] + [ctypes.POINTER(ctypes.c_longlong)] * 4 + \
+        [ctypes.POINTER(ctypes.c_double)] * 2
     lib.gpu_serve_stop.restype = None
     lib.gpu_serve_stop.argtypes = [ctypes.c_void_p]
     lib.gpu_graph_stats.restype = ctypes.c_int
@@ -353,9 +354,10 @@ class GpuServer:
         return out
 
     def stats(self) -> dict:
-        v = [ctypes.c_longlong() for _ in range(4)]
+        v = [ctypes.c_longlong() for _ in range(4)] + [ctypes.c_double() for _ in range(2)]
         self._lib.gpu_serve_stats(self._h, *[ctypes.byref(x) for x in v])
-        return dict(zip(("submitted", "completed", "launches", "mem_in_use"), (x.value for x in v)))
+        return dict(zip(("submitted", "completed", "launches", "mem_in_use", "device_ms", "host_ms"),
+                        (x.value for x in v)))
 
     def stop(self) -> None:
         if getattr(self, "_h", None) is not None:

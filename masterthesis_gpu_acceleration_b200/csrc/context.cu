@@ -36,7 +36,7 @@ void set_error(const std::string& s) {
 }
 
 void Staged::stage(Context& c, std::vector<DevPlan>& plans, const std::vector<const PhasePlan*>& phases,
-                   bool sortTasks, cudaStream_t s) {
+                   bool sortTasks, cudaStream_t s, double walkBudget) {
     nPlans = (int)plans.size();
     nTasks = 0;
     bitmapWords = 0;
@@ -49,9 +49,10 @@ void Staged::stage(Context& c, std::vector<DevPlan>& plans, const std::vector<co
         gOff[i] = bitmapWords;
         bitmapWords += (rows * (size_t)plans[i].wo + 31) / 32;
     }
-    if (bitmapWords) dBitmap.ensure(bitmapWords * 4);
+    cudaStream_t as = streamOrdered ? s : nullptr;
+    if (bitmapWords) dBitmap.ensure(bitmapWords * 4, as);
     std::vector<PhaseTasks> pts;
-    c.tasks->build(phases, c.grid, true, pts);
+    c.tasks->build(phases, c.grid, true, pts, walkBudget);
     std::vector<size_t> hOff(nPlans, 0);
     heavyWords = 0;
     for (int i = 0; i < nPlans; ++i) {
@@ -59,7 +60,7 @@ void Staged::stage(Context& c, std::vector<DevPlan>& plans, const std::vector<co
         hOff[i] = heavyWords;
         heavyWords += (size_t)pts[i].heavyRows * plans[i].rowWords;
     }
-    if (heavyWords) dHeavy.ensure(heavyWords * 4);
+    if (heavyWords) dHeavy.ensure(heavyWords * 4, as);
     std::vector<DevTask> tasks;
     std::vector<double> cost;
     for (int i = 0; i < nPlans; ++i) {
@@ -92,9 +93,9 @@ void Staged::stage(Context& c, std::vector<DevPlan>& plans, const std::vector<co
     hBlob.ensure(blob);
     std::memcpy(hBlob.p, plans.data(), planBytes);
     std::memcpy(static_cast<char*>(hBlob.p) + planBytes, tasks.data(), taskBytes);
-    dBlob.ensure(blob);
-    dResults.ensure((size_t)nPlans * sizeof(unsigned long long));
-    dCtl.ensure(64);
+    dBlob.ensure(blob, as);
+    dResults.ensure((size_t)nPlans * sizeof(unsigned long long), as);
+    dCtl.ensure(64, as);
     hResults.ensure((size_t)nPlans * sizeof(unsigned long long));
     hCtl.ensure(64);
     ck(cudaMemcpyAsync(dBlob.p, hBlob.p, blob, cudaMemcpyHostToDevice, s), "H2D plans");
@@ -104,24 +105,26 @@ void Staged::stage(Context& c, std::vector<DevPlan>& plans, const std::vector<co
     d2hBytes = (size_t)nPlans * sizeof(unsigned long long) + 8;
 }
 
-void Staged::enqueue(Context& c, cudaStream_t s, bool profile) {
+void Staged::enqueue(Context& c, cudaStream_t s, int instr, int gridCap) {
     if (!nPlans) return;
     ck(cudaMemsetAsync(dResults.p, 0, (size_t)nPlans * sizeof(unsigned long long), s), "memset results");
     ck(cudaMemsetAsync(dCtl.p, 0, 8, s), "memset ctl");
     if (bitmapWords) ck(cudaMemsetAsync(dBitmap.p, 0, bitmapWords * 4, s), "memset bitmap");
     if (heavyWords) ck(cudaMemsetAsync(dHeavy.p, 0, heavyWords * 4, s), "memset heavy rows");
     EngineProfile prof;
-    if (profile) {
-        dBytes.ensure(8);
-        dTaskNs.ensure((size_t)std::max(nTasks, 1) * 16);
-        ck(cudaMemsetAsync(dBytes.p, 0, 8, s), "memset bytes");
-        prof.bytes = static_cast<unsigned long long*>(dBytes.p);
+    if (instr >= 1) {
+        dTaskNs.ensure((size_t)std::max(nTasks, 1) * 16, streamOrdered ? s : nullptr);
         prof.taskNs = static_cast<unsigned long long*>(dTaskNs.p);
     }
-    int grid = std::max(1, std::min(nTasks, c.grid));
+    if (instr >= 2) {
+        dBytes.ensure(8, streamOrdered ? s : nullptr);
+        ck(cudaMemsetAsync(dBytes.p, 0, 8, s), "memset bytes");
+        prof.bytes = static_cast<unsigned long long*>(dBytes.p);
+    }
+    int grid = std::max(1, std::min(nTasks, gridCap > 0 ? std::min(gridCap, c.grid) : c.grid));
     ck(engine_launch(c.dix, dPlans, dTasks, nTasks, static_cast<int*>(dCtl.p),
                      static_cast<unsigned long long*>(dResults.p), static_cast<int*>(dCtl.p) + 1, grid,
-                     c.geom.block, s, profile ? &prof : nullptr),
+                     c.geom.block, s, instr ? &prof : nullptr),
        "engine launch");
 }
 
@@ -147,7 +150,7 @@ int64_t run_one_phase(Context& c, const PhasePlan& ph, float* ms) {
     std::vector<DevPlan> plans{ph.plan};
     c.one.stage(c, plans, {&ph}, false, c.stream);
     ck(cudaEventRecord(c.ev[0], c.stream), "event");
-    c.one.enqueue(c, c.stream, false);
+    c.one.enqueue(c, c.stream, 0);
     ck(cudaEventRecord(c.ev[1], c.stream), "event");
     c.one.download(c.stream);
     ck(cudaStreamSynchronize(c.stream), "engine");
@@ -197,7 +200,7 @@ void prepare(Batch& b, Context& c, const char* const* rules, int n, int isJson) 
     if (!b.ev1) ck(cudaEventCreate(&b.ev1), "cudaEventCreate");
     b.plans0 = plans;
     b.phases = phases;
-    b.st.stage(c, plans, phases, true, b.stream);
+    b.st.stage(c, plans, phases, true, b.stream, b.walkBudget);
 }
 
 void collect(const Batch& b, GpuRuleResult* out, int* status) {
@@ -226,13 +229,13 @@ void run_batch(Batch& b, bool useGraph, size_t flushBytes) {
     }
     if (useGraph && !b.exec && b.st.nPlans) {
         ck(cudaStreamBeginCapture(b.stream, cudaStreamCaptureModeThreadLocal), "capture");
-        b.st.enqueue(c, b.stream, false);
+        b.st.enqueue(c, b.stream, 0);
         ck(cudaStreamEndCapture(b.stream, &b.graph), "capture end");
         ck(cudaGraphInstantiate(&b.exec, b.graph, 0), "graph instantiate");
     }
     ck(cudaEventRecord(b.ev0, b.stream), "event");
     if (useGraph && b.exec) ck(cudaGraphLaunch(b.exec, b.stream), "graph launch");
-    else b.st.enqueue(c, b.stream, false);
+    else b.st.enqueue(c, b.stream, 0);
     ck(cudaEventRecord(b.ev1, b.stream), "event");
     b.st.download(b.stream);
     ck(cudaStreamSynchronize(b.stream), "engine");
@@ -342,7 +345,7 @@ int gpu_evaluate_rules_batch(void* ctx, const char* const* rules, int n, int isJ
             Batch& b = *c.pipe[k];
             prepare(b, c, rules + lo, hi - lo, isJson);
             ck(cudaEventRecord(b.ev0, b.stream), "event");
-            b.st.enqueue(c, b.stream, false);
+            b.st.enqueue(c, b.stream, 0);
             ck(cudaEventRecord(b.ev1, b.stream), "event");
             b.st.download(b.stream);
         }
@@ -372,6 +375,7 @@ void* gpu_batch_prepare(void* ctx, const char* const* rules, int n, int isJson) 
     try {
         cudaSetDevice(c.device);
         b = new Batch();
+        b->walkBudget = 4.0e7;   // prepared once, replayed many times
         prepare(*b, c, rules, n, isJson);
         ck(cudaStreamSynchronize(b->stream), "stage");
         return b;
@@ -419,7 +423,7 @@ int gpu_batch_profile(void* batch, unsigned long long* bytes, unsigned long long
         cudaSetDevice(b.c->device);
         if (bytes) *bytes = 0;
         if (!b.st.nPlans) return 0;
-        b.st.enqueue(*b.c, b.stream, true);
+        b.st.enqueue(*b.c, b.stream, 2);
         unsigned long long by = 0;
         ck(cudaMemcpyAsync(&by, b.st.dBytes.p, 8, cudaMemcpyDeviceToHost, b.stream), "D2H bytes");
         long long n = std::min<long long>(maxTasks, b.st.nTasks);
@@ -448,7 +452,7 @@ int gpu_batch_autotune(void* batch, int rounds) {
         Context& c = *b.c;
         cudaSetDevice(c.device);
         for (int r = 0; r < rounds && b.st.nPlans; ++r) {
-            b.st.enqueue(c, b.stream, true);
+            b.st.enqueue(c, b.stream, 1);
             std::vector<unsigned long long> ns(2 * (size_t)b.st.nTasks);
             ck(cudaMemcpyAsync(ns.data(), b.st.dTaskNs.p, ns.size() * 8, cudaMemcpyDeviceToHost, b.stream), "D2H task times");
             ck(cudaStreamSynchronize(b.stream), "autotune");
@@ -456,7 +460,7 @@ int gpu_batch_autotune(void* batch, int rounds) {
             if (b.exec) { cudaGraphExecDestroy(b.exec); b.exec = nullptr; }
             if (b.graph) { cudaGraphDestroy(b.graph); b.graph = nullptr; }
             std::vector<DevPlan> pl = b.plans0;
-            b.st.stage(c, pl, b.phases, true, b.stream);
+            b.st.stage(c, pl, b.phases, true, b.stream, b.walkBudget);
             ck(cudaStreamSynchronize(b.stream), "restage");
         }
         return 0;
@@ -473,6 +477,9 @@ int gpu_set_option(void* ctx, const char* name, long long value) {
     if (n == "block") return c.set_block((int)value) ? 0 : -1;
     if (n == "task_target" && value >= 0) { c.tasks->forceTarget = (double)value; return 0; }
     if (n == "walk_threshold" && value >= 0) { c.tasks->walkThreshold = (double)value; return 0; }
+    if (n == "serve_lanes" && (value == 0 || value == 1)) { c.serveLanes = (int)value; return 0; }
+    if (n == "serve_heavy_share" && value >= 1 && value <= 16) { c.serveHeavyShare = (int)value; return 0; }
+    if (n == "serve_heavy_us" && value >= 0) { c.serveHeavyNs = 1e3 * (double)value; return 0; }
     return -1;
 }
 

@@ -43,15 +43,30 @@ inline void ck(cudaError_t e, const char* what) {
 struct DevBuf {
     void* p = nullptr;
     size_t cap = 0;
-    void ensure(size_t bytes) {
+    bool pooled = false;   // from the stream-ordered allocator
+    // Grows by half again: cudaFree synchronises the device, so resizing
+    // must be rare when request sizes vary.  With a stream, the old buffer
+    // is freed and the new one allocated in that stream's order (no device
+    // synchronisation); the buffer must then only be used on that stream.
+    void ensure(size_t bytes, cudaStream_t s = nullptr) {
         if (bytes <= cap) return;
-        release();
-        size_t want = std::max<size_t>(bytes, 4096);
-        ck(cudaMalloc(&p, want), "cudaMalloc");
+        size_t want = std::max<size_t>(bytes + bytes / 2, 4096);
+        if (s) {
+            if (p && pooled) ck(cudaFreeAsync(p, s), "cudaFreeAsync");
+            else release();
+            p = nullptr;
+            cap = 0;
+            ck(cudaMallocAsync(&p, want, s), "cudaMallocAsync");
+            pooled = true;
+        } else {
+            release();
+            ck(cudaMalloc(&p, want), "cudaMalloc");
+            pooled = false;
+        }
         cap = want;
     }
     void release() {
-        if (p) cudaFree(p);
+        if (p) cudaFree(p);   // also frees pooled memory, after a synchronisation
         p = nullptr;
         cap = 0;
     }
@@ -64,7 +79,7 @@ struct HostBuf {  // pinned
     void ensure(size_t bytes) {
         if (bytes <= cap) return;
         release();
-        size_t want = std::max<size_t>(bytes, 4096);
+        size_t want = std::max<size_t>(bytes + bytes / 2, 4096);
         ck(cudaMallocHost(&p, want), "cudaMallocHost");
         cap = want;
     }
@@ -92,10 +107,31 @@ struct Staged {
     int nPlans = 0, nTasks = 0;
     size_t bitmapWords = 0, heavyWords = 0;
     size_t h2dBytes = 0, d2hBytes = 0;
+    bool streamOrdered = false;   // grow device buffers on the launch stream (serving slots)
 
+    // walkBudget: how much per-root measurement the task builder may do
+    // (prepared batches afford more than one-shot or served launches).
     void stage(Context& c, std::vector<DevPlan>& plans, const std::vector<const PhasePlan*>& phases,
-               bool sortTasks, cudaStream_t s);
-    void enqueue(Context& c, cudaStream_t s, bool profile);
+               bool sortTasks, cudaStream_t s, double walkBudget = 4.0e6);
+    // instr: 0 plain, 1 task times into dTaskNs, 2 also algorithmic bytes
+    // into dBytes.  gridCap > 0 limits the launch to that many blocks (a
+    // share of the SMs).
+    void enqueue(Context& c, cudaStream_t s, int instr, int gridCap = 0);
+    // Pre-sizes the buffers so that launches up to this size never resize
+    // (freeing device or pinned memory synchronises the whole device).
+    void reserve(size_t plans, size_t tasks, cudaStream_t s = nullptr) {
+        const size_t blob = plans * sizeof(DevPlan) + tasks * sizeof(DevTask);
+        dBlob.ensure(blob, s);
+        hBlob.ensure(blob);
+        dResults.ensure(plans * sizeof(unsigned long long), s);
+        hResults.ensure(plans * sizeof(unsigned long long));
+        dCtl.ensure(64, s);
+        hCtl.ensure(64);
+        dHeavy.ensure(1 << 20, s);
+        dBitmap.ensure(1 << 20, s);
+        dBytes.ensure(8, s);
+        dTaskNs.ensure(tasks * 16, s);
+    }
     void download(cudaStream_t s) {
         if (!nPlans) return;
         ck(cudaMemcpyAsync(hResults.p, dResults.p, nPlans * sizeof(unsigned long long), cudaMemcpyDeviceToHost, s), "D2H results");
@@ -121,6 +157,9 @@ struct Context {
     std::vector<struct Batch*> pipe;  // reusable chunks of one-shot batches
     std::unique_ptr<TaskBuilder> tasks;
     Geom geom;
+    int serveLanes = 1;        // servers started on this context keep a heavy lane
+    int serveHeavyShare = 2;   // the heavy lane launches on grid / serveHeavyShare blocks
+    double serveHeavyNs = 5.0e6;
     int grid = 0;
     int sms = 0;
     std::unique_ptr<RuleParser> parser;
@@ -219,6 +258,7 @@ struct Batch {
     cudaGraphExec_t exec = nullptr;
     DevBuf flush;
     double lastMs = 0.0;
+    double walkBudget = 4.0e6;
 
     ~Batch() {
         if (c) cudaSetDevice(c->device);

@@ -458,10 +458,13 @@ __device__ __forceinline__ unsigned long long global_ns() {
     return t;
 }
 
-template <int B, bool kC>
+// kI: 0 plain; 1 records each task's start and end time; 2 also counts
+// the algorithmic bytes.
+template <int B, int kI>
 __global__ void __launch_bounds__(B, 1024 / B)
 engine_kernel(DevIndex ix, const DevPlan* __restrict__ plans, const DevTask* __restrict__ tasks,
               int nTasks, int* taskCounter, unsigned long long* results, int* status, EngineProfile prof) {
+    constexpr bool kC = kI == 2;
     extern __shared__ __align__(16) unsigned char smem_raw[];
     Smem<B>& sm = *reinterpret_cast<Smem<B>*>(smem_raw);
     Meter<kC> mt;
@@ -472,7 +475,7 @@ engine_kernel(DevIndex ix, const DevPlan* __restrict__ plans, const DevTask* __r
         if (t >= nTasks) break;
         const DevTask task = tasks[t];
         unsigned long long t0 = 0;
-        if constexpr (kC) {
+        if constexpr (kI >= 1) {
             if (threadIdx.x == 0) {
                 mt.add(sizeof(DevTask) + sizeof(DevPlan) + 8);
                 t0 = global_ns();
@@ -484,7 +487,7 @@ engine_kernel(DevIndex ix, const DevPlan* __restrict__ plans, const DevTask* __r
         __syncthreads();
         run_task<B, kC>(sm, ix, task, results, status, mt);
         __syncthreads();
-        if constexpr (kC) {
+        if constexpr (kI >= 1) {
             if (threadIdx.x == 0 && prof.taskNs) {
                 prof.taskNs[2 * t] = t0;
                 prof.taskNs[2 * t + 1] = global_ns();
@@ -500,11 +503,13 @@ engine_kernel(DevIndex ix, const DevPlan* __restrict__ plans, const DevTask* __r
 
 template <int B>
 static cudaError_t configure_b() {
-    cudaError_t e = cudaFuncSetAttribute(engine_kernel<B, false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                         (int)sizeof(Smem<B>));
-    if (e != cudaSuccess) return e;
-    return cudaFuncSetAttribute(engine_kernel<B, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                (int)sizeof(Smem<B>));
+    const int smem = (int)sizeof(Smem<B>);
+    cudaError_t e = cudaFuncSetAttribute(engine_kernel<B, 0>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+    if (e == cudaSuccess)
+        e = cudaFuncSetAttribute(engine_kernel<B, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+    if (e == cudaSuccess)
+        e = cudaFuncSetAttribute(engine_kernel<B, 2>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+    return e;
 }
 
 size_t engine_smem_bytes(int block) {
@@ -526,15 +531,18 @@ template <int B>
 static void launch_b(const DevIndex& ix, const DevPlan* plans, const DevTask* tasks, int nTasks, int* taskCounter,
                      unsigned long long* results, int* status, int grid, cudaStream_t stream,
                      const EngineProfile* prof) {
-    if (prof)
-        engine_kernel<B, true><<<grid, B, sizeof(Smem<B>), stream>>>(ix, plans, tasks, nTasks, taskCounter, results,
-                                                                     status, *prof);
+    const size_t smem = sizeof(Smem<B>);
+    if (prof && prof->bytes)
+        engine_kernel<B, 2><<<grid, B, smem, stream>>>(ix, plans, tasks, nTasks, taskCounter, results, status, *prof);
+    else if (prof)
+        engine_kernel<B, 1><<<grid, B, smem, stream>>>(ix, plans, tasks, nTasks, taskCounter, results, status, *prof);
     else
-        engine_kernel<B, false><<<grid, B, sizeof(Smem<B>), stream>>>(ix, plans, tasks, nTasks, taskCounter, results,
-                                                                      status, EngineProfile{});
+        engine_kernel<B, 0><<<grid, B, smem, stream>>>(ix, plans, tasks, nTasks, taskCounter, results, status,
+                                                       EngineProfile{});
 }
 
-// prof != null selects the profiling variant (byte counts, task times).
+// prof != null selects an instrumented variant: task times, and byte counts
+// when prof->bytes is set.
 cudaError_t engine_launch(const DevIndex& ix, const DevPlan* plans, const DevTask* tasks, int nTasks,
                           int* taskCounter, unsigned long long* results, int* status, int grid, int block,
                           cudaStream_t stream, const EngineProfile* prof) {

@@ -10,8 +10,7 @@ namespace gr {
 namespace {
 
 constexpr double kMinTarget = 4096.0;
-constexpr double kWalkBudget = 4.0e7;     // first-segment edges walked per batch
-constexpr size_t kCacheLimit = 256u << 20;
+constexpr size_t kCacheLimit = size_t(2) << 30;
 
 int64_t pd_key(int32_t pred, int dir) { return (int64_t)pred * 2 + dir; }
 
@@ -72,6 +71,49 @@ double TaskBuilder::estimate(const PhasePlan& ph, bool hubAware) {
     return w;
 }
 
+const TaskBuilder::Hop2& TaskBuilder::hop2(int32_t p0, int d0, int32_t p1, int d1) {
+    const uint64_t key = ((uint64_t)(uint32_t)p0 << 33) | ((uint64_t)d0 << 32) | ((uint64_t)(uint32_t)p1 << 1) | (uint64_t)d1;
+    auto it = hop2_.find(key);
+    if (it != hop2_.end()) return it->second;
+    const int32_t* deg = degrees(p1, d1);
+    Hop2 h;
+    const int32_t r0 = ix_.predRow[d0][p0], r1 = ix_.predRow[d0][p0 + 1];
+    h.perRow.resize((size_t)(r1 - r0));
+    for (int32_t r = r0; r < r1; ++r) {
+        double acc = 0;
+        for (int32_t e = ix_.rowBeg[d0][r]; e < ix_.rowBeg[d0][r + 1]; ++e) acc += deg[ix_.val[d0][e]];
+        h.perRow[r - r0] = (float)acc;
+        h.total += acc;
+    }
+    cacheBytes_ += h.perRow.size() * sizeof(float);
+    return hop2_.emplace(key, std::move(h)).first->second;
+}
+
+bool TaskBuilder::chain_shaped(const DevPlan& P) const {
+    return P.m >= 2 && P.steps[0].kind == kExpand && P.steps[1].kind == kExpand &&
+           P.steps[1].keyRef == P.tupleLen[0] && (P.steps[0].keyRef < 0 || P.steps[0].keyRef < P.tupleLen[0]);
+}
+
+double TaskBuilder::estimate2(const PhasePlan& ph) {
+    const DevPlan& P = ph.plan;
+    if (!chain_shaped(P)) return estimate(ph, false);
+    const DevStep& s0 = P.steps[0];
+    const DevStep& s1 = P.steps[1];
+    double tail = 1.0;
+    for (int s = 2; s < P.m; ++s) tail *= std::max(1.0, avg_fan(P.steps[s]));
+    const Hop2& h = hop2(s0.pred, s0.dir, s1.pred, s1.dir);
+    const bool allRows = P.rootKind == kRootRows && P.rootDir == s0.dir && P.rootPred == s0.pred &&
+                         s0.keyRef == kTupleHead && ph.rootBeg == ix_.predRow[s0.dir][s0.pred] &&
+                         ph.rootEnd == ix_.predRow[s0.dir][s0.pred + 1];
+    if (allRows)
+        return (double)(ph.rootEnd - ph.rootBeg) + (double)ix_.pred_size(s0.pred) + h.total * tail;
+    // other roots: average first fan-out, and the transition's exact mean
+    // second degree per first-level edge
+    const double e0 = (double)std::max<int64_t>(1, ix_.pred_size(s0.pred));
+    const double fan0 = std::max(1.0, ix_.avg_degree(s0.pred, s0.dir));
+    return (double)(ph.rootEnd - ph.rootBeg) * (1.0 + fan0 * (1.0 + (h.total / e0) * tail));
+}
+
 int TaskBuilder::root_vals(const DevPlan& P, int32_t r, int32_t* vals) const {
     int nv = 0;
     if (P.rootKind == kRootRows) {
@@ -120,7 +162,9 @@ const std::vector<float>& TaskBuilder::walk(const PhasePlan& ph) {
     const DevPlan& P = ph.plan;
     double tail = 1.0;
     for (int s = 2; s < P.m; ++s) tail *= std::max(1.0, avg_fan(P.steps[s]));
-    const int32_t* deg2 = (P.m >= 2 && P.steps[1].kind == kExpand) ? degrees(P.steps[1].pred, P.steps[1].dir) : nullptr;
+    const bool chain = chain_shaped(P);
+    const Hop2* h = chain ? &hop2(P.steps[0].pred, P.steps[0].dir, P.steps[1].pred, P.steps[1].dir) : nullptr;
+    const int32_t* deg2 = (!chain && P.m >= 2 && P.steps[1].kind == kExpand) ? degrees(P.steps[1].pred, P.steps[1].dir) : nullptr;
     std::vector<float> w((size_t)(ph.rootEnd - ph.rootBeg));
     int32_t vals[2];
     for (int32_t r = ph.rootBeg; r < ph.rootEnd; ++r) {
@@ -128,7 +172,10 @@ const std::vector<float>& TaskBuilder::walk(const PhasePlan& ph) {
         auto seg = first_segment(P, vals);
         double acc = 1.0;
         if (P.m < 2) acc += seg.second - seg.first;
-        else
+        else if (chain) {
+            acc += seg.second - seg.first;
+            if (seg.second > seg.first) acc += h->perRow[ix_.srcRank[P.steps[0].dir][seg.first]] * tail;
+        } else
             for (int32_t e = seg.first; e < seg.second; ++e) acc += child_work(P, vals, e, deg2, tail);
         w[r - ph.rootBeg] = (float)acc;
     }
@@ -137,19 +184,20 @@ const std::vector<float>& TaskBuilder::walk(const PhasePlan& ph) {
 }
 
 void TaskBuilder::build(const std::vector<const PhasePlan*>& phases, int blocks, bool split,
-                        std::vector<PhaseTasks>& out) {
+                        std::vector<PhaseTasks>& out, double walkBudget) {
     size_t n = phases.size();
     out.assign(n, PhaseTasks{});
     if (cacheBytes_ > kCacheLimit) {  // only here: walks hand out references into the cache
         walks_.clear();
         deg_.clear();
+        hop2_.clear();
         cacheBytes_ = 0;
     }
     std::vector<double> estAvg(n), estHub(n), scale(n, defaultCalib_);
     std::vector<const std::vector<float>*> walked(n, nullptr);
     std::vector<char> forced(n, 0);
     for (size_t i = 0; i < n; ++i) {
-        estAvg[i] = estimate(*phases[i], false);
+        estAvg[i] = estimate2(*phases[i]);
         estHub[i] = split ? estimate(*phases[i], true) : estAvg[i];
         out[i].work = estAvg[i];
         if (!calib_.empty() || !mustWalk_.empty()) {
@@ -172,10 +220,14 @@ void TaskBuilder::build(const std::vector<const PhasePlan*>& phases, int blocks,
             if (!forced[i] && estHub[i] < walkThreshold) break;
             const PhasePlan& ph = *phases[i];
             const DevStep& s0 = ph.plan.steps[0];
-            double edges = (double)(ph.rootEnd - ph.rootBeg) *
+            // cost of a walk: one lookup per root for chain-shaped plans,
+            // otherwise every first-segment edge
+            double edges = chain_shaped(ph.plan) ? (double)(ph.rootEnd - ph.rootBeg)
+                         : (double)(ph.rootEnd - ph.rootBeg) *
                            (s0.kind == kExpand ? std::max(1.0, ix_.avg_degree(s0.pred, s0.dir)) : (double)ix_.pred_size(s0.pred));
-            if (!forced[i] && used + edges > kWalkBudget) continue;
-            used += edges;
+            const bool cached = walks_.count(signature(ph)) != 0;
+            if (!forced[i] && !cached && used + edges > walkBudget) continue;
+            if (!cached) used += edges;   // cached walks cost nothing
             walked[i] = &walk(ph);
             double s = 0;
             for (float x : *walked[i]) s += x;
@@ -267,8 +319,20 @@ void TaskBuilder::build(const std::vector<const PhasePlan*>& phases, int blocks,
     }
 }
 
+double TaskBuilder::expected_ns(const PhasePlan& ph) {
+    if (ph.how != kDevice) return 0.0;
+    if (!calib_.empty()) {
+        auto it = calib_.find(signature(ph));
+        if (it != calib_.end()) return estimate2(ph) * it->second;
+    }
+    // the average-fan-out estimate, raised at most tenfold toward the
+    // hub-aware one (which assumes every step lands on a hub)
+    return estimate2(ph) * defaultCalib_;
+}
+
 void TaskBuilder::learn(const std::vector<const PhasePlan*>& phases, const std::vector<DevTask>& tasks,
-                        const std::vector<double>& cost, const unsigned long long* taskNs, int blocks) {
+                        const std::vector<double>& cost, const unsigned long long* taskNs, int blocks,
+                        double weight, double minWorstNs) {
     size_t n = phases.size();
     std::vector<double> ns(n, 0.0), units(n, 0.0), worst(n, 0.0);
     double totNs = 0, totUnits = 0;
@@ -282,12 +346,15 @@ void TaskBuilder::learn(const std::vector<const PhasePlan*>& phases, const std::
         totNs += d;
         totUnits += std::max(cost[t], 1.0);
     }
-    if (totUnits > 0) defaultCalib_ = totNs / totUnits;
-    const double limit = totNs / (std::max(blocks, 1) * 8.0);
+    auto blend = [weight](double old, double now) { return old + weight * (now - old); };
+    if (totUnits > 0) defaultCalib_ = blend(defaultCalib_, totNs / totUnits);
+    const double limit = std::max(minWorstNs, totNs / (std::max(blocks, 1) * 8.0));
     for (size_t p = 0; p < n; ++p) {
         if (units[p] <= 0) continue;
         std::string sig = signature(*phases[p]);
-        calib_[sig] = ns[p] / units[p];
+        auto it = calib_.find(sig);
+        const double now = ns[p] / units[p];
+        calib_[sig] = it == calib_.end() ? now : blend(it->second, now);
         if (worst[p] > limit) mustWalk_[sig] = true;
     }
 }

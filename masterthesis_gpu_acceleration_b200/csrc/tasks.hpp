@@ -36,17 +36,28 @@ public:
 
     // phases[i] is planned as plan number i.  blocks: resident blocks of the
     // launch.  split=false keeps every root in shared-memory tasks.
+    // walkBudget: first-segment edges that may be newly walked (cached
+    // walks and phases marked by learn() are not counted).
     void build(const std::vector<const PhasePlan*>& phases, int blocks, bool split,
-               std::vector<PhaseTasks>& out);
+               std::vector<PhaseTasks>& out, double walkBudget = 4.0e6);
 
     size_t cache_bytes() const { return cacheBytes_; }
+
+    // Estimated device time of a phase: learned ns per unit for plans seen
+    // by learn(), otherwise the work estimate times the learned default
+    // (1 ns per unit before any learning).
+    double expected_ns(const PhasePlan& ph);
 
     // Feedback from an instrumented run of tasks built by build(): taskNs
     // holds each task's start and end time.  Learns, per plan signature, the
     // device time per unit of estimated work, and marks plans whose slowest
     // task exceeded the balancing target for an exact per-root walk.
+    // weight: how far a learned figure moves toward this run's (1 replaces
+    // it; the serving loop, learning from many small launches, uses less).
+    // minWorstNs: slowest-task time below which no walk is requested.
     void learn(const std::vector<const PhasePlan*>& phases, const std::vector<DevTask>& tasks,
-               const std::vector<double>& cost, const unsigned long long* taskNs, int blocks);
+               const std::vector<double>& cost, const unsigned long long* taskNs, int blocks,
+               double weight = 1.0, double minWorstNs = 0.0);
 
     // Overrides: a fixed task work target (0 = automatic) and the hub-aware
     // estimate above which a phase is walked.
@@ -58,6 +69,11 @@ private:
     std::unordered_map<int64_t, std::vector<int32_t>> deg_;      // (pred, dir) -> degree by entity
     std::unordered_map<int64_t, double> sbFan_;                  // (pred, dir) -> size-biased fan-out
     std::unordered_map<std::string, std::vector<float>> walks_;  // plan signature -> per-root work
+    struct Hop2 {
+        std::vector<float> perRow;   // per row of (p0, d0): sum over its edges of the next degree
+        double total = 0.0;
+    };
+    std::unordered_map<uint64_t, Hop2> hop2_;                    // (p0, d0, p1, d1) -> two-hop sums
     std::unordered_map<std::string, double> calib_;             // plan signature -> ns per work unit
     std::unordered_map<std::string, bool> mustWalk_;            // plan signature -> walk next time
     double defaultCalib_ = 1.0;
@@ -67,6 +83,15 @@ private:
     double sb_fan(int32_t pred, int dir);
     double avg_fan(const DevStep& st) const;
     double estimate(const PhasePlan& ph, bool hubAware);
+    // Two-hop sums of the transition from (p0, d0) to (p1, d1), shared by
+    // every plan whose first two steps follow it.
+    const Hop2& hop2(int32_t p0, int d0, int32_t p1, int d1);
+    // Plans whose second step is keyed by the value the first step binds.
+    bool chain_shaped(const DevPlan& P) const;
+    // Exact work of the first two levels times average fan-outs beyond, for
+    // chain-shaped plans whose roots are the first step's rows; otherwise
+    // the average-fan-out estimate.
+    double estimate2(const PhasePlan& ph);
     const std::vector<float>& walk(const PhasePlan& ph);
     double child_work(const DevPlan& P, const int32_t* rootVals, int32_t e, const int32_t* deg2, double tail) const;
     int root_vals(const DevPlan& P, int32_t r, int32_t* vals) const;
