@@ -89,6 +89,23 @@ void* gpu_batch_prepare(void* ctx, const char* const* rules, int n, int isJson);
  * Returns 0, or -1 on a CUDA error. */
 int gpu_batch_run(void* batch, long long flushBytes, GpuRuleResult* out, int* status, double* deviceMs);
 
+/* The last run's counts in 64 bits (GpuRuleResult's int fields saturate at
+ * INT_MAX): counts[4 * i + 0..3] = support, headSize, headSupport, bodySize
+ * of rule i; status (optional) as gpu_batch_run.  No counterpart in the
+ * reference (its counts are int).  Returns 0, or -1 on null arguments. */
+int gpu_batch_counts(void* batch, long long* counts, int* status);
+
+/* One rule split over nShards workers (one per GPU): evaluates only slice
+ * `shard` of each device phase's roots — head triples for support, rows of
+ * the seed atom keyed by the head subject for body size — cut so that the
+ * slices carry about equal estimated work.  Body pairs of different head
+ * subjects are distinct, so summing counts[0] (support) and counts[3]
+ * (bodySize) over all shards gives the whole rule's counts (one int64 sum
+ * all-reduce across GPUs); counts[1..2] (headSize, headSupport) are the
+ * whole rule's in every shard.  No counterpart in the reference.  Returns
+ * 0, or -1 on bad arguments, a malformed rule or a CUDA error. */
+int gpu_evaluate_rule_shard(void* ctx, const char* ruleText, int shard, int nShards, long long* counts);
+
 /* Device plans, tasks, bytes copied host->device at preparation and bytes
  * copied device->host per run. */
 int gpu_batch_info(void* batch, long long* plans, long long* tasks, long long* h2dBytes, long long* d2hBytes);

@@ -43,6 +43,8 @@ API_SYMBOLS = (
     "gpu_serve_stats",
     "gpu_serve_stop",
     "gpu_graph_stats",
+    "gpu_batch_counts",
+    "gpu_evaluate_rule_shard",
     "gpu_last_error",
 )
 
@@ -123,6 +125,11 @@ def load_library(path: os.PathLike | str | None = None) -> ctypes.CDLL:
     lib.gpu_batch_profile.restype = ctypes.c_int
     lib.gpu_batch_profile.argtypes = [ctypes.c_void_p, ctypes.POINTER(ctypes.c_ulonglong), ctypes.c_void_p,
                                       ctypes.c_void_p, ctypes.c_longlong]
+    lib.gpu_batch_counts.restype = ctypes.c_int
+    lib.gpu_batch_counts.argtypes = [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p]
+    lib.gpu_evaluate_rule_shard.restype = ctypes.c_int
+    lib.gpu_evaluate_rule_shard.argtypes = [ctypes.c_void_p, ctypes.c_char_p, ctypes.c_int, ctypes.c_int,
+                                            ctypes.c_void_p]
     lib.gpu_batch_autotune.restype = ctypes.c_int
     lib.gpu_batch_autotune.argtypes = [ctypes.c_void_p, ctypes.c_int]
     lib.gpu_set_option.restype = ctypes.c_int
@@ -208,6 +215,18 @@ class GpuRulesLib:
                                f"({self._lib.gpu_last_error().decode(errors='replace')})")
         return res
 
+    def evaluate_rule_shard(self, rule_text: str, shard: int, n_shards: int):
+        """Slice `shard` of `n_shards` of one rule (gpu_evaluate_rule_shard):
+        int64 array [support part, headSize, headSupport, bodySize part]."""
+        import numpy as np
+        out = np.zeros(4, dtype=np.int64)
+        rc = self._lib.gpu_evaluate_rule_shard(self._handle(), rule_text.encode(), int(shard), int(n_shards),
+                                               out.ctypes.data)
+        if rc != 0:
+            raise RuntimeError(f"gpu_evaluate_rule_shard failed for: {rule_text} "
+                               f"({self._lib.gpu_last_error().decode(errors='replace')})")
+        return out
+
     def prepare_batch(self, rules: Sequence[str], is_json: bool = False) -> "PreparedBatch":
         return PreparedBatch(self, rules, is_json)
 
@@ -272,6 +291,15 @@ class PreparedBatch:
         if not fetch:
             return None, None, ms.value
         return list(self._out)[:self.n], list(self._st)[:self.n], ms.value
+
+    def counts(self):
+        """The last run's counts in 64 bits: int64 array [n, 4] of support,
+        headSize, headSupport, bodySize (gpu_batch_counts)."""
+        import numpy as np
+        out = np.zeros((max(self.n, 1), 4), dtype=np.int64)
+        if self._lib.gpu_batch_counts(self._h, out.ctypes.data, None) != 0:
+            raise RuntimeError("gpu_batch_counts failed")
+        return out[:self.n]
 
     def info(self) -> dict:
         v = [ctypes.c_longlong() for _ in range(4)]

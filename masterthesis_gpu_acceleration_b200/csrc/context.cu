@@ -169,6 +169,32 @@ int evaluate_parsed(Context& c, const Rule& rule, GpuRuleResult* out) {
     return 0;
 }
 
+// Counts of one rule restricted to slice `shard` of `nShards` of each device
+// phase's roots (slices of about equal estimated work).  Support roots are
+// head triples and body-size roots are rows of the seed atom keyed by the
+// head subject, so the slices' counts add up to the whole rule's: distinct
+// (hS, hO) pairs of different hS never collide.  Static parts count in
+// slice 0 only.
+void evaluate_shard(Context& c, const Rule& rule, int shard, int nShards, long long* counts) {
+    RulePlan rp = plan_rule(rule, c.hix, c.geom);
+    int64_t part[2] = {shard == 0 ? rp.support.value : 0, shard == 0 ? rp.body.value : 0};
+    PhasePlan* phs[2] = {&rp.support, &rp.body};
+    for (int k = 0; k < 2 && rp.status == kRuleOk; ++k) {
+        PhasePlan& ph = *phs[k];
+        if (ph.how != kDevice) continue;
+        const std::vector<int32_t> cut = c.tasks->split_roots(ph, nShards);
+        ph.rootBeg = cut[shard];
+        ph.rootEnd = cut[shard + 1];
+        part[k] = 0;
+        float ms = 0.f;
+        if (ph.rootEnd > ph.rootBeg) part[k] = run_one_phase(c, ph, &ms);
+    }
+    counts[0] = rp.status == kRuleOk ? part[0] : 0;
+    counts[1] = rp.headSize;
+    counts[2] = rp.headSupport;
+    counts[3] = rp.status == kRuleOk ? part[1] : 0;
+}
+
 // Parses and plans n rules and stages their device phases.
 void prepare(Batch& b, Context& c, const char* const* rules, int n, int isJson) {
     b.c = &c;
@@ -397,6 +423,43 @@ int gpu_batch_run(void* batch, long long flushBytes, GpuRuleResult* out, int* st
         return 0;
     } catch (const std::exception& e) {
         set_error(std::string("gpu_batch_run error: ") + e.what());
+        return -1;
+    }
+}
+
+int gpu_batch_counts(void* batch, long long* counts, int* status) {
+    if (!batch || !counts) return -1;
+    const Batch& b = *static_cast<const Batch*>(batch);
+    std::vector<int64_t> sup(b.n), body(b.n);
+    for (int i = 0; i < b.n; ++i) { sup[i] = b.rps[i].support.value; body[i] = b.rps[i].body.value; }
+    const unsigned long long* cnt = b.st.counts();
+    for (size_t k = 0; k < b.owner.size(); ++k) {
+        int i = b.owner[k] / 2;
+        if (b.owner[k] % 2 == 0) sup[i] = (int64_t)cnt[k];
+        else body[i] = (int64_t)cnt[k];
+    }
+    for (int i = 0; i < b.n; ++i) {
+        const RulePlan& rp = b.rps[i];
+        const bool ok = b.parseStatus[i] == 0;
+        const bool run = ok && rp.status == kRuleOk;
+        counts[4 * i + 0] = run ? sup[i] : 0;
+        counts[4 * i + 1] = ok ? rp.headSize : 0;
+        counts[4 * i + 2] = ok ? rp.headSupport : 0;
+        counts[4 * i + 3] = run ? body[i] : 0;
+        if (status) status[i] = b.parseStatus[i];
+    }
+    return 0;
+}
+
+int gpu_evaluate_rule_shard(void* ctx, const char* ruleText, int shard, int nShards, long long* counts) {
+    if (!ctx || !ruleText || !counts || nShards < 1 || shard < 0 || shard >= nShards) return -1;
+    Context& c = *static_cast<Context*>(ctx);
+    try {
+        cudaSetDevice(c.device);
+        evaluate_shard(c, c.parser->parse_text(ruleText), shard, nShards, counts);
+        return 0;
+    } catch (const std::exception& e) {
+        set_error(std::string("gpu_evaluate_rule_shard error: ") + e.what());
         return -1;
     }
 }

@@ -181,12 +181,24 @@ static std::string chain_text(int L, int ph, const std::vector<int>& preds, cons
     return out;
 }
 
+// Bumped whenever a configuration's output changes (cached datasets with an
+// older version are regenerated).
+constexpr int kGenVersion = 2;
+
 struct RuleSpec {
     int n = 10;
     std::vector<double> lenWeights;  // index = L-1
     bool predByFreq = false;
     int hubRules = 0;                // first hubRules rules include a hub predicate
     int nHubPreds = 0;
+};
+
+// Shape of the biomedical-style configurations: entities, triples, hub
+// in-degree (two hubs on each of 5 hub predicates).
+struct BioShape {
+    int N;
+    int64_t T;
+    int hubDegree;
 };
 
 static bool write_all(const std::string& dir, const Graph& g, const std::vector<RuleIR>& rules,
@@ -226,8 +238,8 @@ static bool write_all(const std::string& dir, const Graph& g, const std::vector<
     {
         FILE* f = std::fopen((dir + "/meta.txt").c_str(), "wb");
         if (!f) return false;
-        std::fprintf(f, "config=%s\nseed=%llu\nentities=%d\npredicates=%d\ntriples=%zu\nrules=%zu\n",
-                     cfg.c_str(), (unsigned long long)seed, g.N, g.P, g.t.size(), rules.size());
+        std::fprintf(f, "config=%s\nseed=%llu\nentities=%d\npredicates=%d\ntriples=%zu\nrules=%zu\ngen=%d\n",
+                     cfg.c_str(), (unsigned long long)seed, g.N, g.P, g.t.size(), rules.size(), kGenVersion);
         if (ruleSeed != ~0ull) std::fprintf(f, "rule_seed=%llu\n", (unsigned long long)ruleSeed);
         std::fclose(f);
     }
@@ -249,7 +261,18 @@ static void make_rules(const Graph& g, const RuleSpec& rs, Rng& r,
             preds[k] = pick_weighted(predCum, r);
             dirs[k] = (int)r.below(2);
         }
-        if (i < rs.hubRules && rs.nHubPreds > 0) preds[r.below(L)] = (int)r.below(rs.nHubPreds);
+        if (i < rs.hubRules && rs.nHubPreds > 0) {
+            const int hp = (int)r.below(rs.nHubPreds);
+            if (i % 2 == 0 && L >= 2) {
+                // through a hub from both sides: (?x hp ?v) ^ (?y hp ?v)
+                const int k = (int)r.below(L - 1);
+                preds[k] = preds[k + 1] = hp;
+                dirs[k] = 0;
+                dirs[k + 1] = 1;
+            } else {
+                preds[r.below(L)] = hp;
+            }
+        }
         rules.push_back(chain_rule(L, ph, preds, dirs));
         texts.push_back(chain_text(L, ph, preds, dirs));
     }
@@ -259,7 +282,7 @@ static void make_rules(const Graph& g, const RuleSpec& rs, Rng& r,
 
 extern "C" {
 
-// Writes configuration `cfg` (c1, c2, c2s, c3, c4) for graph seed `seed`
+// Writes configuration `cfg` (c1, c2, c2s, c3, c4, c4s) for graph seed `seed`
 // into `outDir`; the rules continue the graph's random stream, or, when
 // ruleSeed != ~0, come from their own stream seeded with ruleSeed (the graph
 // is the same either way).  nRules < 0 keeps the configuration's rule count.
@@ -300,25 +323,28 @@ long long kg_synth_write2(const char* cfg, unsigned long long seed, unsigned lon
         rs.n = 10000;
         rs.lenWeights = {0.2, 0.4, 0.3, 0.1};
         rs.predByFreq = true;
-    } else if (c == "c4") {
-        g.N = 300000; g.P = 50;
-        int64_t T = 6800000;
+    } else if (c == "c4" || c == "c4s") {
+        // c4s: the same construction at a tenth of the size
+        const BioShape sh = c == "c4" ? BioShape{300000, 6800000, 50000} : BioShape{30000, 680000, 5000};
+        g.N = sh.N; g.P = 50;
+        const int64_t T = sh.T;
         g.predCount.assign(g.P, 0);
         seen.reserve((size_t)T * 2);
         const int hubPreds = 5;
+        const double hubShare = (double)T * 400000.0 / 6800000.0;
         std::vector<double> w(g.P);
-        for (int k = 0; k < g.P; ++k) w[k] = k < hubPreds ? 400000.0 : (6800000.0 - hubPreds * 400000.0) / (g.P - hubPreds);
+        for (int k = 0; k < g.P; ++k) w[k] = k < hubPreds ? hubShare : ((double)T - hubPreds * hubShare) / (g.P - hubPreds);
         auto cnt = split_counts(T, w);
         PredSpec ps; ps.od = Dist::Zipf; ps.os = 1.2;
         Zipf zo(g.N, 1.2);
         for (int p = 0; p < g.P; ++p) {
             std::vector<std::pair<int,int>> forced;
             if (p < hubPreds) {
-                // two hub objects with in-degree 50,000 each
+                // two hub objects with in-degree sh.hubDegree each
                 for (int h = 0; h < 2; ++h) {
                     int hub = (int)r.below(g.N);
                     std::vector<int> subj = permutation(g.N, r);
-                    for (int k = 0; k < 50000; ++k) forced.push_back({subj[k], hub});
+                    for (int k = 0; k < sh.hubDegree; ++k) forced.push_back({subj[k], hub});
                 }
             }
             fill_pred(g, seen, p, cnt[p], ps, nullptr, &zo, r, forced);

@@ -319,6 +319,24 @@ void TaskBuilder::build(const std::vector<const PhasePlan*>& phases, int blocks,
     }
 }
 
+std::vector<int32_t> TaskBuilder::split_roots(const PhasePlan& ph, int n) {
+    n = std::max(n, 1);
+    std::vector<int32_t> cut(n + 1, ph.rootEnd);
+    cut[0] = ph.rootBeg;
+    const int32_t R = ph.rootEnd - ph.rootBeg;
+    if (R <= 0) return cut;
+    const std::vector<float>& w = walk(ph);
+    double total = 0;
+    for (float x : w) total += x;
+    double acc = 0;
+    int k = 1;
+    for (int32_t r = 0; r < R && k < n; ++r) {
+        acc += w[r];
+        while (k < n && acc >= total * k / n) cut[k++] = ph.rootBeg + r + 1;
+    }
+    return cut;
+}
+
 double TaskBuilder::expected_ns(const PhasePlan& ph) {
     if (ph.how != kDevice) return 0.0;
     if (!calib_.empty()) {

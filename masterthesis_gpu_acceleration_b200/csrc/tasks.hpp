@@ -59,6 +59,11 @@ public:
                const std::vector<double>& cost, const unsigned long long* taskNs, int blocks,
                double weight = 1.0, double minWorstNs = 0.0);
 
+    // Boundaries of n contiguous slices of a device phase's roots with about
+    // equal estimated work (per-root walk): slice k is [cut[k], cut[k+1]),
+    // cut[0] = rootBeg, cut[n] = rootEnd.
+    std::vector<int32_t> split_roots(const PhasePlan& ph, int n);
+
     // Overrides: a fixed task work target (0 = automatic) and the hub-aware
     // estimate above which a phase is walked.
     double forceTarget = 0.0;

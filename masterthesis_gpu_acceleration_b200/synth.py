@@ -14,6 +14,9 @@ Configurations (sizes of the reference's benchmark shapes):
     c4   biomedical-shaped: 300,000 entities, 50 predicates, 6.8M triples,
          Zipf(1.2) objects, two 50,000-in-degree hubs on each of 5 hub
          predicates; 50 chain rules with 2-5 body atoms, 10 through hubs
+         (5 of them cross a hub from both sides, (?x p ?v) ^ (?y p ?v))
+    c4s  c4 at a tenth of the size (30,000 entities, 680,000 triples,
+         5,000-in-degree hubs), small enough for the CPU oracle
 """
 from __future__ import annotations
 
@@ -43,6 +46,9 @@ def _load():
     return _lib
 
 
+GEN_VERSION = "2"   # kGenVersion of kg_synth.cpp
+
+
 def generate(cfg: str, out_dir: Path | str, seed: int = 0, n_rules: int = -1, rule_seed: int | None = None) -> Path:
     """Writes graph.ttl, triples.bin, rules.txt, rules.ir and meta.txt (cached).
 
@@ -55,7 +61,7 @@ def generate(cfg: str, out_dir: Path | str, seed: int = 0, n_rules: int = -1, ru
     if meta.exists() and meta.read_text().startswith(want) and (out / "graph.ttl").exists():
         m = read_meta(out)
         if (n_rules < 0 or m.get("rules") == str(n_rules)) and m.get("rule_seed") == (
-                None if rule_seed is None else str(rule_seed)):
+                None if rule_seed is None else str(rule_seed)) and m.get("gen") == GEN_VERSION:
             return out
     rs = (1 << 64) - 1 if rule_seed is None else int(rule_seed)
     n = _load().kg_synth_write2(cfg.encode(), seed, rs, n_rules, str(out).encode())

@@ -7,8 +7,10 @@ run on the Turtle graph and rule file the fixture describes.  Nothing is
 computed by the engine or by the C restatement.
 
 Fixtures:
-  synthetic_<cfg>.json   c1 / c2 / c2s, seed 0: the generator's rules and the
-                         reference's measures, plus a checksum of the graph
+  synthetic_<cfg>.json   c1 / c2 / c2s / c4s, seed 0: the generator's rules
+                         and the reference's measures, plus a checksum of the
+                         graph (c4s: the biomedical shape at a tenth of the
+                         size, hub rules included; generated with --threads)
   c3_seed0.npz           all 10,000 c3 rules: support, headSize, headSupport,
                          bodySize per rule (generated with --threads)
   fuzz_<k>.json          small dense graphs with prefixes, literals,
@@ -47,13 +49,13 @@ def ref_rows(ttl: Path, rules: Path, threads: int = 1):
             for r in rows]
 
 
-def synthetic(cfg: str, tmp: Path):
+def synthetic(cfg: str, tmp: Path, threads: int = 1):
     d = synth.generate(cfg, tmp / cfg, seed=0)
     fx = {
         "config": cfg, "seed": 0,
         "triples_sha256": sha(d / "triples.bin"),
         "rules": synth.read_rules(d),
-        "expected": ref_rows(d / "graph.ttl", d / "rules.txt"),
+        "expected": ref_rows(d / "graph.ttl", d / "rules.txt", threads=threads),
     }
     (OUT / f"synthetic_{cfg}.json").write_text(json.dumps(fx, indent=1))
 
@@ -272,8 +274,15 @@ def main():
         oracle.build()
     with tempfile.TemporaryDirectory() as t:
         tmp = Path(t)
+        only = [a.split("=", 1)[1] for a in sys.argv if a.startswith("--only=")]
+        if only:
+            for cfg in only[0].split(","):
+                synthetic(cfg, tmp, threads=8)
+            print("fixtures written to", OUT)
+            return
         for cfg in ("c1", "c2", "c2s"):
             synthetic(cfg, tmp)
+        synthetic("c4s", tmp, threads=8)
         edge_cases(tmp)
         for k in range(6):
             fuzz_fixture(k, tmp, n_rules=150)

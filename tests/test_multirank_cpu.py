@@ -2,8 +2,9 @@
 
 The engine needs a GPU, but everything the multi-GPU layout adds around it
 runs on the host: each rank's data (same graph, own rule set), the slice of a
-shared rule list, the max-over-ranks timing that the benchmark reports, and
-the gather of per-rank results back into rule order.
+shared rule list, the max-over-ranks timing that the benchmark reports, the
+gather of per-rank results back into rule order, and the int64 sum
+all-reduce that joins the slices of one rule split over the ranks.
 """
 import hashlib
 import os
@@ -45,9 +46,40 @@ def _worker(rank, world, port, data_dir, q):
         parts = [None] * world
         dist.all_gather_object(parts, [r.upper() for r in mine])
         back = shard.gather_results(parts, len(shared), world)
-        q.put((rank, triples, rules, mx, back))
+        # one rule split over the ranks: partial counts, one int64 all-reduce
+        whole = shard.evaluate_rule_split(_tiny_shard_eval, "tiny")
+        q.put((rank, triples, rules, mx, back, whole))
     finally:
         dist.destroy_process_group()
+
+
+# A tiny graph and the rule (?a p ?v) ^ (?b p ?v) => (?a q ?b), counted by
+# brute force: body pairs of a slice of head subjects, support of a slice of
+# head triples.  Stands in for gpu_evaluate_rule_shard on the CPU.
+_P = [(a, v) for a in range(12) for v in range(4) if (a * 7 + v * 3) % 5 < 2]
+_Q = [(a, b) for a in range(12) for b in range(12) if (a + 2 * b) % 7 == 0]
+
+
+def _grounded(a, b):
+    return a != b and any(v not in (a, b) and (a, v) in _P and (b, v) in _P for v in range(4))
+
+
+def _tiny_shard_eval(rule, k, n):
+    subj = sorted({a for a, _ in _P})
+    lo, hi = shard.shard_bounds(len(subj), k, n)
+    mine = set(subj[lo:hi])
+    body = sum(1 for a in mine for b in range(12) if _grounded(a, b))
+    lo, hi = shard.shard_bounds(len(_Q), k, n)
+    sup = sum(1 for a, b in _Q[lo:hi] if _grounded(a, b))
+    return [sup, len(_Q), len(_Q), body]
+
+
+def test_tiny_shard_eval_is_additive():
+    whole = _tiny_shard_eval("tiny", 0, 1)
+    assert whole[0] > 0 and whole[3] > 0
+    for n in (2, 3, 5):
+        parts = [_tiny_shard_eval("tiny", k, n) for k in range(n)]
+        assert sum(p[0] for p in parts) == whole[0] and sum(p[3] for p in parts) == whole[3]
 
 
 def test_two_ranks_gloo(tmp_path):
@@ -60,8 +92,8 @@ def test_two_ranks_gloo(tmp_path):
         p.start()
     out = {}
     for _ in range(world):
-        rank, triples, rules, mx, back = q.get(timeout=120)
-        out[rank] = (triples, rules, mx, back)
+        rank, triples, rules, mx, back, whole = q.get(timeout=120)
+        out[rank] = (triples, rules, mx, back, whole)
     for p in procs:
         p.join(timeout=60)
         assert p.exitcode == 0
@@ -69,6 +101,11 @@ def test_two_ranks_gloo(tmp_path):
     assert out[0][1] != out[1][1], "ranks must evaluate different rule sets"
     assert out[0][2] == out[1][2] == 150.0
     assert out[0][3] == out[1][3] == [f"RULE{i}" for i in range(11)]
+    single = _tiny_shard_eval("tiny", 0, 1)
+    for r in range(world):
+        w = out[r][4]
+        assert (w["support"], w["headSize"], w["bodySize"]) == (single[0], single[1], single[3])
+        assert w["confidence"] == (single[0] / single[3] if single[3] else 0.0)
     assert shard.weak_value(10000, 2, 5, 150.0) == pytest.approx(2 * 10000 * 5 / 0.15)
 
 

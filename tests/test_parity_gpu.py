@@ -87,7 +87,7 @@ def test_fuzz(name, tmp_path):
         _check(res, fx["expected_json"], "batch json")
 
 
-@pytest.mark.parametrize("cfg", ["c1", "c2", "c2s"])
+@pytest.mark.parametrize("cfg", ["c1", "c2", "c2s", "c4s"])
 def test_synthetic(cfg, data_dir):
     fx = load_fixture(f"synthetic_{cfg}.json")
     d = synth.generate(cfg, data_dir / cfg, seed=fx["seed"])
