@@ -44,7 +44,16 @@ ROOT = Path(__file__).resolve().parent
 sys.path.insert(0, str(ROOT))
 
 METRIC = "rules/s batched vs per-rule on 1 B200 (exact counts); p99 latency; HBM GB/s"
-WORKLOAD = "c3: DBpedia-shaped, 100k entities, 600 predicates, 206k triples, 10,000 chain rules (1-4 atoms)"
+WORKLOADS = {
+    "c1": "c1: 10k entities, 20 predicates, 100k uniform triples, 10 chain rules (1-2 atoms)",
+    "c2": "c2: 2k entities, 10 predicates, 100k uniform triples, 10 chain rules (2-3 atoms)",
+    "c2s": "c2s: c2 with Zipf(1.3) subjects, 10 chain rules (2-3 atoms)",
+    "c3": "c3: DBpedia-shaped, 100k entities, 600 predicates, 206k triples, 10,000 chain rules (1-4 atoms)",
+    "c4": "c4: biomedical-shaped, 300k entities, 50 predicates, 6.8M triples, 50,000-in-degree hubs, "
+          "50 chain rules (2-5 atoms, 10 through hubs)",
+    "c4s": "c4s: c4 at a tenth of the size (30k entities, 680k triples, 5,000-in-degree hubs), 50 rules",
+}
+WORKLOAD = WORKLOADS["c3"]
 FLUSH_BYTES = 256 << 20
 CPU_SAMPLE_STRIDE = 20
 
@@ -55,7 +64,8 @@ def parse_args():
     ap.add_argument("--steps", type=int, default=10)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="engine", choices=["engine", "reference"])
-    ap.add_argument("--config", default="c3")
+    ap.add_argument("--config", default="c3", choices=sorted(WORKLOADS),
+                    help="workload (c3 is the headline; the others are parity configurations)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-per-rule", action="store_true")
     ap.add_argument("--max-rules", type=int, default=0, help="use only the first N rules (profiling case)")
@@ -142,11 +152,23 @@ def profile_traffic() -> float | None:
     return None
 
 
-def cpu_baseline(d: Path, rules: list[str], timeout: float = 300.0) -> dict:
-    """The reference's CPU_01 code, one thread, on every 20th rule."""
+def cpu_sample(cfg: str, n: int) -> tuple[list[int], str]:
+    """Rule indices of a bounded CPU sample: every 20th c3 rule; for the
+    biomedical shapes the 40 rules that do not cross a hub (a hub rule takes
+    the CPU code minutes); every rule of the small configurations."""
+    if cfg == "c3":
+        return list(range(0, n, CPU_SAMPLE_STRIDE)), f"every {CPU_SAMPLE_STRIDE}th c3 rule"
+    if cfg in ("c4", "c4s"):
+        return list(range(10, n)), f"the {cfg} rules that do not cross a hub (10..{n - 1})"
+    return list(range(n)), f"every {cfg} rule"
+
+
+def cpu_baseline(d: Path, rules: list[str], cfg: str = "c3", timeout: float = 300.0) -> dict:
+    """The reference's CPU_01 code, one thread, on a bounded sample."""
     import oracle
-    sample = rules[::CPU_SAMPLE_STRIDE]
-    desc = f"every {CPU_SAMPLE_STRIDE}th c3 rule ({len(sample)} of {len(rules)}), support + body size, 1 thread"
+    idx, what = cpu_sample(cfg, len(rules))
+    sample = [rules[i] for i in idx]
+    desc = f"{what} ({len(sample)} of {len(rules)}), support + body size, 1 thread"
     with tempfile.TemporaryDirectory() as t:
         rf = Path(t) / "rules.txt"
         rf.write_text("\n".join(sample) + "\n")
@@ -157,7 +179,8 @@ def cpu_baseline(d: Path, rules: list[str], timeout: float = 300.0) -> dict:
         else:
             from masterthesis_gpu_acceleration_b200 import synth
             g = oracle.OracleGraph(synth.read_triples(d), int(synth.read_meta(d)["predicates"]))
-            ir = oracle.split_ir(synth.read_rule_ir(d))[::CPU_SAMPLE_STRIDE]
+            irs = oracle.split_ir(synth.read_rule_ir(d))
+            ir = [irs[i] for i in idx]
             secs = oracle.time_oracle(g, np.concatenate(ir), len(ir))
             kind = "port"
     return {"value": len(sample) / secs, "unit": "rules/s", "cores": 1, "kind": kind, "sample": desc,
@@ -235,12 +258,14 @@ def reference_arm(args):
     rules = synth.read_rules(d)
     threads = os.cpu_count() or 1
     steps, warm = args.steps, args.warmup
-    stride = CPU_SAMPLE_STRIDE * max(1, math.ceil((steps + warm) / 13))
+    stride = CPU_SAMPLE_STRIDE * max(1, math.ceil((steps + warm) / 13)) if args.config == "c3" else 1
+    fixed, what = cpu_sample(args.config, len(rules))
     base = {"metric": METRIC, "unit": "rules/s", "higher_is_better": True, "impl": "reference",
             "n_gpus": args.gpus, "steps": steps, "warmup": warm, "dtype": "int32", "data": "synthetic",
             "scaling": "weak", "vs_baseline": None,
-            "config": {"workload": WORKLOAD, "parallelism": f"{threads} host threads, rules spread over threads",
-                       "global_batch": len(rules[::stride])}}
+            "config": {"workload": WORKLOADS[args.config],
+                       "parallelism": f"{threads} host threads, rules spread over threads",
+                       "global_batch": len(rules[::stride]) if args.config == "c3" else len(fixed)}}
     if not oracle.ref_available():
         kind = "port"
     else:
@@ -248,7 +273,8 @@ def reference_arm(args):
     total_rules, total_s = 0, 0.0
     with tempfile.TemporaryDirectory() as t:
         for step in range(warm + steps):
-            sample = rules[step % stride::stride]
+            idx = list(range(step % stride, len(rules), stride)) if args.config == "c3" else fixed
+            sample = [rules[i] for i in idx]
             rf = Path(t) / f"rules{step}.txt"
             rf.write_text("\n".join(sample) + "\n")
             if kind == "reference":
@@ -256,14 +282,14 @@ def reference_arm(args):
                 secs = summ["eval_wall_ms"] / 1e3
             else:
                 g = oracle.OracleGraph(synth.read_triples(d), int(synth.read_meta(d)["predicates"]))
-                ir = oracle.split_ir(synth.read_rule_ir(d))[step % stride::stride]
-                secs = oracle.time_oracle(g, np.concatenate(ir), len(ir))
+                irs = oracle.split_ir(synth.read_rule_ir(d))
+                secs = oracle.time_oracle(g, np.concatenate([irs[i] for i in idx]), len(idx))
             if step >= warm:
                 total_rules += len(sample)
                 total_s += secs
     value = total_rules / total_s
-    desc = (f"per step every {stride}th c3 rule (offset = step), {threads} threads "
-            f"(CPU_01_nonparallel per rule, rules spread over threads)")
+    per_step = f"every {stride}th c3 rule (offset = step)" if args.config == "c3" else what
+    desc = f"per step {per_step}, {threads} threads (CPU_01_nonparallel per rule, rules spread over threads)"
     line = dict(base)
     line.update({"value": value, "ms_per_step": 1e3 * total_s / steps,
                  "cpu_baseline": {"value": value, "unit": "rules/s", "cores": threads if kind == "reference" else 1,
@@ -325,19 +351,23 @@ def engine_arm(args):
     value = shard.weak_value(len(rules), world, args.steps, max_ms)
 
     exact = None
-    if rank == 0 and args.config == "c3" and not args.max_rules:
-        gold = ROOT / "tests" / "golden" / "c3_seed0.npz"
-        if gold.exists():
-            exp = np.load(gold)["expected"]
-            got = np.array([[r.support, r.headSize, r.headSupport, r.bodySize] for r in results], dtype=np.int64)
-            exact = bool((got == exp).all())
+    if rank == 0 and not args.max_rules:
+        exp = None
+        if args.config == "c3" and (ROOT / "tests" / "golden" / "c3_seed0.npz").exists():
+            exp = np.load(ROOT / "tests" / "golden" / "c3_seed0.npz")["expected"]
+        elif (ROOT / "tests" / "golden" / f"synthetic_{args.config}.json").exists():
+            fx = json.loads((ROOT / "tests" / "golden" / f"synthetic_{args.config}.json").read_text())
+            exp = np.array([[e[k] for k in ("support", "headSize", "headSupport", "bodySize")]
+                            for e in fx["expected"]], dtype=np.int64)
+        if exp is not None:
+            exact = bool((batch.counts() == exp).all())
 
     # ---- roofline: algorithmic bytes per launch over the average launch ----
     alg_bytes = batch.count_bytes()
     avg_s = total_ms / args.steps / 1e3
     peaks = measured_peaks()
     achieved = alg_bytes / avg_s / 1e9
-    traffic = profile_traffic()
+    traffic = profile_traffic() if args.config == "c3" and not args.max_rules else None
 
     # ---- end to end through the C ABI with host strings ----
     for _ in range(max(1, args.warmup // 2)):
@@ -369,10 +399,10 @@ def engine_arm(args):
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
-        cpu = cpu_baseline(d, rules)
+        cpu = cpu_baseline(d, rules, args.config)
 
     serving = None
-    if rank == 0 and world == 1 and not args.no_serve:
+    if rank == 0 and world == 1 and not args.no_serve and args.config == "c3":
         serving = serving_sweep(lib, d, args)
 
     batch.close()
@@ -382,7 +412,8 @@ def engine_arm(args):
             "metric": METRIC, "value": value, "unit": "rules/s", "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": max_ms / args.steps, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "int32", "data": "synthetic",
-            "config": {"workload": WORKLOAD, "global_batch": world * len(rules), "rules_per_rank": len(rules),
+            "config": {"workload": WORKLOADS[args.config], "global_batch": world * len(rules),
+                       "rules_per_rank": len(rules),
                        "parallelism": f"rule sets sharded over {world} GPU(s), no collective",
                        "l2": "flushed before every step (256 MiB write, outside the timed span)",
                        "exact_vs_reference_golden": exact, "plans": info["plans"], "tasks": info["tasks"]},

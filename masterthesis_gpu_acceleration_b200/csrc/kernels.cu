@@ -392,10 +392,17 @@ __device__ __forceinline__ void run_task(Smem<B>& sm, const DevIndex& ix, const 
                     lo_[u] = -1;
                     e_[u] = 0;
                     if (j < take) {
-                        int lo = hint, hi = nw - 1;
-                        while (lo < hi) {
-                            const int mid = (lo + hi) >> 1;
-                            if (sm.wPre[mid] > j) hi = mid; else lo = mid + 1;
+                        // the item holding candidate j: j only grows for this
+                        // thread, so try the previous item first (a hub's long
+                        // segment then costs one probe per candidate)
+                        int lo = hint;
+                        if (sm.wPre[lo] <= j) {
+                            int hi = nw - 1;
+                            ++lo;
+                            while (lo < hi) {
+                                const int mid = (lo + hi) >> 1;
+                                if (sm.wPre[mid] > j) hi = mid; else lo = mid + 1;
+                            }
                         }
                         hint = lo;
                         lo_[u] = lo;
