@@ -54,6 +54,11 @@ struct DevIndex {
     const int32_t* predEdge[2];  // P + 1 entries
     // (predicate, direction, key) -> edge range, open addressing
     const struct HashSlot* hash;
+    // hub rows (rows whose values also exist as a rank bitmap)
+    const int32_t* hubOf[2];     // per row: hub index or -1
+    const int64_t* hubOff;       // per hub: first word in hubBits
+    const uint32_t* hubBits;
+    int32_t nHub;
     uint32_t hashMask;
     int32_t nPred;
     int32_t nEnt;

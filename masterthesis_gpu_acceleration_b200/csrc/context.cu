@@ -47,7 +47,7 @@ void Staged::stage(Context& c, std::vector<DevPlan>& plans, const std::vector<co
         if (!phases[i]->needsGlobalBitmap) continue;
         size_t rows = (size_t)(phases[i]->rootEnd - phases[i]->rootBeg);
         gOff[i] = bitmapWords;
-        bitmapWords += (rows * (size_t)plans[i].wo + 31) / 32;
+        bitmapWords += rows * (size_t)std::max(plans[i].rowWords, 1);   // word-aligned rows
     }
     cudaStream_t as = streamOrdered ? s : nullptr;
     if (bitmapWords) dBitmap.ensure(bitmapWords * 4, as);
@@ -306,7 +306,10 @@ void* gpu_load_graph(const char* ttlPath) {
             return nullptr;
         }
         c->prefixes = scan_rule_prefixes(ttlPath);
-        c->hix = build_index(spo, (int32_t)c->ents.size(), (int32_t)c->preds.size());
+        // GPU_RULES_HUB_MIN_DEGREE overrides the hub-row threshold (0: no hub rows)
+        int32_t hubMin = kHubMinDegree;
+        if (const char* h = std::getenv("GPU_RULES_HUB_MIN_DEGREE")) hubMin = std::max(0, std::atoi(h));
+        c->hix = build_index(spo, (int32_t)c->ents.size(), (int32_t)c->preds.size(), hubMin);
         c->tasks.reset(new TaskBuilder(c->hix));
         c->parser.reset(new RuleParser(c->ents, c->preds, c->prefixes));
         c->init_device();
@@ -624,7 +627,7 @@ int64_t run_phase_noalloc(Context& c, const PhasePlan& ph, char* scratch, float*
     const size_t bitmapOff = align256(taskOff + tasks.size() * sizeof(DevTask));
     size_t bitmapWords = 0;
     if (ph.needsGlobalBitmap)
-        bitmapWords = ((size_t)(ph.rootEnd - ph.rootBeg) * (size_t)plan.wo + 31) / 32;
+        bitmapWords = (size_t)(ph.rootEnd - ph.rootBeg) * (size_t)std::max(plan.rowWords, 1);
     const size_t need = bitmapOff + bitmapWords * 4;
     if (need > kNoAllocScratchBytes)
         throw CudaError("rule needs " + std::to_string(need) + " bytes of scratch; the no-allocation limit is " +

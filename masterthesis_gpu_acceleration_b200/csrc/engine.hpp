@@ -188,6 +188,10 @@ struct Context {
             add(h.predEdge[d].data(), h.predEdge[d].size() * 4);
         }
         add(h.hash.data(), h.hash.size() * sizeof(HashSlot));
+        add(h.hubOf[0].data(), h.hubOf[0].size() * 4);
+        add(h.hubOf[1].data(), h.hubOf[1].size() * 4);
+        add(h.hubOff.data(), h.hubOff.size() * 8);
+        add(h.hubBits.data(), h.hubBits.size() * 4);
         size_t total = 0;
         std::vector<size_t> off;
         for (auto& pp : parts) {
@@ -216,6 +220,11 @@ struct Context {
             dix.predEdge[d] = reinterpret_cast<const int32_t*>(base + off[k++]);
         }
         dix.hash = reinterpret_cast<const HashSlot*>(base + off[k++]);
+        dix.hubOf[0] = reinterpret_cast<const int32_t*>(base + off[k++]);
+        dix.hubOf[1] = reinterpret_cast<const int32_t*>(base + off[k++]);
+        dix.hubOff = reinterpret_cast<const int64_t*>(base + off[k++]);
+        dix.hubBits = reinterpret_cast<const uint32_t*>(base + off[k++]);
+        dix.nHub = (int32_t)h.hubOff.size();
         dix.hashMask = h.hashMask;
         dix.nPred = h.nPred;
         dix.nEnt = h.nEnt;

@@ -70,6 +70,48 @@ int32_t key_rank(const HostIndex& ix, int d, int32_t p, int32_t key) {
     return (int32_t)(std::lower_bound(b, e, key) - b);
 }
 
+// Rows whose expansion is cheaper as a bitmap OR than edge by edge: at
+// least minDegree edges and a value domain (the predicate's rows in the
+// other direction) of at most 8 words per edge.  Heaviest rows first, up to
+// kHubBudgetWords of bitmap in total.
+constexpr int64_t kHubBudgetWords = int64_t(1) << 28;   // 1 GiB
+
+void build_hubs(HostIndex& ix, int32_t minDegree) {
+    struct Cand { int32_t d, row, deg; int64_t words; };
+    std::vector<Cand> c;
+    for (int d = 0; d < 2; ++d) {
+        ix.hubOf[d].assign(ix.rowKey[d].size(), -1);
+        for (int32_t p = 0; p < ix.nPred; ++p) {
+            const int64_t words = (ix.pred_rows(p, 1 - d) + 31) / 32;
+            for (int32_t r = ix.predRow[d][p]; r < ix.predRow[d][p + 1]; ++r) {
+                const int32_t deg = ix.rowBeg[d][r + 1] - ix.rowBeg[d][r];
+                if (minDegree > 0 && deg >= minDegree && words <= 8LL * deg) c.push_back({d, r, deg, words});
+            }
+        }
+    }
+    std::sort(c.begin(), c.end(), [](const Cand& a, const Cand& b) { return a.deg > b.deg; });
+    int64_t used = 0;
+    ix.hubOff.clear();
+    ix.hubBits.clear();
+    for (const Cand& h : c) {
+        if (used + h.words > kHubBudgetWords) continue;
+        ix.hubOf[h.d][h.row] = (int32_t)ix.hubOff.size();
+        ix.hubOff.push_back(used);
+        used += h.words;
+    }
+    ix.hubBits.assign((size_t)used, 0u);
+    for (int d = 0; d < 2; ++d)
+        for (size_t r = 0; r < ix.hubOf[d].size(); ++r) {
+            const int32_t h = ix.hubOf[d][r];
+            if (h < 0) continue;
+            uint32_t* bits = ix.hubBits.data() + ix.hubOff[h];
+            for (int32_t e = ix.rowBeg[d][r]; e < ix.rowBeg[d][r + 1]; ++e) {
+                const int32_t k = ix.valRank[d][e];
+                bits[k >> 5] |= 1u << (k & 31);
+            }
+        }
+}
+
 }  // namespace
 
 std::pair<int32_t, int32_t> HostIndex::row_range(int32_t p, int d, int32_t key) const {
@@ -92,7 +134,7 @@ bool HostIndex::has_triple(int32_t p, int32_t s, int32_t o) const {
     return std::binary_search(b, e, o);
 }
 
-HostIndex build_index(const std::vector<int32_t>& spo, int32_t nEnt, int32_t nPred) {
+HostIndex build_index(const std::vector<int32_t>& spo, int32_t nEnt, int32_t nPred, int32_t hubMinDegree) {
     HostIndex ix;
     ix.nEnt = nEnt;
     ix.nPred = nPred;
@@ -133,6 +175,7 @@ HostIndex build_index(const std::vector<int32_t>& spo, int32_t nEnt, int32_t nPr
             }
         }
     }
+    build_hubs(ix, hubMinDegree);
     return ix;
 }
 

@@ -16,6 +16,13 @@ struct HostIndex {
     std::vector<int32_t> predRow[2], predEdge[2];
     std::vector<HashSlot> hash;
     uint32_t hashMask = 0;
+    // Hub rows: rows with many edges get a bitmap of their values' ranks
+    // (bit valRank of every edge), so that a body-size expansion through
+    // them can OR 32 candidates at a time.  hubOf[d][row] = hub index or -1;
+    // hub h's bitmap is hubBits[hubOff[h] .. hubOff[h] + words of its domain).
+    std::vector<int32_t> hubOf[2];
+    std::vector<int64_t> hubOff;
+    std::vector<uint32_t> hubBits;
 
     int64_t pred_size(int32_t p) const {
         return (p < 0 || p >= nPred) ? 0 : predEdge[0][p + 1] - predEdge[0][p];
@@ -32,7 +39,12 @@ struct HostIndex {
     }
 };
 
+// Rows with at least this many edges may become hub rows (0 = none).
+constexpr int32_t kHubMinDegree = 128;
+
 // Builds the index from (s, p, o) triples (duplicates removed).
-HostIndex build_index(const std::vector<int32_t>& spo, int32_t nEnt, int32_t nPred);
+// hubMinDegree: see kHubMinDegree.
+HostIndex build_index(const std::vector<int32_t>& spo, int32_t nEnt, int32_t nPred,
+                      int32_t hubMinDegree = kHubMinDegree);
 
 }  // namespace gr

@@ -62,6 +62,7 @@ struct BlockState {
     int levelOff[kMaxBody + 1];
     long long warpSum[kWarps];
     unsigned long long red[kWarps];
+    int exRank[kWarps][kMaxVars];   // per warp: hO-domain ranks of the bound values of a hub item
 };
 
 template <int B>
@@ -189,7 +190,9 @@ __device__ __forceinline__ void run_task(Smem<B>& sm, const DevIndex& ix, const 
     const long long rowBase = (heavy || shared) ? 0 : (long long)task.beg - P.gRowBase;
 
     // clear the task's shared dedup bits
-    const int nWords = heavy ? 0 : (shared ? (int)(pairs ? (((long long)G * P.wo + 31) >> 5) : ((G + 31) >> 5))
+    // pair rows are word-aligned: row r occupies words [r * rowWords, (r + 1) * rowWords)
+    const long long rowBits = (long long)P.rowWords << 5;
+    const int nWords = heavy ? 0 : (shared ? (int)(pairs ? (long long)G * P.rowWords : ((G + 31) >> 5))
                                            : (pairs ? 0 : ((G + 31) >> 5)));
     for (int i = tid; i < nWords; i += B) sbits[i] = 0u;
     if (tid == 0) {
@@ -283,8 +286,14 @@ __device__ __forceinline__ void run_task(Smem<B>& sm, const DevIndex& ix, const 
             const DevStep stp = P.steps[k];   // uniform for the round: keep it in registers
             const bool leaf = (k + 1 == P.m);
             const bool hasFilters = (P.chkN[k + 1] | P.usedN[k + 1]) != 0;
-            const int wo = P.wo;
             const bool itemHasRank = pairs && P.hoLevel >= 1 && k >= P.hoLevel;
+            // Hub path: when the leaf binds hO and tests nothing but
+            // injectivity, an item whose segment is a whole hub row is
+            // counted by OR-ing the row's rank bitmap into its pair row (32
+            // candidates per word) instead of candidate by candidate.
+            const bool hubPath = leaf && pairs && stp.hoWhich != 0 && stp.kind == kExpand && stp.nNew == 1 &&
+                                 !hasFilters && ix.nHub > 0 && !(heavy && k == 0);
+            bool isHub = false;
 
             // window: the stored neighbour segment of each item
             int myBeg = 0;
@@ -296,20 +305,32 @@ __device__ __forceinline__ void run_task(Smem<B>& sm, const DevIndex& ix, const 
                     pruned = (fb[it[0] >> 5] >> (it[0] & 31)) & 1u;
                     if (heavy) mt.add(4);
                 } else if (itemHasRank) {
-                    const long long bit = (rowBase + it[0]) * (long long)P.wo + it[1];
+                    const long long bit = (rowBase + it[0]) * rowBits + it[1];
                     pruned = (bm[bit >> 5] >> (bit & 31)) & 1u;
                     if (!shared) mt.add(4);
                 }
                 if (!pruned) {
                     myBeg = it[lenK];
                     myLen = it[lenK + 1];
-                    if (tid == 0) {
+                    if (hubPath && myLen > 0 && !(tid == 0 && S.curOff[k] != 0)) {
+                        const int row = __ldg(ix.predRow[stp.dir] + stp.pred) + __ldg(ix.srcRank[stp.dir] + myBeg);
+                        const int h = __ldg(ix.hubOf[stp.dir] + row);
+                        mt.add(12);
+                        if (h >= 0 && __ldg(ix.rowBeg[stp.dir] + row) == myBeg &&
+                            __ldg(ix.rowBeg[stp.dir] + row + 1) - myBeg == myLen) {
+                            isHub = true;
+                            myBeg = -2 - h;   // marks the item for the hub pass; no candidates
+                            myLen = 0;
+                        }
+                    }
+                    if (tid == 0 && !isHub) {
                         const long long off = S.curOff[k];
                         myBeg += (int)off;
                         myLen = myLen > off ? myLen - off : 0;
                     }
                 }
             }
+            const bool anyHub = hubPath && __syncthreads_or(isHub);
             sm.wBeg[tid] = myBeg;
             sm.wLen[tid] = myLen;
             if (tid == 0 && !leaf) S.count[k + 1] = 0;
@@ -343,7 +364,7 @@ __device__ __forceinline__ void run_task(Smem<B>& sm, const DevIndex& ix, const 
                 if (pairs && stp.hoWhich) {
                     rank = rankLoaded;
                     if (!leaf) {
-                        const long long bit = (rowBase + root) * (long long)wo + rank;
+                        const long long bit = (rowBase + root) * rowBits + rank;
                         if (!shared) mt.add(4);
                         if ((bm[bit >> 5] >> (bit & 31)) & 1u) return;
                     }
@@ -354,7 +375,7 @@ __device__ __forceinline__ void run_task(Smem<B>& sm, const DevIndex& ix, const 
                         const uint32_t old = atomicOr(&fb[root >> 5], mask);
                         if (heavy) { mt.add(8); myNew += (old & mask) ? 0ull : 1ull; }
                     } else {
-                        const long long bit = (rowBase + root) * (long long)wo + rank;
+                        const long long bit = (rowBase + root) * rowBits + rank;
                         const uint32_t mask = 1u << (bit & 31);
                         const uint32_t old = atomicOr(&bm[bit >> 5], mask);
                         if (!shared) mt.add(8);
@@ -420,6 +441,60 @@ __device__ __forceinline__ void run_task(Smem<B>& sm, const DevIndex& ix, const 
 #pragma unroll
                 for (int u = 0; u < kU; ++u)
                     if (lo_[u] >= 0) eval(lo_[u], e_[u], n0_[u], n1_[u], rk_[u]);
+            }
+            if (anyHub) {
+                // hub items of the consumed part of the window: [0, cut)
+                int cut = nw;
+                if (take < total) {
+                    int lo = 0, hi = nw - 1;
+                    while (lo < hi) {
+                        const int mid = (lo + hi) >> 1;
+                        if (sm.wPre[mid] > take) hi = mid; else lo = mid + 1;
+                    }
+                    cut = lo;
+                }
+                const int lane = tid & 31, warp = tid >> 5;
+                constexpr int kWarps = B / 32;
+                const int words = P.rowWords;
+                const bool perWarp = words <= 128;   // small domains: one warp per item
+                const int nEx = lenK - kTupleHead;
+                const int exDir = 1 - stp.dir;
+                int ordinal = 0;
+                for (int base = 0; base < cut; base += 32) {
+                    const int i = base + lane;
+                    unsigned bal = __ballot_sync(0xffffffffu, i < cut && sm.wBeg[i] <= -2);
+                    while (bal) {
+                        const int item = base + __ffs(bal) - 1;
+                        bal &= bal - 1;
+                        const int mine = ordinal++;
+                        if (perWarp && mine % kWarps != warp) continue;
+                        const int* par = baseK + (w0 + item) * strideK;
+                        // hO must differ from every bound value: their ranks in hO's domain
+                        int* ex = S.exRank[warp];
+                        if (lane < nEx) {
+                            const int2 r = row_lookup(ix, stp.pred, exDir, par[kTupleHead + lane], mt);
+                            ex[lane] = r.y > r.x ? __ldg(ix.srcRank[exDir] + r.x) : -1;
+                        }
+                        __syncwarp();
+                        const int h = -2 - sm.wBeg[item];
+                        const uint32_t* hb = ix.hubBits + __ldg(ix.hubOff + h);
+                        uint32_t* dst = bm + (rowBase + par[0]) * (long long)words;
+                        const int w0b = perWarp ? lane : tid;
+                        const int step = perWarp ? 32 : B;
+                        for (int w = w0b; w < words; w += step) {
+                            uint32_t m = __ldg(hb + w);
+                            for (int q = 0; q < nEx; ++q)
+                                if ((ex[q] >> 5) == w && ex[q] >= 0) m &= ~(1u << (ex[q] & 31));
+                            mt.add(4);
+                            if (m) {
+                                const uint32_t old = atomicOr(dst + w, m);
+                                if (!shared) mt.add(8);
+                                myNew += (unsigned long long)__popc(m & ~old);
+                            }
+                        }
+                        __syncwarp();
+                    }
+                }
             }
             __syncthreads();
             if (tid == 0) {

@@ -220,6 +220,7 @@ bool finish_capacity(DevPlan& P, const Geom& geom) {
     P.cap = std::max(((pool - bitmapInts) / sum) & ~31, 32);
     P.bitmapOff = pool - bitmapInts;
     P.groupMax = std::min(groupMax, P.cap);
+    P.rowWords = P.mode == kPairs ? std::max(1, (P.wo + 31) / 32) : 1;
     return local;
 }
 

@@ -99,7 +99,7 @@ struct Server {
             size_t roots = (size_t)std::max(1, ph->rootEnd - ph->rootBeg);
             size_t tasks = roots / (size_t)std::max(1, std::min(P.groupMax, P.cap)) + 1;
             b += sizeof(DevPlan) + 8 + tasks * sizeof(DevTask) * 2;
-            if (ph->needsGlobalBitmap) b += roots * (size_t)P.wo / 8 + 4;
+            if (ph->needsGlobalBitmap) b += roots * (size_t)std::max(P.rowWords, 1) * 4;
         }
         return b;
     }

@@ -176,3 +176,29 @@ def test_fuzz_forced_splitting(name, block, tmp_path):
         res, st, _ = lib.evaluate_rules_batch(fx["rules"])
         _check(res, fx["expected"], f"batch split block={block}")
         _check([lib.evaluate_rule(t) for t in fx["rules"][:60]], fx["expected"][:60], "per-rule split")
+
+
+@pytest.mark.parametrize("hub_min", ["1", "0"])
+def test_hub_rows_everywhere_or_nowhere(hub_min, tmp_path, monkeypatch):
+    """Body sizes through hub-row bitmaps (every row a hub) and without any,
+    on the fuzz graphs, the edge cases and c2s, against the reference."""
+    monkeypatch.setenv("GPU_RULES_HUB_MIN_DEGREE", hub_min)
+    for name in fuzz_names():
+        fx = load_fixture(name)
+        p = tmp_path / f"{name}.ttl"
+        p.write_text(fx["ttl"])
+        with eng.GpuRulesLib(p) as lib:
+            res, st, _ = lib.evaluate_rules_batch(fx["rules"])
+            _check(res, fx["expected"], f"{name} hub_min={hub_min} batch")
+            _check([lib.evaluate_rule(t) for t in fx["rules"][:40]], fx["expected"][:40], f"{name} per-rule")
+    fx = load_fixture("edge_cases.json")
+    p = tmp_path / "edge.ttl"
+    p.write_text(fx["ttl"])
+    with eng.GpuRulesLib(p) as lib:
+        res, _, _ = lib.evaluate_rules_batch([c["rule"] for c in fx["cases"]])
+        _check(res, [c["expected"] for c in fx["cases"]], f"edge hub_min={hub_min}")
+    fx = load_fixture("synthetic_c2s.json")
+    d = synth.generate("c2s", tmp_path / "c2s", seed=fx["seed"])
+    with eng.GpuRulesLib(d / "graph.ttl") as lib:
+        res, _, _ = lib.evaluate_rules_batch(fx["rules"])
+        _check(res, fx["expected"], f"c2s hub_min={hub_min}")
