@@ -159,6 +159,10 @@ struct Geom {
 struct EngineProfile {
     unsigned long long* bytes = nullptr;
     unsigned long long* taskNs = nullptr;
+    // Launch span (any variant): span[0] = max of ~start over blocks (so a
+    // zeroed word works as the initial value), span[1] = max block end,
+    // both in device global-timer ns.
+    unsigned long long* span = nullptr;
 };
 
 }  // namespace gr

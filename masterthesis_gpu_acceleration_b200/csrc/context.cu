@@ -36,7 +36,7 @@ void set_error(const std::string& s) {
 }
 
 void Staged::stage(Context& c, std::vector<DevPlan>& plans, const std::vector<const PhasePlan*>& phases,
-                   bool sortTasks, cudaStream_t s, double walkBudget) {
+                   bool sortTasks, cudaStream_t s, double walkBudget, bool costAware) {
     nPlans = (int)plans.size();
     nTasks = 0;
     bitmapWords = 0;
@@ -52,7 +52,7 @@ void Staged::stage(Context& c, std::vector<DevPlan>& plans, const std::vector<co
     cudaStream_t as = streamOrdered ? s : nullptr;
     if (bitmapWords) dBitmap.ensure(bitmapWords * 4, as);
     std::vector<PhaseTasks> pts;
-    c.tasks->build(phases, c.grid, true, pts, walkBudget);
+    c.tasks->build(phases, c.grid, true, pts, walkBudget, costAware);
     std::vector<size_t> hOff(nPlans, 0);
     heavyWords = 0;
     for (int i = 0; i < nPlans; ++i) {
@@ -85,6 +85,11 @@ void Staged::stage(Context& c, std::vector<DevPlan>& plans, const std::vector<co
         cost.swap(c2);
     }
     nTasks = (int)tasks.size();
+    planTaskEnd.clear();
+    if (!sortTasks) {
+        int32_t acc = 0;
+        for (int i = 0; i < nPlans; ++i) planTaskEnd.push_back(acc += (int32_t)pts[i].tasks.size());
+    }
     hTasks = tasks;
     hCost = cost;
     size_t planBytes = (size_t)nPlans * sizeof(DevPlan);
@@ -128,6 +133,34 @@ void Staged::enqueue(Context& c, cudaStream_t s, int instr, int gridCap) {
        "engine launch");
 }
 
+void Staged::enqueue_per_plan(Context& c, cudaStream_t s) {
+    if (!nPlans) return;
+    if (nPlans > kMaxPerPlan || (int)planTaskEnd.size() != nPlans) throw CudaError("bad per-plan staging");
+    // control words: [0..1] task counters, [2] status (int), then per plan
+    // two u64 span words at byte 16 + 16 * i; all start at zero
+    ck(cudaMemsetAsync(dResults.p, 0, (size_t)nPlans * sizeof(unsigned long long), s), "memset results");
+    ck(cudaMemsetAsync(dCtl.p, 0, 16 + 16 * kMaxPerPlan, s), "memset ctl");
+    if (bitmapWords) ck(cudaMemsetAsync(dBitmap.p, 0, bitmapWords * 4, s), "memset bitmap");
+    if (heavyWords) ck(cudaMemsetAsync(dHeavy.p, 0, heavyWords * 4, s), "memset heavy rows");
+    int* ctl = static_cast<int*>(dCtl.p);
+    for (int i = 0; i < nPlans; ++i) {
+        const int32_t b = i ? planTaskEnd[i - 1] : 0, e = planTaskEnd[i];
+        EngineProfile prof;
+        prof.span = reinterpret_cast<unsigned long long*>(static_cast<char*>(dCtl.p) + 16 + 16 * i);
+        const int grid = std::max(1, std::min(e - b, c.grid));
+        ck(engine_launch(c.dix, dPlans, dTasks + b, e - b, ctl + i, static_cast<unsigned long long*>(dResults.p),
+                         ctl + 2, grid, c.geom.block, s, &prof),
+           "engine launch");
+    }
+}
+
+void Staged::download_spans(cudaStream_t s) {
+    if (!nPlans) return;
+    ck(cudaMemcpyAsync(hResults.p, dResults.p, nPlans * sizeof(unsigned long long), cudaMemcpyDeviceToHost, s),
+       "D2H results");
+    ck(cudaMemcpyAsync(hCtl.p, dCtl.p, 16 + 16 * kMaxPerPlan, cudaMemcpyDeviceToHost, s), "D2H status");
+}
+
 void compose(const RulePlan& rp, int64_t sup, int64_t body, double supMs, double confMs, GpuRuleResult* out) {
     *out = GpuRuleResult{};
     out->headSize = (int)clamp_int(rp.headSize);
@@ -148,7 +181,7 @@ namespace {
 // One phase in its own launch (the plain per-rule form), timed by events.
 int64_t run_one_phase(Context& c, const PhasePlan& ph, float* ms) {
     std::vector<DevPlan> plans{ph.plan};
-    c.one.stage(c, plans, {&ph}, false, c.stream);
+    c.one.stage(c, plans, {&ph}, false, c.stream, c.ruleWalkBudget, true);
     ck(cudaEventRecord(c.ev[0], c.stream), "event");
     c.one.enqueue(c, c.stream, 0);
     ck(cudaEventRecord(c.ev[1], c.stream), "event");
@@ -159,12 +192,30 @@ int64_t run_one_phase(Context& c, const PhasePlan& ph, float* ms) {
     return (int64_t)c.one.counts()[0];
 }
 
+// Both phases of one rule, each in its own launch timed by its own events,
+// issued back to back with one host synchronisation.
 int evaluate_parsed(Context& c, const Rule& rule, GpuRuleResult* out) {
     RulePlan rp = plan_rule(rule, c.hix, c.geom);
     int64_t sup = rp.support.value, body = rp.body.value;
     float supMs = 0.f, confMs = 0.f;
-    if (rp.status == kRuleOk && rp.support.how == kDevice) sup = run_one_phase(c, rp.support, &supMs);
-    if (rp.status == kRuleOk && rp.body.how == kDevice) body = run_one_phase(c, rp.body, &confMs);
+    const bool runS = rp.status == kRuleOk && rp.support.how == kDevice;
+    const bool runB = rp.status == kRuleOk && rp.body.how == kDevice;
+    std::vector<DevPlan> plans;
+    std::vector<const PhasePlan*> phases;
+    if (runS) { plans.push_back(rp.support.plan); phases.push_back(&rp.support); }
+    if (runB) { plans.push_back(rp.body.plan); phases.push_back(&rp.body); }
+    if (!plans.empty()) {
+        // one upload, one launch per phase (each timed on the device), one download
+        c.one.stage(c, plans, phases, false, c.stream, c.ruleWalkBudget, true);
+        c.one.enqueue_per_plan(c, c.stream);
+        c.one.download_spans(c.stream);
+        ck(cudaStreamSynchronize(c.stream), "engine");
+        if (static_cast<const int*>(c.one.hCtl.p)[2] != 0)
+            throw CudaError("engine reported internal status " + std::to_string(static_cast<const int*>(c.one.hCtl.p)[2]));
+        int k = 0;
+        if (runS) { sup = (int64_t)c.one.counts()[k]; supMs = (float)c.one.span_ms(k); ++k; }
+        if (runB) { body = (int64_t)c.one.counts()[k]; confMs = (float)c.one.span_ms(k); }
+    }
     compose(rp, sup, body, supMs, confMs, out);
     return 0;
 }
@@ -544,6 +595,7 @@ int gpu_set_option(void* ctx, const char* name, long long value) {
     if (n == "task_target" && value >= 0) { c.tasks->forceTarget = (double)value; return 0; }
     if (n == "walk_threshold" && value >= 0) { c.tasks->walkThreshold = (double)value; return 0; }
     if (n == "serve_lanes" && (value == 0 || value == 1)) { c.serveLanes = (int)value; return 0; }
+    if (n == "rule_walk_budget" && value >= 0) { c.ruleWalkBudget = (double)value; return 0; }
     if (n == "serve_heavy_share" && value >= 1 && value <= 16) { c.serveHeavyShare = (int)value; return 0; }
     if (n == "serve_heavy_us" && value >= 0) { c.serveHeavyNs = 1e3 * (double)value; return 0; }
     return -1;

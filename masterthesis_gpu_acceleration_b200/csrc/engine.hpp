@@ -108,15 +108,29 @@ struct Staged {
     size_t bitmapWords = 0, heavyWords = 0;
     size_t h2dBytes = 0, d2hBytes = 0;
     bool streamOrdered = false;   // grow device buffers on the launch stream (serving slots)
+    std::vector<int32_t> planTaskEnd;   // tasks in plan order (unsorted staging): end of each plan's tasks
 
     // walkBudget: how much per-root measurement the task builder may do
     // (prepared batches afford more than one-shot or served launches).
     void stage(Context& c, std::vector<DevPlan>& plans, const std::vector<const PhasePlan*>& phases,
-               bool sortTasks, cudaStream_t s, double walkBudget = 4.0e6);
+               bool sortTasks, cudaStream_t s, double walkBudget = 4.0e6, bool costAware = false);
     // instr: 0 plain, 1 task times into dTaskNs, 2 also algorithmic bytes
     // into dBytes.  gridCap > 0 limits the launch to that many blocks (a
     // share of the SMs).
     void enqueue(Context& c, cudaStream_t s, int instr, int gridCap = 0);
+    // One launch per plan of an unsorted staging (at most kMaxPerPlan plans),
+    // each with its own task counter and launch span in the control words;
+    // download_spans then brings results, status and spans back in two
+    // copies.  The plain per-rule form: support and body size of one rule.
+    static constexpr int kMaxPerPlan = 2;
+    void enqueue_per_plan(Context& c, cudaStream_t s);
+    void download_spans(cudaStream_t s);
+    // Device span (ms) of plan i's launch after download_spans and a sync.
+    double span_ms(int i) const {
+        const unsigned long long* w = static_cast<const unsigned long long*>(hCtl.p) + 2 + 2 * i;
+        const unsigned long long t0 = ~w[0], t1 = w[1];
+        return t1 > t0 ? (double)(t1 - t0) * 1e-6 : 0.0;
+    }
     // Pre-sizes the buffers so that launches up to this size never resize
     // (freeing device or pinned memory synchronises the whole device).
     void reserve(size_t plans, size_t tasks, cudaStream_t s = nullptr) {
@@ -157,6 +171,7 @@ struct Context {
     std::vector<struct Batch*> pipe;  // reusable chunks of one-shot batches
     std::unique_ptr<TaskBuilder> tasks;
     Geom geom;
+    double ruleWalkBudget = 4.0e6;   // per-root measurement allowed per plain per-rule launch
     int serveLanes = 1;        // servers started on this context keep a heavy lane
     int serveHeavyShare = 2;   // the heavy lane launches on grid / serveHeavyShare blocks
     double serveHeavyNs = 5.0e6;

@@ -550,6 +550,7 @@ engine_kernel(DevIndex ix, const DevPlan* __restrict__ plans, const DevTask* __r
     extern __shared__ __align__(16) unsigned char smem_raw[];
     Smem<B>& sm = *reinterpret_cast<Smem<B>*>(smem_raw);
     Meter<kC> mt;
+    if (prof.span && threadIdx.x == 0) atomicMax(prof.span, ~global_ns());
     for (;;) {
         if (threadIdx.x == 0) sm.st.task = atomicAdd(taskCounter, 1);
         __syncthreads();
@@ -581,6 +582,7 @@ engine_kernel(DevIndex ix, const DevPlan* __restrict__ plans, const DevTask* __r
         for (int d = 16; d; d >>= 1) b += __shfl_down_sync(0xffffffffu, b, d);
         if ((threadIdx.x & 31) == 0 && b && prof.bytes) atomicAdd(prof.bytes, b);
     }
+    if (prof.span && threadIdx.x == 0) atomicMax(prof.span + 1, global_ns());
 }
 
 template <int B>
@@ -614,17 +616,18 @@ static void launch_b(const DevIndex& ix, const DevPlan* plans, const DevTask* ta
                      unsigned long long* results, int* status, int grid, cudaStream_t stream,
                      const EngineProfile* prof) {
     const size_t smem = sizeof(Smem<B>);
-    if (prof && prof->bytes)
-        engine_kernel<B, 2><<<grid, B, smem, stream>>>(ix, plans, tasks, nTasks, taskCounter, results, status, *prof);
-    else if (prof)
-        engine_kernel<B, 1><<<grid, B, smem, stream>>>(ix, plans, tasks, nTasks, taskCounter, results, status, *prof);
+    const EngineProfile p = prof ? *prof : EngineProfile{};
+    if (p.bytes)
+        engine_kernel<B, 2><<<grid, B, smem, stream>>>(ix, plans, tasks, nTasks, taskCounter, results, status, p);
+    else if (p.taskNs)
+        engine_kernel<B, 1><<<grid, B, smem, stream>>>(ix, plans, tasks, nTasks, taskCounter, results, status, p);
     else
-        engine_kernel<B, 0><<<grid, B, smem, stream>>>(ix, plans, tasks, nTasks, taskCounter, results, status,
-                                                       EngineProfile{});
+        engine_kernel<B, 0><<<grid, B, smem, stream>>>(ix, plans, tasks, nTasks, taskCounter, results, status, p);
 }
 
-// prof != null selects an instrumented variant: task times, and byte counts
-// when prof->bytes is set.
+// prof (optional): task times when prof->taskNs is set, also byte counts
+// when prof->bytes is set (instrumented variants); a launch span when
+// prof->span is set (any variant).
 cudaError_t engine_launch(const DevIndex& ix, const DevPlan* plans, const DevTask* tasks, int nTasks,
                           int* taskCounter, unsigned long long* results, int* status, int grid, int block,
                           cudaStream_t stream, const EngineProfile* prof) {

@@ -132,9 +132,12 @@ static int32_t resolve(const DevPlan& P, TermRef ref, const int32_t* vals, int32
     return ref == P.tupleLen[0] ? n0 : n1;
 }
 
-std::pair<int32_t, int32_t> TaskBuilder::first_segment(const DevPlan& P, const int32_t* vals) const {
+std::pair<int32_t, int32_t> TaskBuilder::first_segment(const DevPlan& P, int32_t r, const int32_t* vals) const {
     const DevStep& st = P.steps[0];
     if (st.kind == kScan) return {ix_.predEdge[0][st.pred], ix_.predEdge[0][st.pred + 1]};
+    // the first step expands the root's own row: no lookup
+    if (P.rootKind == kRootRows && P.rootDir == st.dir && P.rootPred == st.pred && st.keyRef == kTupleHead)
+        return {ix_.rowBeg[st.dir][r], ix_.rowBeg[st.dir][r + 1]};
     return ix_.row_range(st.pred, st.dir, resolve(P, st.keyRef, vals, -1, -1));
 }
 
@@ -169,7 +172,7 @@ const std::vector<float>& TaskBuilder::walk(const PhasePlan& ph) {
     int32_t vals[2];
     for (int32_t r = ph.rootBeg; r < ph.rootEnd; ++r) {
         root_vals(P, r, vals);
-        auto seg = first_segment(P, vals);
+        auto seg = first_segment(P, r, vals);
         double acc = 1.0;
         if (P.m < 2) acc += seg.second - seg.first;
         else if (chain) {
@@ -184,7 +187,7 @@ const std::vector<float>& TaskBuilder::walk(const PhasePlan& ph) {
 }
 
 void TaskBuilder::build(const std::vector<const PhasePlan*>& phases, int blocks, bool split,
-                        std::vector<PhaseTasks>& out, double walkBudget) {
+                        std::vector<PhaseTasks>& out, double walkBudget, bool costAware) {
     size_t n = phases.size();
     out.assign(n, PhaseTasks{});
     if (cacheBytes_ > kCacheLimit) {  // only here: walks hand out references into the cache
@@ -227,6 +230,9 @@ void TaskBuilder::build(const std::vector<const PhasePlan*>& phases, int blocks,
                            (s0.kind == kExpand ? std::max(1.0, ix_.avg_degree(s0.pred, s0.dir)) : (double)ix_.pred_size(s0.pred));
             const bool cached = walks_.count(signature(ph)) != 0;
             if (!forced[i] && !cached && used + edges > walkBudget) continue;
+            // a walk whose own cost exceeds the phase's expected device time
+            // cannot pay for itself (a single rule on the whole GPU)
+            if (costAware && !cached && estAvg[i] * scale[i] < kWalkNsPerEdge * edges) continue;
             if (!cached) used += edges;   // cached walks cost nothing
             walked[i] = &walk(ph);
             double s = 0;
@@ -282,7 +288,7 @@ void TaskBuilder::build(const std::vector<const PhasePlan*>& phases, int blocks,
                 flush(r);
                 int32_t vals[2];
                 root_vals(P, r, vals);
-                auto seg = first_segment(P, vals);
+                auto seg = first_segment(P, r, vals);
                 double tail = 1.0;
                 for (int s = 2; s < P.m; ++s) tail *= std::max(1.0, avg_fan(P.steps[s]));
                 const int32_t* deg2 =

@@ -30,6 +30,9 @@ struct PhaseTasks {
 // at most `target` (about 1/8 of a block's fair share of the batch); a root
 // heavier than that is split into slices of its first segment, each a task
 // of its own that deduplicates in a global row.
+// Host time of one step of a per-root walk (ns), for the cost-aware mode.
+constexpr double kWalkNsPerEdge = 8.0;
+
 class TaskBuilder {
 public:
     explicit TaskBuilder(const HostIndex& ix) : ix_(ix) {}
@@ -38,8 +41,10 @@ public:
     // launch.  split=false keeps every root in shared-memory tasks.
     // walkBudget: first-segment edges that may be newly walked (cached
     // walks and phases marked by learn() are not counted).
+    // costAware: walk a phase only when its expected device time exceeds
+    // the walk's own host time (per-rule launches, where nothing overlaps).
     void build(const std::vector<const PhasePlan*>& phases, int blocks, bool split,
-               std::vector<PhaseTasks>& out, double walkBudget = 4.0e6);
+               std::vector<PhaseTasks>& out, double walkBudget = 4.0e6, bool costAware = false);
 
     size_t cache_bytes() const { return cacheBytes_; }
 
@@ -100,7 +105,7 @@ private:
     const std::vector<float>& walk(const PhasePlan& ph);
     double child_work(const DevPlan& P, const int32_t* rootVals, int32_t e, const int32_t* deg2, double tail) const;
     int root_vals(const DevPlan& P, int32_t r, int32_t* vals) const;
-    std::pair<int32_t, int32_t> first_segment(const DevPlan& P, const int32_t* vals) const;
+    std::pair<int32_t, int32_t> first_segment(const DevPlan& P, int32_t r, const int32_t* vals) const;
 };
 
 }  // namespace gr
