@@ -71,6 +71,8 @@ def parse_args():
     ap.add_argument("--max-rules", type=int, default=0, help="use only the first N rules (profiling case)")
     ap.add_argument("--serve-seconds", type=float, default=1.5, help="seconds per offered rate in the serving sweep")
     ap.add_argument("--no-serve", action="store_true")
+    ap.add_argument("--no-gpu03", action="store_true",
+                    help="skip the reference GPU library (GPU_03) per-rule comparator")
     ap.add_argument("--data", default=os.environ.get("KG_DATA_DIR", str(Path(tempfile.gettempdir()) / "kg_synth_data")))
     return ap.parse_args()
 
@@ -239,13 +241,45 @@ def serving_sweep(lib, d: Path, args) -> dict:
     pc = synth.pred_counts(synth.read_triples(d), n_pred)
     sd = synth.rule_stream(pc, 20000, Path(args.data) / "c5_stream", p=0.4, max_len=8, seed=1)
     rules = synth.read_rules(sd)
-    rates = [1000, 5000, 20000, 50000]
+    rates = [1000, 2000, 5000, 10000, 20000, 50000]
     rows, res = serving.sweep(lib, rules, rates, duration=args.serve_seconds, seed=11)
     check = check_sample(d, sd, res, n_pred)
     return {"workload": "c5-shaped stream on the c3 graph: 20,000 chain rules, lengths geometric(0.4) in 1..8, "
                         "predicates by frequency, open-loop Poisson arrivals",
             "seconds_per_rate": args.serve_seconds, "slots": "4 (3 light + 1 heavy lane)", "rates": rows,
             "oracle_check_1pct": check}
+
+
+def gpu03_comparator(d: Path, per_rule: dict | None, timeout: float = 600.0) -> dict:
+    """The reference's own GPU library (GPU_03, built from its sources for
+    sm_100a by baseline/build_gpu03.sh) on every rule, one call per rule, in a
+    separate process.  GPU_03 skips the body size when support is 0 and
+    differs from CPU_01 on rules that reuse the head triple or hold
+    constants, so it does less work than this engine on most rules; its
+    results are counted against the reference fixture, not required to match."""
+    lib = ROOT / "baseline" / "_ref" / "gpu03" / "libgpu_rules.so"
+    if not lib.exists():
+        return {"unavailable": "baseline/_ref/gpu03/libgpu_rules.so not built (baseline/build_gpu03.sh)"}
+    r = subprocess.run([sys.executable, str(ROOT / "baseline" / "gpu03.py"), str(d / "graph.ttl"),
+                        str(d / "rules.txt"), "--stride", "1", "--max-seconds", "240"],
+                       capture_output=True, text=True, timeout=timeout)
+    lines = r.stdout.strip().splitlines()
+    if r.returncode != 0 or not lines:
+        return {"unavailable": f"GPU_03 run failed (rc {r.returncode})"}
+    g = json.loads(lines[-1])
+    if "unavailable" in g:
+        return g
+    out = {k: g[k] for k in ("rules", "wall_s", "device_ms", "rules_per_s_wall", "rules_per_s_device")}
+    gold = ROOT / "tests" / "golden" / "c3_seed0.npz"
+    if gold.exists():
+        exp = np.load(gold)["expected"].tolist()
+        res = g["results"]
+        out["equal_to_reference_cpu"] = sum(1 for a, b in zip(res, exp) if a == b)
+        out["support_equal_to_reference_cpu"] = sum(1 for a, b in zip(res, exp) if a and a[0] == b[0])
+    if per_rule:
+        out["engine_per_rule_speedup_wall"] = per_rule["rules_per_s_wall"] / out["rules_per_s_wall"]
+    out["api"] = "GPU_03 gpu_evaluate_rule, one call per rule (the reference library's calling pattern)"
+    return out
 
 
 def reference_arm(args):
@@ -401,6 +435,12 @@ def engine_arm(args):
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         cpu = cpu_baseline(d, rules, args.config)
 
+    gpu03 = None
+    if rank == 0 and world == 1 and not args.no_gpu03 and args.config == "c3" and not args.max_rules:
+        gpu03 = gpu03_comparator(d, per_rule)
+        if "rules_per_s_wall" in gpu03:
+            gpu03["engine_batched_speedup_wall"] = value / gpu03["rules_per_s_wall"]
+
     serving = None
     if rank == 0 and world == 1 and not args.no_serve and args.config == "c3":
         serving = serving_sweep(lib, d, args)
@@ -419,6 +459,7 @@ def engine_arm(args):
                        "exact_vs_reference_golden": exact, "plans": info["plans"], "tasks": info["tasks"]},
             "e2e": e2e,
             "per_rule": per_rule,
+            "reference_gpu_per_rule": gpu03,
             "serving": serving,
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": peaks["hbm_gbs"], "unit": "GB/s",
                          "frac": achieved / peaks["hbm_gbs"], "traffic": traffic,
