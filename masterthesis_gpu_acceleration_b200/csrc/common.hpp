@@ -128,7 +128,10 @@ struct DevPlan {
     int64_t gRowBase;             // first root of the plan, for global bitmap rows
     uint32_t* gHeavy;             // global dedup rows of split heavy roots
     int32_t rowWords;             // words per heavy row (kPairs: ceil(wo / 32); kExist: 1)
-    int32_t pad1;
+    int32_t memoLevel;            // kPairs ending in two expand steps: level + 1 whose items may
+                                  // use a suffix memo (0: none; see memo_item)
+    const int32_t* memoTab;       // per hub row: memo slot or -1 (null: no memo)
+    const uint32_t* memoBits;     // per slot: S1 then S2, rowWords words each
 };
 
 // A unit of device work: the roots [beg, end) of one plan.  A heavy root is

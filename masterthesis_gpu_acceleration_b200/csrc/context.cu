@@ -51,6 +51,13 @@ void Staged::stage(Context& c, std::vector<DevPlan>& plans, const std::vector<co
     }
     cudaStream_t as = streamOrdered ? s : nullptr;
     if (bitmapWords) dBitmap.ensure(bitmapWords * 4, as);
+    // suffix memos first: the task builder weighs memoised roots by them
+    for (int i = 0; i < nPlans; ++i)
+        if (plans[i].memoLevel > 0) {
+            const DevStep& a = plans[i].steps[plans[i].m - 2];
+            const DevStep& b = plans[i].steps[plans[i].m - 1];
+            c.memo_for(a.pred, a.dir, b.pred, b.dir, s);
+        }
     std::vector<PhaseTasks> pts;
     c.tasks->build(phases, c.grid, true, pts, walkBudget, costAware);
     std::vector<size_t> hOff(nPlans, 0);
@@ -64,6 +71,17 @@ void Staged::stage(Context& c, std::vector<DevPlan>& plans, const std::vector<co
     std::vector<DevTask> tasks;
     std::vector<double> cost;
     for (int i = 0; i < nPlans; ++i) {
+        plans[i].memoTab = nullptr;
+        plans[i].memoBits = nullptr;
+        if (plans[i].memoLevel > 0) {
+            const DevStep& a = plans[i].steps[plans[i].m - 2];
+            const DevStep& b = plans[i].steps[plans[i].m - 1];
+            const SuffixMemo* m = c.memo_for(a.pred, a.dir, b.pred, b.dir, s);
+            if (m && m->words == plans[i].rowWords) {
+                plans[i].memoTab = m->tab;
+                plans[i].memoBits = m->bits;
+            }
+        }
         plans[i].resultSlot = i;
         plans[i].gBitmap = phases[i]->needsGlobalBitmap ? static_cast<uint32_t*>(dBitmap.p) + gOff[i] : nullptr;
         plans[i].gRowBase = phases[i]->needsGlobalBitmap ? phases[i]->rootBeg : 0;
@@ -108,6 +126,55 @@ void Staged::stage(Context& c, std::vector<DevPlan>& plans, const std::vector<co
     dTasks = reinterpret_cast<const DevTask*>(static_cast<const char*>(dBlob.p) + planBytes);
     h2dBytes = blob;
     d2hBytes = (size_t)nPlans * sizeof(unsigned long long) + 8;
+}
+
+const SuffixMemo* Context::memo_for(int p1, int d1, int p2, int d2, cudaStream_t s) {
+    const uint64_t key = ((uint64_t)(uint32_t)(p1 * 2 + d1) << 32) | (uint32_t)(p2 * 2 + d2);
+    auto it = memos.find(key);
+    if (it != memos.end()) return it->second.get();
+    memos[key] = nullptr;
+    const HostIndex& h = hix;
+    const int nHub = (int)h.hubOff.size();
+    if (memoGain < 0 || nHub == 0 || p1 < 0 || p2 < 0 || p1 >= h.nPred || p2 >= h.nPred) return nullptr;
+    const int words = (int)((h.pred_rows(p2, 1 - d2) + 31) / 32);
+    std::vector<int2> jobs;
+    std::vector<int32_t> tab(nHub, -1);
+    for (int32_t r = h.predRow[d1][p1]; r < h.predRow[d1][p1 + 1]; ++r) {
+        const int32_t hub = h.hubOf[d1][r];
+        if (hub < 0) continue;
+        double cand = 0;   // suffix candidates of this row: sum of the second-step degrees
+        for (int32_t e = h.rowBeg[d1][r]; e < h.rowBeg[d1][r + 1]; ++e) {
+            auto rr = h.row_range(p2, d2, h.val[d1][e]);
+            cand += rr.second - rr.first;
+        }
+        if (cand < memoGain * words) continue;
+        tab[hub] = (int32_t)jobs.size();
+        jobs.push_back(make_int2(r, (int)jobs.size()));
+    }
+    const size_t tabBytes = ((size_t)nHub * 4 + 255) & ~size_t(255);
+    const size_t jobBytes = ((jobs.size() * sizeof(int2)) + 255) & ~size_t(255);
+    const size_t bitBytes = jobs.size() * 2 * (size_t)words * 4;
+    if (jobs.empty() || memoBytes + bitBytes > kMemoBudgetBytes) return nullptr;
+    auto m = std::make_unique<SuffixMemo>();
+    m->rowHasMemo.assign((size_t)h.pred_rows(p1, d1), 0);
+    for (const int2& j : jobs) m->rowHasMemo[(size_t)(j.x - h.predRow[d1][p1])] = 1;
+    m->buf.ensure(tabBytes + jobBytes + bitBytes);
+    char* base = static_cast<char*>(m->buf.p);
+    ck(cudaMemcpyAsync(base, tab.data(), (size_t)nHub * 4, cudaMemcpyHostToDevice, s), "H2D memo table");
+    ck(cudaMemcpyAsync(base + tabBytes, jobs.data(), jobs.size() * sizeof(int2), cudaMemcpyHostToDevice, s),
+       "H2D memo jobs");
+    ck(cudaMemsetAsync(base + tabBytes + jobBytes, 0, bitBytes, s), "clear memo bits");
+    ck(memo_build(dix, p1, d1, p2, d2, reinterpret_cast<const int2*>(base + tabBytes), (int)jobs.size(),
+                  reinterpret_cast<uint32_t*>(base + tabBytes + jobBytes), words, s),
+       "memo build");
+    ck(cudaStreamSynchronize(s), "memo build");   // memos are shared by every stream afterwards
+    m->tab = reinterpret_cast<const int32_t*>(base);
+    m->bits = reinterpret_cast<const uint32_t*>(base + tabBytes + jobBytes);
+    m->words = words;
+    m->slots = (int)jobs.size();
+    memoBytes += m->buf.cap;
+    memos[key] = std::move(m);
+    return memos[key].get();
 }
 
 void Staged::enqueue(Context& c, cudaStream_t s, int instr, int gridCap) {
@@ -357,11 +424,20 @@ void* gpu_load_graph(const char* ttlPath) {
             return nullptr;
         }
         c->prefixes = scan_rule_prefixes(ttlPath);
+        // GPU_RULES_MEMO_GAIN overrides the suffix-memo threshold (negative: no memos)
+        if (const char* g = std::getenv("GPU_RULES_MEMO_GAIN")) c->memoGain = std::atof(g);
         // GPU_RULES_HUB_MIN_DEGREE overrides the hub-row threshold (0: no hub rows)
         int32_t hubMin = kHubMinDegree;
         if (const char* h = std::getenv("GPU_RULES_HUB_MIN_DEGREE")) hubMin = std::max(0, std::atoi(h));
         c->hix = build_index(spo, (int32_t)c->ents.size(), (int32_t)c->preds.size(), hubMin);
         c->tasks.reset(new TaskBuilder(c->hix));
+        c->tasks->memoRows = [c](int p1, int d1, int p2, int d2, double* cost) -> const std::vector<uint8_t>* {
+            const uint64_t key = ((uint64_t)(uint32_t)(p1 * 2 + d1) << 32) | (uint32_t)(p2 * 2 + d2);
+            auto it = c->memos.find(key);
+            if (it == c->memos.end() || !it->second) return nullptr;
+            *cost = it->second->words / 4.0 + 8.0;   // a memo word costs about a quarter of a candidate
+            return &it->second->rowHasMemo;
+        };
         c->parser.reset(new RuleParser(c->ents, c->preds, c->prefixes));
         c->init_device();
         c->upload_index();

@@ -25,6 +25,8 @@ namespace gr {
 
 size_t engine_smem_bytes(int block);
 cudaError_t engine_configure();
+cudaError_t memo_build(const DevIndex& ix, int p1, int d1, int p2, int d2, const int2* jobs, int nJobs,
+                       uint32_t* bits, int words, cudaStream_t stream);
 cudaError_t engine_launch(const DevIndex& ix, const DevPlan* plans, const DevTask* tasks, int nTasks,
                           int* taskCounter, unsigned long long* results, int* status, int grid, int block,
                           cudaStream_t stream, const EngineProfile* prof);
@@ -158,6 +160,20 @@ struct Staged {
     }
 };
 
+// Suffix memo of one predicate transition (p1, d1) -> (p2, d2): per hub row
+// of (p1, d1) worth it, the S1/S2 bitmaps over (p2, 1 - d2)'s rows (see
+// memo_item in kernels.cu).  Built once per context, never moved.
+constexpr size_t kMemoBudgetBytes = size_t(1) << 30;   // all suffix memos of a context
+
+struct SuffixMemo {
+    DevBuf buf;
+    const int32_t* tab = nullptr;
+    const uint32_t* bits = nullptr;
+    int words = 0;
+    int slots = 0;
+    std::vector<uint8_t> rowHasMemo;   // per row of (p1, d1), from the predicate's first row
+};
+
 struct Context {
     int device = 0;
     TermDict ents, preds;
@@ -172,6 +188,14 @@ struct Context {
     std::unique_ptr<TaskBuilder> tasks;
     Geom geom;
     double ruleWalkBudget = 4.0e6;   // per-root measurement allowed per plain per-rule launch
+    // suffix memos: a hub row gets one when its suffix candidates are at
+    // least memoGain x the memo's words (negative: no memos)
+    double memoGain = 0.25;
+    std::unordered_map<uint64_t, std::unique_ptr<SuffixMemo>> memos;
+    size_t memoBytes = 0;
+    // The memo for (p1, d1) -> (p2, d2), built (synchronously, on stream s)
+    // on first use; null when no hub row of (p1, d1) is worth one.
+    const SuffixMemo* memo_for(int p1, int d1, int p2, int d2, cudaStream_t s);
     int serveLanes = 1;        // servers started on this context keep a heavy lane
     int serveHeavyShare = 2;   // the heavy lane launches on grid / serveHeavyShare blocks
     double serveHeavyNs = 5.0e6;

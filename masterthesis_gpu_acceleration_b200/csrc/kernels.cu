@@ -104,6 +104,18 @@ __device__ __forceinline__ bool has_edge(const DevIndex& ix, int pred, int dir, 
     return lo < r.y && __ldg(v + lo) == target;
 }
 
+// Whether value x occurs in the sorted values v[beg, beg + len).
+template <bool kC>
+__device__ __forceinline__ bool seg_has(const int* v, int beg, int len, int x, Meter<kC>& mt) {
+    int lo = beg, hi = beg + len;
+    while (lo < hi) {
+        const int mid = (lo + hi) >> 1;
+        mt.add(4);
+        if (__ldg(v + mid) < x) lo = mid + 1; else hi = mid;
+    }
+    return lo < beg + len && __ldg(v + lo) == x;
+}
+
 template <bool kC, class Val>
 __device__ __forceinline__ bool pass_filters(const DevPlan& P, const DevIndex& ix, int lvl, Meter<kC>& mt, Val val) {
     const int cb = P.chkBeg[lvl], cn = P.chkN[lvl];
@@ -166,6 +178,81 @@ __device__ __forceinline__ unsigned long long block_sum(unsigned long long x, Bl
     if (threadIdx.x == 0)
         for (int w = 0; w < kWarps; ++w) t += st.red[w];
     return t;  // valid in thread 0
+}
+
+// One level-k item whose first suffix step expands a hub row x with a memo:
+// for the plan suffix x -[stA]-> y -[stB]-> hO, the memo holds, over hO's
+// rank domain, S1 = {h : at least one y in N1(x) with h in N2(y), h != y}
+// and S2 = {h : at least two such y}.  The item's valid hO are S1 minus the
+// ranks of its bound values (injectivity on hO) minus, when one bound value
+// y0 lies in N1(x) (injectivity on y), the h in N2(y0) that have no witness
+// but y0 (those outside S2).  Ranks within a row ascend with the values, so
+// each lane merges its own run of words with N2(y0)'s sorted ranks.  The
+// whole warp calls this; new pair bits are counted on insertion.
+template <bool kC>
+__device__ __noinline__ void memo_item(const DevPlan& P, const DevIndex& ix, const DevStep& stA,
+                                          const DevStep& stB, const int* par, int lenK, int slot, uint32_t* dst,
+                                          int words, int* ex, int lane, unsigned long long& myNew, Meter<kC>& mt,
+                                          bool sharedDst) {
+    const int nEx = lenK - kTupleHead;
+    const int exDir = 1 - stB.dir;
+    const int segBeg = par[lenK], segLen = par[lenK + 1];
+    bool isW = false;
+    if (lane < nEx) {
+        const int u = par[kTupleHead + lane];
+        const int2 r = row_lookup(ix, stB.pred, exDir, u, mt);
+        ex[lane] = r.y > r.x ? __ldg(ix.srcRank[exDir] + r.x) : -1;
+        isW = seg_has(ix.val[stA.dir], segBeg, segLen, u, mt);
+    }
+    const unsigned wmask = __ballot_sync(0xffffffffu, isW);
+    __syncwarp();
+    int e0 = 0, e1 = 0;
+    if (wmask) {
+        const int2 r = row_lookup(ix, stB.pred, stB.dir, par[kTupleHead + __ffs(wmask) - 1], mt);
+        e0 = r.x;
+        e1 = r.y;
+    }
+    const uint32_t* S1 = P.memoBits + (long long)slot * 2 * words;
+    const uint32_t* S2 = S1 + words;
+    const int* rk = ix.valRank[stB.dir];
+    const int per = (words + 31) >> 5;
+    const int wb = min(words, lane * per), we = min(words, wb + per);
+    int e = e0;
+    if (e1 > e0 && wb < we) {
+        int lo = e0, hi = e1;
+        const int key = wb << 5;
+        while (lo < hi) {
+            const int mid = (lo + hi) >> 1;
+            mt.add(4);
+            if (__ldg(rk + mid) < key) lo = mid + 1; else hi = mid;
+        }
+        e = lo;
+    }
+    for (int w = wb; w < we; ++w) {
+        uint32_t m = __ldg(S1 + w);
+        mt.add(4);
+        for (int q = 0; q < nEx; ++q)
+            if (ex[q] >= 0 && (ex[q] >> 5) == w) m &= ~(1u << (ex[q] & 31));
+        if (e < e1) {
+            const int lim = (w + 1) << 5;
+            uint32_t s2 = 0u;
+            bool s2Loaded = false;
+            while (e < e1) {
+                const int r = __ldg(rk + e);
+                if (r >= lim) break;
+                if (!s2Loaded) { s2 = __ldg(S2 + w); s2Loaded = true; mt.add(4); }
+                if (!((s2 >> (r & 31)) & 1u)) m &= ~(1u << (r & 31));
+                ++e;
+                mt.add(4);
+            }
+        }
+        if (m) {
+            const uint32_t old = atomicOr(dst + w, m);
+            if (!sharedDst) mt.add(8);
+            myNew += (unsigned long long)__popc(m & ~old);
+        }
+    }
+    __syncwarp();
 }
 
 template <int B, bool kC>
@@ -293,7 +380,12 @@ __device__ __forceinline__ void run_task(Smem<B>& sm, const DevIndex& ix, const 
             // candidates per word) instead of candidate by candidate.
             const bool hubPath = leaf && pairs && stp.hoWhich != 0 && stp.kind == kExpand && stp.nNew == 1 &&
                                  !hasFilters && ix.nHub > 0 && !(heavy && k == 0);
-            bool isHub = false;
+            // Memo path: the plan ends in two expand steps x -> y -> hO with
+            // nothing but injectivity to test; an item whose first segment
+            // is a hub row with a suffix memo is counted from the memo's
+            // "one witness y" / "two witnesses y" bitmaps (see below).
+            const bool memoPath = !leaf && pairs && P.memoTab != nullptr && k + 1 == P.memoLevel;
+            bool isHub = false;   // item marked for the hub or memo pass
 
             // window: the stored neighbour segment of each item
             int myBeg = 0;
@@ -323,6 +415,26 @@ __device__ __forceinline__ void run_task(Smem<B>& sm, const DevIndex& ix, const 
                             myLen = 0;
                         }
                     }
+                    if (memoPath && myLen > 0 && !(tid == 0 && S.curOff[k] != 0)) {
+                        const int row = __ldg(ix.predRow[stp.dir] + stp.pred) + __ldg(ix.srcRank[stp.dir] + myBeg);
+                        const int h = __ldg(ix.hubOf[stp.dir] + row);
+                        const int slot = h >= 0 ? __ldg(P.memoTab + h) : -1;
+                        mt.add(12);
+                        if (slot >= 0 && __ldg(ix.rowBeg[stp.dir] + row) == myBeg &&
+                            __ldg(ix.rowBeg[stp.dir] + row + 1) - myBeg == myLen) {
+                            // bound values that are also first-step neighbours are
+                            // witnesses the memo must not count; one is corrected
+                            // exactly, more fall back to enumeration
+                            int nR = 0;
+                            for (int q = kTupleHead; q < lenK && nR < 2; ++q)
+                                nR += seg_has(ix.val[stp.dir], myBeg, (int)myLen, it[q], mt) ? 1 : 0;
+                            if (nR <= 1) {
+                                isHub = true;
+                                myBeg = -2 - slot;
+                                myLen = 0;
+                            }
+                        }
+                    }
                     if (tid == 0 && !isHub) {
                         const long long off = S.curOff[k];
                         myBeg += (int)off;
@@ -330,7 +442,7 @@ __device__ __forceinline__ void run_task(Smem<B>& sm, const DevIndex& ix, const 
                     }
                 }
             }
-            const bool anyHub = hubPath && __syncthreads_or(isHub);
+            const bool anyHub = (hubPath || memoPath) && __syncthreads_or(isHub);
             sm.wBeg[tid] = myBeg;
             sm.wLen[tid] = myLen;
             if (tid == 0 && !leaf) S.count[k + 1] = 0;
@@ -456,7 +568,7 @@ __device__ __forceinline__ void run_task(Smem<B>& sm, const DevIndex& ix, const 
                 const int lane = tid & 31, warp = tid >> 5;
                 constexpr int kWarps = B / 32;
                 const int words = P.rowWords;
-                const bool perWarp = words <= 128;   // small domains: one warp per item
+                const bool perWarp = !leaf || words <= 128;   // memo items and small domains: one warp per item
                 const int nEx = lenK - kTupleHead;
                 const int exDir = 1 - stp.dir;
                 int ordinal = 0;
@@ -469,6 +581,12 @@ __device__ __forceinline__ void run_task(Smem<B>& sm, const DevIndex& ix, const 
                         const int mine = ordinal++;
                         if (perWarp && mine % kWarps != warp) continue;
                         const int* par = baseK + (w0 + item) * strideK;
+                        if (!leaf) {
+                            memo_item(P, ix, stp, P.steps[k + 1], par, lenK, -2 - sm.wBeg[item],
+                                      bm + (rowBase + par[0]) * (long long)words, words, S.exRank[warp], lane,
+                                      myNew, mt, shared);
+                            continue;
+                        }
                         // hO must differ from every bound value: their ranks in hO's domain
                         int* ex = S.exRank[warp];
                         if (lane < nEx) {
@@ -623,6 +741,39 @@ static void launch_b(const DevIndex& ix, const DevPlan* plans, const DevTask* ta
         engine_kernel<B, 1><<<grid, B, smem, stream>>>(ix, plans, tasks, nTasks, taskCounter, results, status, p);
     else
         engine_kernel<B, 0><<<grid, B, smem, stream>>>(ix, plans, tasks, nTasks, taskCounter, results, status, p);
+}
+
+// Suffix memos (see memo_item): one block per (hub row x, slot) job; warps
+// take the y in N1(x), lanes the h in N2(y).  The first witness of h sets
+// its S1 bit, any later one its S2 bit (atomicOr returns the old word).
+__global__ void memo_build_kernel(DevIndex ix, int p1, int d1, int p2, int d2, const int2* jobs, int nJobs,
+                                  uint32_t* bits, int words) {
+    if ((int)blockIdx.x >= nJobs) return;
+    const int2 job = jobs[blockIdx.x];
+    uint32_t* S1 = bits + (long long)job.y * 2 * words;
+    uint32_t* S2 = S1 + words;
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nWarps = blockDim.x >> 5;
+    const int b = ix.rowBeg[d1][job.x], e = ix.rowBeg[d1][job.x + 1];
+    Meter<false> mt;
+    for (int i = b + warp; i < e; i += nWarps) {
+        const int y = __ldg(ix.val[d1] + i);
+        const int2 r = row_lookup(ix, p2, d2, y, mt);
+        for (int j = r.x + lane; j < r.y; j += 32) {
+            if (__ldg(ix.val[d2] + j) == y) continue;
+            const int rank = __ldg(ix.valRank[d2] + j);
+            if (rank < 0 || rank >= (words << 5)) continue;
+            const uint32_t bit = 1u << (rank & 31);
+            const uint32_t old = atomicOr(S1 + (rank >> 5), bit);
+            if (old & bit) atomicOr(S2 + (rank >> 5), bit);
+        }
+    }
+}
+
+cudaError_t memo_build(const DevIndex& ix, int p1, int d1, int p2, int d2, const int2* jobs, int nJobs,
+                       uint32_t* bits, int words, cudaStream_t stream) {
+    if (nJobs <= 0) return cudaSuccess;
+    memo_build_kernel<<<nJobs, 256, 0, stream>>>(ix, p1, d1, p2, d2, jobs, nJobs, bits, words);
+    return cudaGetLastError();
 }
 
 // prof (optional): task times when prof->taskNs is set, also byte counts

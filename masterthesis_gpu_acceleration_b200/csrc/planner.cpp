@@ -348,6 +348,18 @@ RulePlan plan_rule(const Rule& rule, const HostIndex& ix, const Geom& geom) {
                     }
                 }
                 const bool local = finish_capacity(P, geom);
+                // suffix memo eligibility: the last two steps expand x -> y -> hO
+                // (y bound by the first, keying the second) with no test at
+                // either level but injectivity
+                if (pairs && P.m >= 2) {
+                    const int k = P.m - 2;
+                    const DevStep& a = P.steps[k];
+                    const DevStep& c = P.steps[k + 1];
+                    if (a.kind == kExpand && a.nNew == 1 && a.hoWhich == 0 && c.kind == kExpand && c.nNew == 1 &&
+                        c.hoWhich != 0 && c.keyRef == P.tupleLen[k] && P.chkN[k + 1] == 0 && P.usedN[k + 1] == 0 &&
+                        P.chkN[k + 2] == 0 && P.usedN[k + 2] == 0)
+                        P.memoLevel = k + 1;
+                }
                 B.how = kDevice;
                 B.rootBeg = ix.predRow[seedDir][seedPred];
                 B.rootEnd = ix.predRow[seedDir][seedPred + 1];

@@ -21,6 +21,8 @@ std::string signature(const PhasePlan& ph) {
     p.gRowBase = 0;
     p.gHeavy = nullptr;
     p.rowWords = 0;
+    p.memoTab = nullptr;
+    p.memoBits = nullptr;
     std::string s(reinterpret_cast<const char*>(&p), sizeof(p));
     s.append(reinterpret_cast<const char*>(&ph.rootBeg), sizeof(ph.rootBeg));
     s.append(reinterpret_cast<const char*>(&ph.rootEnd), sizeof(ph.rootEnd));
@@ -168,6 +170,13 @@ const std::vector<float>& TaskBuilder::walk(const PhasePlan& ph) {
     const bool chain = chain_shaped(P);
     const Hop2* h = chain ? &hop2(P.steps[0].pred, P.steps[0].dir, P.steps[1].pred, P.steps[1].dir) : nullptr;
     const int32_t* deg2 = (!chain && P.m >= 2 && P.steps[1].kind == kExpand) ? degrees(P.steps[1].pred, P.steps[1].dir) : nullptr;
+    // three-step plans whose last two steps are memoised: an item of level
+    // 1 costs the memo's price when its row has a memo, else its enumeration
+    const std::vector<uint8_t>* memo = nullptr;
+    double memoCost = 0.0;
+    const DevStep& s1 = P.steps[1];
+    if (chain && P.m == 3 && P.memoLevel == 2 && memoRows)
+        memo = memoRows(s1.pred, s1.dir, P.steps[2].pred, P.steps[2].dir, &memoCost);
     std::vector<float> w((size_t)(ph.rootEnd - ph.rootBeg));
     int32_t vals[2];
     for (int32_t r = ph.rootBeg; r < ph.rootEnd; ++r) {
@@ -175,7 +184,16 @@ const std::vector<float>& TaskBuilder::walk(const PhasePlan& ph) {
         auto seg = first_segment(P, r, vals);
         double acc = 1.0;
         if (P.m < 2) acc += seg.second - seg.first;
-        else if (chain) {
+        else if (chain && memo) {
+            acc += seg.second - seg.first;
+            const int d0 = P.steps[0].dir;
+            for (int32_t e = seg.first; e < seg.second; ++e) {
+                const auto rr = ix_.row_range(s1.pred, s1.dir, ix_.val[d0][e]);
+                if (rr.second <= rr.first) continue;
+                const int32_t row = ix_.srcRank[s1.dir][rr.first];   // row index within the predicate
+                acc += (*memo)[(size_t)row] ? memoCost : (double)(rr.second - rr.first) * tail;
+            }
+        } else if (chain) {
             acc += seg.second - seg.first;
             if (seg.second > seg.first) acc += h->perRow[ix_.srcRank[P.steps[0].dir][seg.first]] * tail;
         } else

@@ -1,6 +1,7 @@
 // tasks.hpp — splitting device phases into balanced tasks (the autotuner).
 #pragma once
 #include <cstdint>
+#include <functional>
 #include <string>
 #include <unordered_map>
 #include <utility>
@@ -68,6 +69,12 @@ public:
     // equal estimated work (per-root walk): slice k is [cut[k], cut[k+1]),
     // cut[0] = rootBeg, cut[n] = rootEnd.
     std::vector<int32_t> split_roots(const PhasePlan& ph, int n);
+
+    // Suffix memos known to the context: per-row flags of (p1, d1) for the
+    // memo of (p1, d1) -> (p2, d2) and its cost per item in work units, or
+    // null.  Walks of plans that end in such a suffix weigh memoised items
+    // by that cost instead of their enumeration.
+    std::function<const std::vector<uint8_t>*(int, int, int, int, double*)> memoRows;
 
     // Overrides: a fixed task work target (0 = automatic) and the hub-aware
     // estimate above which a phase is walked.

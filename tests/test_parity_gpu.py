@@ -178,11 +178,13 @@ def test_fuzz_forced_splitting(name, block, tmp_path):
         _check([lib.evaluate_rule(t) for t in fx["rules"][:60]], fx["expected"][:60], "per-rule split")
 
 
-@pytest.mark.parametrize("hub_min", ["1", "0"])
-def test_hub_rows_everywhere_or_nowhere(hub_min, tmp_path, monkeypatch):
-    """Body sizes through hub-row bitmaps (every row a hub) and without any,
-    on the fuzz graphs, the edge cases and c2s, against the reference."""
+@pytest.mark.parametrize("hub_min,memo_gain", [("1", "0"), ("1", "-1"), ("0", "8")])
+def test_hub_rows_everywhere_or_nowhere(hub_min, memo_gain, tmp_path, monkeypatch):
+    """Body sizes through hub-row bitmaps and two-step suffix memos (every row
+    a hub and every hub memoised; hubs without memos; neither), on the fuzz
+    graphs, the edge cases and c2s, against the reference."""
     monkeypatch.setenv("GPU_RULES_HUB_MIN_DEGREE", hub_min)
+    monkeypatch.setenv("GPU_RULES_MEMO_GAIN", memo_gain)
     for name in fuzz_names():
         fx = load_fixture(name)
         p = tmp_path / f"{name}.ttl"
