@@ -128,10 +128,14 @@ struct DevPlan {
     int64_t gRowBase;             // first root of the plan, for global bitmap rows
     uint32_t* gHeavy;             // global dedup rows of split heavy roots
     int32_t rowWords;             // words per heavy row (kPairs: ceil(wo / 32); kExist: 1)
-    int32_t memoLevel;            // kPairs ending in two expand steps: level + 1 whose items may
-                                  // use a suffix memo (0: none; see memo_item)
+    int32_t memoLevel;            // level + 1 whose items may use a suffix memo (0: none): kPairs
+                                  // plans ending in two expand steps x -> y -> hO (memo_item),
+                                  // kExist plans ending in x -> y and the check (h, y) (memo_exists)
+    int32_t memoP2, memoD2;       // the memo's second relation: y -> h through (memoP2, memoD2) rows
+    TermRef memoH;                // kExist: tuple ref (or constant) of h
+    int32_t memoWords;            // words per memo bitmap (the rows of (memoP2, 1 - memoD2))
     const int32_t* memoTab;       // per hub row: memo slot or -1 (null: no memo)
-    const uint32_t* memoBits;     // per slot: S1 then S2, rowWords words each
+    const uint32_t* memoBits;     // per slot: S1 then S2, memoWords words each
 };
 
 // A unit of device work: the roots [beg, end) of one plan.  A heavy root is

@@ -54,9 +54,8 @@ void Staged::stage(Context& c, std::vector<DevPlan>& plans, const std::vector<co
     // suffix memos first: the task builder weighs memoised roots by them
     for (int i = 0; i < nPlans; ++i)
         if (plans[i].memoLevel > 0) {
-            const DevStep& a = plans[i].steps[plans[i].m - 2];
-            const DevStep& b = plans[i].steps[plans[i].m - 1];
-            c.memo_for(a.pred, a.dir, b.pred, b.dir, s);
+            const DevStep& a = plans[i].steps[plans[i].memoLevel - 1];
+            c.memo_for(a.pred, a.dir, plans[i].memoP2, plans[i].memoD2, s);
         }
     std::vector<PhaseTasks> pts;
     c.tasks->build(phases, c.grid, true, pts, walkBudget, costAware);
@@ -74,12 +73,12 @@ void Staged::stage(Context& c, std::vector<DevPlan>& plans, const std::vector<co
         plans[i].memoTab = nullptr;
         plans[i].memoBits = nullptr;
         if (plans[i].memoLevel > 0) {
-            const DevStep& a = plans[i].steps[plans[i].m - 2];
-            const DevStep& b = plans[i].steps[plans[i].m - 1];
-            const SuffixMemo* m = c.memo_for(a.pred, a.dir, b.pred, b.dir, s);
-            if (m && m->words == plans[i].rowWords) {
+            const DevStep& a = plans[i].steps[plans[i].memoLevel - 1];
+            const SuffixMemo* m = c.memo_for(a.pred, a.dir, plans[i].memoP2, plans[i].memoD2, s);
+            if (m && (plans[i].mode != kPairs || m->words == plans[i].rowWords)) {
                 plans[i].memoTab = m->tab;
                 plans[i].memoBits = m->bits;
+                plans[i].memoWords = m->words;
             }
         }
         plans[i].resultSlot = i;

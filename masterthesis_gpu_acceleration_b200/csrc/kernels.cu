@@ -255,6 +255,69 @@ __device__ __noinline__ void memo_item(const DevPlan& P, const DevIndex& ix, con
     __syncwarp();
 }
 
+// kExist counterpart of memo_item: the item's last step expands a hub row x
+// with a memo and its only remaining test is the check (h, y) for a bound
+// variable h.  A valid y exists iff h has a witness y in N1(x) other than
+// the bound values: with no bound value among h's witnesses that is the S1
+// bit of h, with one the S2 bit; with more the item is left to enumeration.
+// Returns 1 (a grounding exists), 0 (none) or -1 (undecided).
+template <bool kC>
+__device__ __noinline__ int memo_exists(const DevPlan& P, const DevIndex& ix, const DevStep& stA, const int* it,
+                                        int lenK, int segBeg, int segLen, int slot, Meter<kC>& mt) {
+    const int h = it[P.memoH];
+    const int dDom = 1 - P.memoD2;
+    const int2 hr = row_lookup(ix, P.memoP2, dDom, h, mt);
+    if (hr.y <= hr.x) return 0;   // no y reaches h at all
+    const int rank = __ldg(ix.srcRank[dDom] + hr.x);
+    int nRem = 0;
+    for (int q = kTupleHead; q < lenK; ++q) {
+        const int u = it[q];
+        if (u == h || !seg_has(ix.val[stA.dir], segBeg, segLen, u, mt)) continue;
+        if (!has_edge(ix, P.memoP2, P.memoD2, u, h, mt)) continue;
+        if (++nRem >= 2) return -1;
+    }
+    const uint32_t* S = P.memoBits + ((long long)slot * 2 + nRem) * P.memoWords;
+    mt.add(4);
+    return (int)((__ldg(S + (rank >> 5)) >> (rank & 31)) & 1u);
+}
+
+// Items of a round that may skip enumeration, kept out of line so that the
+// main loop's registers stay free.  kind 1: a leaf item whose segment is a
+// whole hub row (returns the hub index); 2: an item at the memo level whose
+// segment is a memoised hub row with at most one bound value among its
+// neighbours (returns the memo slot); 3: a kExist leaf item decided by the
+// existence memo (returns -3, its found bit set).  -1: enumerate as usual.
+template <bool kC>
+__device__ __noinline__ int classify_item(const DevPlan& P, const DevIndex& ix, const DevStep& stp, const int* it,
+                                          int lenK, int kind, int segBeg, int segLen, uint32_t* fb, bool heavy,
+                                          unsigned long long* myNew, Meter<kC>* mt) {
+    const int row = __ldg(ix.predRow[stp.dir] + stp.pred) + __ldg(ix.srcRank[stp.dir] + segBeg);
+    const int h = __ldg(ix.hubOf[stp.dir] + row);
+    mt->add(12);
+    if (h < 0 || __ldg(ix.rowBeg[stp.dir] + row) != segBeg || __ldg(ix.rowBeg[stp.dir] + row + 1) - segBeg != segLen)
+        return -1;
+    if (kind == 1) return h;
+    const int slot = __ldg(P.memoTab + h);
+    if (slot < 0) return -1;
+    if (kind == 2) {
+        // bound values that are also first-step neighbours are witnesses the
+        // memo must not count; one is corrected exactly, more enumerate
+        int nR = 0;
+        for (int q = kTupleHead; q < lenK && nR < 2; ++q)
+            nR += seg_has(ix.val[stp.dir], segBeg, segLen, it[q], *mt) ? 1 : 0;
+        return nR <= 1 ? slot : -1;
+    }
+    const int res = memo_exists(P, ix, stp, it, lenK, segBeg, segLen, slot, *mt);
+    if (res < 0) return -1;
+    if (res == 1) {
+        const int root = it[0];
+        const uint32_t mask = 1u << (root & 31);
+        const uint32_t old = atomicOr(&fb[root >> 5], mask);
+        if (heavy) { mt->add(8); *myNew += (old & mask) ? 0ull : 1ull; }
+    }
+    return -3;
+}
+
 template <int B, bool kC>
 __device__ __forceinline__ void run_task(Smem<B>& sm, const DevIndex& ix, const DevTask& task,
                                          unsigned long long* results, int* status, Meter<kC>& mt) {
@@ -385,6 +448,8 @@ __device__ __forceinline__ void run_task(Smem<B>& sm, const DevIndex& ix, const 
             // is a hub row with a suffix memo is counted from the memo's
             // "one witness y" / "two witnesses y" bitmaps (see below).
             const bool memoPath = !leaf && pairs && P.memoTab != nullptr && k + 1 == P.memoLevel;
+            const bool existMemo = leaf && !pairs && P.memoTab != nullptr && k + 1 == P.memoLevel &&
+                                   !(heavy && k == 0);
             bool isHub = false;   // item marked for the hub or memo pass
 
             // window: the stored neighbour segment of each item
@@ -404,35 +469,16 @@ __device__ __forceinline__ void run_task(Smem<B>& sm, const DevIndex& ix, const 
                 if (!pruned) {
                     myBeg = it[lenK];
                     myLen = it[lenK + 1];
-                    if (hubPath && myLen > 0 && !(tid == 0 && S.curOff[k] != 0)) {
-                        const int row = __ldg(ix.predRow[stp.dir] + stp.pred) + __ldg(ix.srcRank[stp.dir] + myBeg);
-                        const int h = __ldg(ix.hubOf[stp.dir] + row);
-                        mt.add(12);
-                        if (h >= 0 && __ldg(ix.rowBeg[stp.dir] + row) == myBeg &&
-                            __ldg(ix.rowBeg[stp.dir] + row + 1) - myBeg == myLen) {
+                    const int pathKind = hubPath ? 1 : (memoPath ? 2 : (existMemo ? 3 : 0));
+                    if (pathKind && myLen > 0 && !(tid == 0 && S.curOff[k] != 0)) {
+                        const int code = classify_item(P, ix, stp, it, lenK, pathKind, myBeg, (int)myLen, fb, heavy,
+                                                       &myNew, &mt);
+                        if (code >= 0) {
                             isHub = true;
-                            myBeg = -2 - h;   // marks the item for the hub pass; no candidates
+                            myBeg = -2 - code;   // marks the item for the hub or memo pass; no candidates
                             myLen = 0;
-                        }
-                    }
-                    if (memoPath && myLen > 0 && !(tid == 0 && S.curOff[k] != 0)) {
-                        const int row = __ldg(ix.predRow[stp.dir] + stp.pred) + __ldg(ix.srcRank[stp.dir] + myBeg);
-                        const int h = __ldg(ix.hubOf[stp.dir] + row);
-                        const int slot = h >= 0 ? __ldg(P.memoTab + h) : -1;
-                        mt.add(12);
-                        if (slot >= 0 && __ldg(ix.rowBeg[stp.dir] + row) == myBeg &&
-                            __ldg(ix.rowBeg[stp.dir] + row + 1) - myBeg == myLen) {
-                            // bound values that are also first-step neighbours are
-                            // witnesses the memo must not count; one is corrected
-                            // exactly, more fall back to enumeration
-                            int nR = 0;
-                            for (int q = kTupleHead; q < lenK && nR < 2; ++q)
-                                nR += seg_has(ix.val[stp.dir], myBeg, (int)myLen, it[q], mt) ? 1 : 0;
-                            if (nR <= 1) {
-                                isHub = true;
-                                myBeg = -2 - slot;
-                                myLen = 0;
-                            }
+                        } else if (code == -3) {
+                            myLen = 0;           // decided by the existence memo
                         }
                     }
                     if (tid == 0 && !isHub) {

@@ -194,6 +194,31 @@ bool build_steps(Builder& b, const std::vector<Atom>& body, const Atom* head, in
 // rows up to half the pool (ceil(wo / 32) words per root), or none when one
 // row does not fit next to a minimal frontier (the plan then deduplicates in
 // a global bitmap).  Returns false in that last case.
+// kExist plans whose last step expands x -> y (y new) and whose only test
+// after it is one membership check between y and a bound value or
+// constant h: whether some valid y exists is one bit of the suffix memo of
+// (last step) -> (the check seen from y), see memo_exists in kernels.cu.
+void exist_memo_eligibility(DevPlan& P) {
+    if (P.mode != kExist || P.m < 1) return;
+    const int k = P.m - 1;
+    const DevStep& a = P.steps[k];
+    if (a.kind != kExpand || a.nNew != 1 || P.usedN[k + 1] != 0 || P.chkN[k + 1] != 1) return;
+    const DevCheck& c = P.checks[P.chkBeg[k + 1]];
+    const TermRef y = (TermRef)P.tupleLen[k];
+    TermRef hRef;
+    int d2;
+    if (c.s == y && c.o != y) { hRef = c.o; d2 = 0; }        // (y p h): h among y's objects
+    else if (c.o == y && c.s != y) { hRef = c.s; d2 = 1; }   // (h p y): h among y's subjects
+    else return;
+    // h must be a variable: the memo never lets y equal h, which injectivity
+    // forbids only between variables
+    if (hRef < kTupleHead || hRef >= y) return;
+    P.memoLevel = k + 1;
+    P.memoP2 = c.pred;
+    P.memoD2 = d2;
+    P.memoH = hRef;
+}
+
 bool finish_capacity(DevPlan& P, const Geom& geom) {
     int sum = 0;
     if (P.m == 0) sum = P.tupleLen[0];
@@ -301,6 +326,7 @@ RulePlan plan_rule(const Rule& rule, const HostIndex& ix, const Geom& geom) {
             }
             if (build_steps(b, rule.body, &h, -1, false) && b.ok) {
                 finish_capacity(P, geom);
+                exist_memo_eligibility(P);
                 S.how = kDevice;
                 S.rootBeg = range.first;
                 S.rootEnd = range.second;
@@ -357,8 +383,11 @@ RulePlan plan_rule(const Rule& rule, const HostIndex& ix, const Geom& geom) {
                     const DevStep& c = P.steps[k + 1];
                     if (a.kind == kExpand && a.nNew == 1 && a.hoWhich == 0 && c.kind == kExpand && c.nNew == 1 &&
                         c.hoWhich != 0 && c.keyRef == P.tupleLen[k] && P.chkN[k + 1] == 0 && P.usedN[k + 1] == 0 &&
-                        P.chkN[k + 2] == 0 && P.usedN[k + 2] == 0)
+                        P.chkN[k + 2] == 0 && P.usedN[k + 2] == 0) {
                         P.memoLevel = k + 1;
+                        P.memoP2 = c.pred;
+                        P.memoD2 = c.dir;
+                    }
                 }
                 B.how = kDevice;
                 B.rootBeg = ix.predRow[seedDir][seedPred];

@@ -175,7 +175,7 @@ const std::vector<float>& TaskBuilder::walk(const PhasePlan& ph) {
     const std::vector<uint8_t>* memo = nullptr;
     double memoCost = 0.0;
     const DevStep& s1 = P.steps[1];
-    if (chain && P.m == 3 && P.memoLevel == 2 && memoRows)
+    if (chain && P.mode == kPairs && P.m == 3 && P.memoLevel == 2 && memoRows)
         memo = memoRows(s1.pred, s1.dir, P.steps[2].pred, P.steps[2].dir, &memoCost);
     std::vector<float> w((size_t)(ph.rootEnd - ph.rootBeg));
     int32_t vals[2];
