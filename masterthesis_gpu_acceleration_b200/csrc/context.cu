@@ -317,6 +317,8 @@ void prepare(Batch& b, Context& c, const char* const* rules, int n, int isJson) 
     b.c = &c;
     b.n = n;
     b.owner.clear();
+    b.shared.clear();
+    std::unordered_map<std::string, int> seen;
     if (b.exec) { cudaGraphExecDestroy(b.exec); b.exec = nullptr; }
     if (b.graph) { cudaGraphDestroy(b.graph); b.graph = nullptr; }
     b.rps.assign(n, RulePlan{});
@@ -335,8 +337,20 @@ void prepare(Batch& b, Context& c, const char* const* rules, int n, int isJson) 
         }
         RulePlan& rp = b.rps[i];
         if (rp.status != kRuleOk) continue;
-        if (rp.support.how == kDevice) { plans.push_back(rp.support.plan); phases.push_back(&rp.support); b.owner.push_back(2 * i); }
-        if (rp.body.how == kDevice) { plans.push_back(rp.body.plan); phases.push_back(&rp.body); b.owner.push_back(2 * i + 1); }
+        for (int k = 0; k < 2; ++k) {
+            const PhasePlan& ph = k == 0 ? rp.support : rp.body;
+            if (ph.how != kDevice) continue;
+            // identical computations (same plan and roots, e.g. one body under
+            // several heads) run once; the others share the count
+            auto ins = seen.emplace(phase_signature(ph), (int)plans.size());
+            if (!ins.second) {
+                b.shared.emplace_back(2 * i + k, ins.first->second);
+                continue;
+            }
+            plans.push_back(ph.plan);
+            phases.push_back(&ph);
+            b.owner.push_back(2 * i + k);
+        }
     }
     if (!b.stream) ck(cudaStreamCreateWithFlags(&b.stream, cudaStreamNonBlocking), "cudaStreamCreate");
     if (!b.ev0) ck(cudaEventCreate(&b.ev0), "cudaEventCreate");
@@ -354,6 +368,11 @@ void collect(const Batch& b, GpuRuleResult* out, int* status) {
         int i = b.owner[k] / 2;
         if (b.owner[k] % 2 == 0) sup[i] = (int64_t)cnt[k];
         else body[i] = (int64_t)cnt[k];
+    }
+    for (const auto& sh : b.shared) {
+        int i = sh.first / 2;
+        if (sh.first % 2 == 0) sup[i] = (int64_t)cnt[sh.second];
+        else body[i] = (int64_t)cnt[sh.second];
     }
     for (int i = 0; i < b.n; ++i) {
         if (status) status[i] = b.parseStatus[i];
@@ -566,6 +585,11 @@ int gpu_batch_counts(void* batch, long long* counts, int* status) {
         int i = b.owner[k] / 2;
         if (b.owner[k] % 2 == 0) sup[i] = (int64_t)cnt[k];
         else body[i] = (int64_t)cnt[k];
+    }
+    for (const auto& sh : b.shared) {
+        int i = sh.first / 2;
+        if (sh.first % 2 == 0) sup[i] = (int64_t)cnt[sh.second];
+        else body[i] = (int64_t)cnt[sh.second];
     }
     for (int i = 0; i < b.n; ++i) {
         const RulePlan& rp = b.rps[i];

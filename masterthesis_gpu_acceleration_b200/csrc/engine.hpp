@@ -297,6 +297,9 @@ struct Batch {
     std::vector<RulePlan> rps;
     std::vector<int> parseStatus;
     std::vector<int> owner;  // plan -> rule * 2 + phase
+    // phases identical to an earlier one of the batch (same plan and roots):
+    // (rule * 2 + phase, plan whose count they share); computed once per run
+    std::vector<std::pair<int, int>> shared;
     std::vector<DevPlan> plans0;
     std::vector<const PhasePlan*> phases;
     Staged st;

@@ -14,7 +14,12 @@ constexpr size_t kCacheLimit = size_t(2) << 30;
 
 int64_t pd_key(int32_t pred, int dir) { return (int64_t)pred * 2 + dir; }
 
-std::string signature(const PhasePlan& ph) {
+
+std::string signature(const PhasePlan& ph) { return phase_signature(ph); }
+
+}  // namespace
+
+std::string phase_signature(const PhasePlan& ph) {
     DevPlan p = ph.plan;
     p.resultSlot = 0;
     p.gBitmap = nullptr;
@@ -28,8 +33,6 @@ std::string signature(const PhasePlan& ph) {
     s.append(reinterpret_cast<const char*>(&ph.rootEnd), sizeof(ph.rootEnd));
     return s;
 }
-
-}  // namespace
 
 const int32_t* TaskBuilder::degrees(int32_t pred, int dir) {
     auto it = deg_.find(pd_key(pred, dir));

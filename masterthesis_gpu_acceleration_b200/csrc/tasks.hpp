@@ -34,6 +34,11 @@ struct PhaseTasks {
 // Host time of one step of a per-root walk (ns), for the cost-aware mode.
 constexpr double kWalkNsPerEdge = 8.0;
 
+// Identity of a phase's device computation: the plan without its
+// per-launch fields, and its root range.  Phases with equal signatures
+// produce equal counts.
+std::string phase_signature(const PhasePlan& ph);
+
 class TaskBuilder {
 public:
     explicit TaskBuilder(const HostIndex& ix) : ix_(ix) {}
