@@ -24,7 +24,8 @@ NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 
 ENGINE_SOURCES = ["turtle.cpp", "rules.cpp", "index.cpp", "planner.cpp", "tasks.cpp", "kernels.cu", "context.cu", "serve.cu"]
-HEADERS = ["common.hpp", "turtle.hpp", "rules.hpp", "index.hpp", "planner.hpp", "tasks.hpp", "engine.hpp"]
+HEADERS = ["common.hpp", "turtle.hpp", "rules.hpp", "index.hpp", "planner.hpp", "tasks.hpp", "engine.hpp",
+           "parallel.hpp"]
 
 
 def _newer(target: Path, deps) -> bool:

@@ -23,6 +23,7 @@
 #include <vector>
 
 #include "engine.hpp"
+#include "parallel.hpp"
 
 namespace gr {
 
@@ -318,7 +319,7 @@ void prepare(Batch& b, Context& c, const char* const* rules, int n, int isJson) 
     b.n = n;
     b.owner.clear();
     b.shared.clear();
-    std::unordered_map<std::string, int> seen;
+    std::unordered_multimap<uint64_t, int> seen;
     if (b.exec) { cudaGraphExecDestroy(b.exec); b.exec = nullptr; }
     if (b.graph) { cudaGraphDestroy(b.graph); b.graph = nullptr; }
     b.rps.assign(n, RulePlan{});
@@ -326,15 +327,18 @@ void prepare(Batch& b, Context& c, const char* const* rules, int n, int isJson) 
     std::vector<DevPlan> plans;
     std::vector<const PhasePlan*> phases;
     plans.reserve(2 * (size_t)n);
-    for (int i = 0; i < n; ++i) {
-        if (!rules[i]) { b.parseStatus[i] = -1; continue; }
+    // parsing and planning only read the graph and the dictionaries: in parallel
+    parallel_for((size_t)n, [&](size_t i) {
+        if (!rules[i]) { b.parseStatus[i] = -1; return; }
         try {
             Rule r = isJson ? c.parser->parse_json(rules[i]) : c.parser->parse_text(rules[i]);
             b.rps[i] = plan_rule(r, c.hix, c.geom);
         } catch (const RuleError&) {
             b.parseStatus[i] = -1;
-            continue;
         }
+    }, 128);
+    for (int i = 0; i < n; ++i) {
+        if (b.parseStatus[i] != 0) continue;
         RulePlan& rp = b.rps[i];
         if (rp.status != kRuleOk) continue;
         for (int k = 0; k < 2; ++k) {
@@ -342,11 +346,17 @@ void prepare(Batch& b, Context& c, const char* const* rules, int n, int isJson) 
             if (ph.how != kDevice) continue;
             // identical computations (same plan and roots, e.g. one body under
             // several heads) run once; the others share the count
-            auto ins = seen.emplace(phase_signature(ph), (int)plans.size());
-            if (!ins.second) {
-                b.shared.emplace_back(2 * i + k, ins.first->second);
+            // keyed by hash, confirmed by the full signature (plans are
+            // zero-initialised, so equal signatures mean equal computations)
+            auto range = seen.equal_range(phase_hash(ph));
+            int same = -1;
+            for (auto it = range.first; it != range.second && same < 0; ++it)
+                if (phase_signature(*phases[it->second]) == phase_signature(ph)) same = it->second;
+            if (same >= 0) {
+                b.shared.emplace_back(2 * i + k, same);
                 continue;
             }
+            seen.emplace(phase_hash(ph), (int)plans.size());
             plans.push_back(ph.plan);
             phases.push_back(&ph);
             b.owner.push_back(2 * i + k);

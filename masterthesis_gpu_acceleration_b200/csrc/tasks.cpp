@@ -1,5 +1,6 @@
 // tasks.cpp — balanced task construction (see tasks.hpp).
 #include "tasks.hpp"
+#include "parallel.hpp"
 
 #include <algorithm>
 #include <cmath>
@@ -15,11 +16,13 @@ constexpr size_t kCacheLimit = size_t(2) << 30;
 int64_t pd_key(int32_t pred, int dir) { return (int64_t)pred * 2 + dir; }
 
 
-std::string signature(const PhasePlan& ph) { return phase_signature(ph); }
+uint64_t signature(const PhasePlan& ph) { return phase_hash(ph); }
 
 }  // namespace
 
-std::string phase_signature(const PhasePlan& ph) {
+namespace {
+// The plan without its per-launch fields.
+DevPlan plan_identity(const PhasePlan& ph) {
     DevPlan p = ph.plan;
     p.resultSlot = 0;
     p.gBitmap = nullptr;
@@ -28,10 +31,33 @@ std::string phase_signature(const PhasePlan& ph) {
     p.rowWords = 0;
     p.memoTab = nullptr;
     p.memoBits = nullptr;
+    p.memoWords = 0;
+    return p;
+}
+}  // namespace
+
+std::string phase_signature(const PhasePlan& ph) {
+    const DevPlan p = plan_identity(ph);
     std::string s(reinterpret_cast<const char*>(&p), sizeof(p));
     s.append(reinterpret_cast<const char*>(&ph.rootBeg), sizeof(ph.rootBeg));
     s.append(reinterpret_cast<const char*>(&ph.rootEnd), sizeof(ph.rootEnd));
     return s;
+}
+
+uint64_t phase_hash(const PhasePlan& ph) {
+    static_assert(sizeof(DevPlan) % 8 == 0, "plan hashed in 8-byte words");
+    const DevPlan p = plan_identity(ph);
+    const unsigned char* b = reinterpret_cast<const unsigned char*>(&p);
+    uint64_t h = 0x243F6A8885A308D3ull ^ ((uint64_t)(uint32_t)ph.rootBeg << 32 | (uint32_t)ph.rootEnd);
+    for (size_t i = 0; i < sizeof(DevPlan); i += 8) {
+        uint64_t w;
+        std::memcpy(&w, b + i, 8);
+        h = (h ^ w) * 0x9E3779B97F4A7C15ull;
+        h ^= h >> 29;
+    }
+    h ^= h >> 32;
+    h *= 0xD6E8FEB86659FD93ull;
+    return h ^ (h >> 32);
 }
 
 const int32_t* TaskBuilder::degrees(int32_t pred, int dir) {
@@ -164,7 +190,7 @@ double TaskBuilder::child_work(const DevPlan& P, const int32_t* vals, int32_t e,
 }
 
 const std::vector<float>& TaskBuilder::walk(const PhasePlan& ph) {
-    std::string sig = signature(ph);
+    const uint64_t sig = signature(ph);
     auto it = walks_.find(sig);
     if (it != walks_.end()) return it->second;
     const DevPlan& P = ph.plan;
@@ -203,7 +229,7 @@ const std::vector<float>& TaskBuilder::walk(const PhasePlan& ph) {
             for (int32_t e = seg.first; e < seg.second; ++e) acc += child_work(P, vals, e, deg2, tail);
         w[r - ph.rootBeg] = (float)acc;
     }
-    cacheBytes_ += w.size() * sizeof(float) + sig.size();
+    cacheBytes_ += w.size() * sizeof(float) + sizeof(sig);
     return walks_.emplace(std::move(sig), std::move(w)).first->second;
 }
 
@@ -225,7 +251,7 @@ void TaskBuilder::build(const std::vector<const PhasePlan*>& phases, int blocks,
         estHub[i] = split ? estimate(*phases[i], true) : estAvg[i];
         out[i].work = estAvg[i];
         if (!calib_.empty() || !mustWalk_.empty()) {
-            std::string sig = signature(*phases[i]);
+            const uint64_t sig = signature(*phases[i]);
             auto c = calib_.find(sig);
             if (c != calib_.end()) scale[i] = c->second;
             forced[i] = mustWalk_.count(sig) ? 1 : 0;
@@ -267,7 +293,13 @@ void TaskBuilder::build(const std::vector<const PhasePlan*>& phases, int blocks,
     const double target = forceTarget > 0 ? forceTarget
                                           : std::max(kMinTarget * defaultCalib_, total / (std::max(blocks, 1) * 8.0));
 
+    // task lists per phase: independent once the degree arrays that heavy
+    // roots split by exist, so built in parallel
     for (size_t i = 0; i < n; ++i) {
+        const DevPlan& P = phases[i]->plan;
+        if (walked[i] && P.m >= 2 && P.steps[1].kind == kExpand) degrees(P.steps[1].pred, P.steps[1].dir);
+    }
+    parallel_for(n, [&](size_t i) {
         const PhasePlan& ph = *phases[i];
         const DevPlan& P = ph.plan;
         PhaseTasks& pt = out[i];
@@ -288,7 +320,7 @@ void TaskBuilder::build(const std::vector<const PhasePlan*>& phases, int blocks,
                 pt.tasks.push_back(DevTask{(int32_t)i, b, e, 0, 0, -1});
                 pt.cost.push_back(uniform * (e - b));
             }
-            continue;
+            return;
         }
         int32_t gb = ph.rootBeg;
         double acc = 0, accUnits = 0;
@@ -343,7 +375,7 @@ void TaskBuilder::build(const std::vector<const PhasePlan*>& phases, int blocks,
             accUnits += wu;
         }
         flush(ph.rootEnd);
-    }
+    });
 }
 
 std::vector<int32_t> TaskBuilder::split_roots(const PhasePlan& ph, int n) {
@@ -396,7 +428,7 @@ void TaskBuilder::learn(const std::vector<const PhasePlan*>& phases, const std::
     const double limit = std::max(minWorstNs, totNs / (std::max(blocks, 1) * 8.0));
     for (size_t p = 0; p < n; ++p) {
         if (units[p] <= 0) continue;
-        std::string sig = signature(*phases[p]);
+        const uint64_t sig = signature(*phases[p]);
         auto it = calib_.find(sig);
         const double now = ns[p] / units[p];
         calib_[sig] = it == calib_.end() ? now : blend(it->second, now);

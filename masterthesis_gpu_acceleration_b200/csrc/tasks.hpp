@@ -38,6 +38,8 @@ constexpr double kWalkNsPerEdge = 8.0;
 // per-launch fields, and its root range.  Phases with equal signatures
 // produce equal counts.
 std::string phase_signature(const PhasePlan& ph);
+// 64-bit hash of phase_signature (keys of the task builder's caches).
+uint64_t phase_hash(const PhasePlan& ph);
 
 class TaskBuilder {
 public:
@@ -90,14 +92,14 @@ private:
     const HostIndex& ix_;
     std::unordered_map<int64_t, std::vector<int32_t>> deg_;      // (pred, dir) -> degree by entity
     std::unordered_map<int64_t, double> sbFan_;                  // (pred, dir) -> size-biased fan-out
-    std::unordered_map<std::string, std::vector<float>> walks_;  // plan signature -> per-root work
+    std::unordered_map<uint64_t, std::vector<float>> walks_;     // phase hash -> per-root work
     struct Hop2 {
         std::vector<float> perRow;   // per row of (p0, d0): sum over its edges of the next degree
         double total = 0.0;
     };
     std::unordered_map<uint64_t, Hop2> hop2_;                    // (p0, d0, p1, d1) -> two-hop sums
-    std::unordered_map<std::string, double> calib_;             // plan signature -> ns per work unit
-    std::unordered_map<std::string, bool> mustWalk_;            // plan signature -> walk next time
+    std::unordered_map<uint64_t, double> calib_;                // phase hash -> ns per work unit
+    std::unordered_map<uint64_t, bool> mustWalk_;               // phase hash -> walk next time
     double defaultCalib_ = 1.0;
     size_t cacheBytes_ = 0;
 
