@@ -97,6 +97,8 @@ enum PlanMode : int32_t { kExist = 0, kPairs = 1 };
 enum RootKind : int32_t { kRootEdges = 0, kRootRows = 1 };
 
 // One phase (support or body size) of one rule.
+// Every byte of a plan belongs to a field (explicit pads, no implicit
+// padding), so that equal plans compare and hash equal after any copy.
 struct DevPlan {
     int32_t mode;            // kExist: count roots with a grounding; kPairs: count distinct (root, hO)
     int32_t m;               // binding steps
@@ -124,6 +126,7 @@ struct DevPlan {
     DevStep steps[kMaxBody];
     DevCheck checks[kMaxChecks];
     DevUsed used[kMaxUsed];
+    int32_t pad1;                 // explicit: plans are compared and hashed byte by byte
     uint32_t* gBitmap;            // kPairs with a global bitmap (null: shared memory)
     int64_t gRowBase;             // first root of the plan, for global bitmap rows
     uint32_t* gHeavy;             // global dedup rows of split heavy roots
@@ -132,7 +135,8 @@ struct DevPlan {
                                   // plans ending in two expand steps x -> y -> hO (memo_item),
                                   // kExist plans ending in x -> y and the check (h, y) (memo_exists)
     int32_t memoP2, memoD2;       // the memo's second relation: y -> h through (memoP2, memoD2) rows
-    TermRef memoH;                // kExist: tuple ref (or constant) of h
+    TermRef memoH;                // kExist: tuple ref of h
+    int16_t pad2;
     int32_t memoWords;            // words per memo bitmap (the rows of (memoP2, 1 - memoD2))
     const int32_t* memoTab;       // per hub row: memo slot or -1 (null: no memo)
     const uint32_t* memoBits;     // per slot: S1 then S2, memoWords words each

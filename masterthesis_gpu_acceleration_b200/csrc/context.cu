@@ -522,7 +522,8 @@ int gpu_evaluate_rules_batch(void* ctx, const char* const* rules, int n, int isJ
         cudaSetDevice(c.device);
         // Pipelined: chunk k+1 is parsed, planned and staged on the host
         // while chunk k runs on the device (each chunk on its own stream).
-        const int K = std::max(1, std::min(4, (n + 2499) / 2500));
+        const int K = c.batchChunks > 0 ? std::max(1, std::min(c.batchChunks, std::max(n, 1)))
+                                        : std::max(1, std::min(4, (n + 2499) / 2500));
         while ((int)c.pipe.size() < K) c.pipe.push_back(new Batch());
         for (int k = 0; k < K; ++k) {
             const int lo = (int)((long long)n * k / K), hi = (int)((long long)n * (k + 1) / K);
@@ -705,6 +706,7 @@ int gpu_set_option(void* ctx, const char* name, long long value) {
     if (n == "walk_threshold" && value >= 0) { c.tasks->walkThreshold = (double)value; return 0; }
     if (n == "serve_lanes" && (value == 0 || value == 1)) { c.serveLanes = (int)value; return 0; }
     if (n == "rule_walk_budget" && value >= 0) { c.ruleWalkBudget = (double)value; return 0; }
+    if (n == "batch_chunks" && value >= 0 && value <= 16) { c.batchChunks = (int)value; return 0; }
     if (n == "serve_heavy_share" && value >= 1 && value <= 16) { c.serveHeavyShare = (int)value; return 0; }
     if (n == "serve_heavy_us" && value >= 0) { c.serveHeavyNs = 1e3 * (double)value; return 0; }
     return -1;

@@ -188,6 +188,7 @@ struct Context {
     std::unique_ptr<TaskBuilder> tasks;
     Geom geom;
     double ruleWalkBudget = 4.0e6;   // per-root measurement allowed per plain per-rule launch
+    int batchChunks = 0;             // pipelined chunks of one-shot batches (0: automatic)
     // suffix memos: a hub row gets one when its suffix candidates are at
     // least memoGain x the memo's words (negative: no memos)
     double memoGain = 0.25;

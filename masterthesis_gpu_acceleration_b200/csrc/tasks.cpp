@@ -32,6 +32,9 @@ DevPlan plan_identity(const PhasePlan& ph) {
     p.memoTab = nullptr;
     p.memoBits = nullptr;
     p.memoWords = 0;
+    p.pad0 = 0;
+    p.pad1 = 0;
+    p.pad2 = 0;
     return p;
 }
 }  // namespace
@@ -189,8 +192,7 @@ double TaskBuilder::child_work(const DevPlan& P, const int32_t* vals, int32_t e,
     return 1.0 + d2 * tail;
 }
 
-const std::vector<float>& TaskBuilder::walk(const PhasePlan& ph) {
-    const uint64_t sig = signature(ph);
+const TaskBuilder::Walk& TaskBuilder::walk(const PhasePlan& ph, uint64_t sig) {
     auto it = walks_.find(sig);
     if (it != walks_.end()) return it->second;
     const DevPlan& P = ph.plan;
@@ -229,8 +231,11 @@ const std::vector<float>& TaskBuilder::walk(const PhasePlan& ph) {
             for (int32_t e = seg.first; e < seg.second; ++e) acc += child_work(P, vals, e, deg2, tail);
         w[r - ph.rootBeg] = (float)acc;
     }
-    cacheBytes_ += w.size() * sizeof(float) + sizeof(sig);
-    return walks_.emplace(std::move(sig), std::move(w)).first->second;
+    cacheBytes_ += w.size() * sizeof(float) + sizeof(Walk);
+    Walk entry;
+    for (float x : w) entry.sum += x;
+    entry.w = std::move(w);
+    return walks_.emplace(sig, std::move(entry)).first->second;
 }
 
 void TaskBuilder::build(const std::vector<const PhasePlan*>& phases, int blocks, bool split,
@@ -275,16 +280,16 @@ void TaskBuilder::build(const std::vector<const PhasePlan*>& phases, int blocks,
             double edges = chain_shaped(ph.plan) ? (double)(ph.rootEnd - ph.rootBeg)
                          : (double)(ph.rootEnd - ph.rootBeg) *
                            (s0.kind == kExpand ? std::max(1.0, ix_.avg_degree(s0.pred, s0.dir)) : (double)ix_.pred_size(s0.pred));
-            const bool cached = walks_.count(signature(ph)) != 0;
+            const uint64_t sig = signature(ph);
+            const bool cached = walks_.count(sig) != 0;
             if (!forced[i] && !cached && used + edges > walkBudget) continue;
             // a walk whose own cost exceeds the phase's expected device time
             // cannot pay for itself (a single rule on the whole GPU)
             if (costAware && !cached && estAvg[i] * scale[i] < kWalkNsPerEdge * edges) continue;
             if (!cached) used += edges;   // cached walks cost nothing
-            walked[i] = &walk(ph);
-            double s = 0;
-            for (float x : *walked[i]) s += x;
-            out[i].work = s;
+            const Walk& wk = walk(ph, sig);
+            walked[i] = &wk.w;
+            out[i].work = wk.sum;
         }
     }
     // work in device-time units (learned ns per unit, where known)
@@ -384,7 +389,7 @@ std::vector<int32_t> TaskBuilder::split_roots(const PhasePlan& ph, int n) {
     cut[0] = ph.rootBeg;
     const int32_t R = ph.rootEnd - ph.rootBeg;
     if (R <= 0) return cut;
-    const std::vector<float>& w = walk(ph);
+    const std::vector<float>& w = walk(ph).w;
     double total = 0;
     for (float x : w) total += x;
     double acc = 0;

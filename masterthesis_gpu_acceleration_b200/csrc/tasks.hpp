@@ -92,7 +92,11 @@ private:
     const HostIndex& ix_;
     std::unordered_map<int64_t, std::vector<int32_t>> deg_;      // (pred, dir) -> degree by entity
     std::unordered_map<int64_t, double> sbFan_;                  // (pred, dir) -> size-biased fan-out
-    std::unordered_map<uint64_t, std::vector<float>> walks_;     // phase hash -> per-root work
+    struct Walk {
+        std::vector<float> w;   // per-root work
+        double sum = 0.0;
+    };
+    std::unordered_map<uint64_t, Walk> walks_;                   // phase hash -> per-root work
     struct Hop2 {
         std::vector<float> perRow;   // per row of (p0, d0): sum over its edges of the next degree
         double total = 0.0;
@@ -116,7 +120,8 @@ private:
     // chain-shaped plans whose roots are the first step's rows; otherwise
     // the average-fan-out estimate.
     double estimate2(const PhasePlan& ph);
-    const std::vector<float>& walk(const PhasePlan& ph);
+    const Walk& walk(const PhasePlan& ph, uint64_t sig);
+    const Walk& walk(const PhasePlan& ph) { return walk(ph, phase_hash(ph)); }
     double child_work(const DevPlan& P, const int32_t* rootVals, int32_t e, const int32_t* deg2, double tail) const;
     int root_vals(const DevPlan& P, int32_t r, int32_t* vals) const;
     std::pair<int32_t, int32_t> first_segment(const DevPlan& P, int32_t r, const int32_t* vals) const;
