@@ -167,6 +167,13 @@ struct Geom {
 // Profiling outputs of the instrumented kernel variant (null members are
 // skipped): requested global-memory bytes, and per task its start and end
 // time (globaltimer ns).
+// One suffix-memo bitmap pair to build: hub row `row` of (p1, d1) through
+// (p2, d2), `words` words per bitmap at `bits` (S1, then S2).
+struct MemoJob {
+    int32_t p1, d1, p2, d2, row, words;
+    uint32_t* bits;
+};
+
 struct EngineProfile {
     unsigned long long* bytes = nullptr;
     unsigned long long* taskNs = nullptr;

@@ -53,11 +53,13 @@ void Staged::stage(Context& c, std::vector<DevPlan>& plans, const std::vector<co
     cudaStream_t as = streamOrdered ? s : nullptr;
     if (bitmapWords) dBitmap.ensure(bitmapWords * 4, as);
     // suffix memos first: the task builder weighs memoised roots by them
+    std::vector<std::array<int, 4>> memoKeys;
     for (int i = 0; i < nPlans; ++i)
         if (plans[i].memoLevel > 0) {
             const DevStep& a = plans[i].steps[plans[i].memoLevel - 1];
-            c.memo_for(a.pred, a.dir, plans[i].memoP2, plans[i].memoD2, s);
+            memoKeys.push_back({a.pred, a.dir, plans[i].memoP2, plans[i].memoD2});
         }
+    if (!memoKeys.empty()) c.ensure_memos(memoKeys, s);
     std::vector<PhaseTasks> pts;
     c.tasks->build(phases, c.grid, true, pts, walkBudget, costAware);
     std::vector<size_t> hOff(nPlans, 0);
@@ -75,7 +77,7 @@ void Staged::stage(Context& c, std::vector<DevPlan>& plans, const std::vector<co
         plans[i].memoBits = nullptr;
         if (plans[i].memoLevel > 0) {
             const DevStep& a = plans[i].steps[plans[i].memoLevel - 1];
-            const SuffixMemo* m = c.memo_for(a.pred, a.dir, plans[i].memoP2, plans[i].memoD2, s);
+            const SuffixMemo* m = c.memo_for(a.pred, a.dir, plans[i].memoP2, plans[i].memoD2);
             if (m && (plans[i].mode != kPairs || m->words == plans[i].rowWords)) {
                 plans[i].memoTab = m->tab;
                 plans[i].memoBits = m->bits;
@@ -128,53 +130,68 @@ void Staged::stage(Context& c, std::vector<DevPlan>& plans, const std::vector<co
     d2hBytes = (size_t)nPlans * sizeof(unsigned long long) + 8;
 }
 
-const SuffixMemo* Context::memo_for(int p1, int d1, int p2, int d2, cudaStream_t s) {
-    const uint64_t key = ((uint64_t)(uint32_t)(p1 * 2 + d1) << 32) | (uint32_t)(p2 * 2 + d2);
-    auto it = memos.find(key);
-    if (it != memos.end()) return it->second.get();
-    memos[key] = nullptr;
+namespace {
+uint64_t memo_key(int p1, int d1, int p2, int d2) {
+    return ((uint64_t)(uint32_t)(p1 * 2 + d1) << 32) | (uint32_t)(p2 * 2 + d2);
+}
+}  // namespace
+
+const SuffixMemo* Context::memo_for(int p1, int d1, int p2, int d2) const {
+    auto it = memos.find(memo_key(p1, d1, p2, d2));
+    return it == memos.end() ? nullptr : it->second.get();
+}
+
+void Context::ensure_memos(const std::vector<std::array<int, 4>>& keys, cudaStream_t s) {
     const HostIndex& h = hix;
     const int nHub = (int)h.hubOff.size();
-    if (memoGain < 0 || nHub == 0 || p1 < 0 || p2 < 0 || p1 >= h.nPred || p2 >= h.nPred) return nullptr;
-    const int words = (int)((h.pred_rows(p2, 1 - d2) + 31) / 32);
-    std::vector<int2> jobs;
-    std::vector<int32_t> tab(nHub, -1);
-    for (int32_t r = h.predRow[d1][p1]; r < h.predRow[d1][p1 + 1]; ++r) {
-        const int32_t hub = h.hubOf[d1][r];
-        if (hub < 0) continue;
-        double cand = 0;   // suffix candidates of this row: sum of the second-step degrees
-        for (int32_t e = h.rowBeg[d1][r]; e < h.rowBeg[d1][r + 1]; ++e) {
-            auto rr = h.row_range(p2, d2, h.val[d1][e]);
-            cand += rr.second - rr.first;
+    std::vector<MemoJob> all;
+    for (const auto& k : keys) {
+        const int p1 = k[0], d1 = k[1], p2 = k[2], d2 = k[3];
+        const uint64_t key = memo_key(p1, d1, p2, d2);
+        if (memos.count(key)) continue;
+        memos[key] = nullptr;
+        if (memoGain < 0 || nHub == 0 || p1 < 0 || p2 < 0 || p1 >= h.nPred || p2 >= h.nPred) continue;
+        const int words = (int)((h.pred_rows(p2, 1 - d2) + 31) / 32);
+        std::vector<int32_t> rows;
+        std::vector<int32_t> tab(nHub, -1);
+        for (int32_t r = h.predRow[d1][p1]; r < h.predRow[d1][p1 + 1]; ++r) {
+            const int32_t hub = h.hubOf[d1][r];
+            if (hub < 0) continue;
+            double cand = 0;   // suffix candidates of this row: sum of the second-step degrees
+            for (int32_t e = h.rowBeg[d1][r]; e < h.rowBeg[d1][r + 1]; ++e) {
+                auto rr = h.row_range(p2, d2, h.val[d1][e]);
+                cand += rr.second - rr.first;
+            }
+            if (cand < memoGain * words) continue;
+            tab[hub] = (int32_t)rows.size();
+            rows.push_back(r);
         }
-        if (cand < memoGain * words) continue;
-        tab[hub] = (int32_t)jobs.size();
-        jobs.push_back(make_int2(r, (int)jobs.size()));
+        const size_t tabBytes = ((size_t)nHub * 4 + 255) & ~size_t(255);
+        const size_t bitBytes = rows.size() * 2 * (size_t)words * 4;
+        if (rows.empty() || memoBytes + bitBytes > kMemoBudgetBytes) continue;
+        auto m = std::make_unique<SuffixMemo>();
+        m->rowHasMemo.assign((size_t)h.pred_rows(p1, d1), 0);
+        for (int32_t r : rows) m->rowHasMemo[(size_t)(r - h.predRow[d1][p1])] = 1;
+        m->buf.ensure(tabBytes + bitBytes);
+        char* base = static_cast<char*>(m->buf.p);
+        ck(cudaMemcpyAsync(base, tab.data(), (size_t)nHub * 4, cudaMemcpyHostToDevice, s), "H2D memo table");
+        ck(cudaMemsetAsync(base + tabBytes, 0, bitBytes, s), "clear memo bits");
+        m->tab = reinterpret_cast<const int32_t*>(base);
+        m->bits = reinterpret_cast<const uint32_t*>(base + tabBytes);
+        m->words = words;
+        m->slots = (int)rows.size();
+        for (size_t i = 0; i < rows.size(); ++i)
+            all.push_back(MemoJob{p1, d1, p2, d2, rows[i], words,
+                                  reinterpret_cast<uint32_t*>(base + tabBytes) + i * 2 * (size_t)words});
+        memoBytes += m->buf.cap;
+        memos[key] = std::move(m);
     }
-    const size_t tabBytes = ((size_t)nHub * 4 + 255) & ~size_t(255);
-    const size_t jobBytes = ((jobs.size() * sizeof(int2)) + 255) & ~size_t(255);
-    const size_t bitBytes = jobs.size() * 2 * (size_t)words * 4;
-    if (jobs.empty() || memoBytes + bitBytes > kMemoBudgetBytes) return nullptr;
-    auto m = std::make_unique<SuffixMemo>();
-    m->rowHasMemo.assign((size_t)h.pred_rows(p1, d1), 0);
-    for (const int2& j : jobs) m->rowHasMemo[(size_t)(j.x - h.predRow[d1][p1])] = 1;
-    m->buf.ensure(tabBytes + jobBytes + bitBytes);
-    char* base = static_cast<char*>(m->buf.p);
-    ck(cudaMemcpyAsync(base, tab.data(), (size_t)nHub * 4, cudaMemcpyHostToDevice, s), "H2D memo table");
-    ck(cudaMemcpyAsync(base + tabBytes, jobs.data(), jobs.size() * sizeof(int2), cudaMemcpyHostToDevice, s),
+    if (all.empty()) return;
+    memoJobs.ensure(all.size() * sizeof(MemoJob));
+    ck(cudaMemcpyAsync(memoJobs.p, all.data(), all.size() * sizeof(MemoJob), cudaMemcpyHostToDevice, s),
        "H2D memo jobs");
-    ck(cudaMemsetAsync(base + tabBytes + jobBytes, 0, bitBytes, s), "clear memo bits");
-    ck(memo_build(dix, p1, d1, p2, d2, reinterpret_cast<const int2*>(base + tabBytes), (int)jobs.size(),
-                  reinterpret_cast<uint32_t*>(base + tabBytes + jobBytes), words, s),
-       "memo build");
+    ck(memo_build(dix, static_cast<const MemoJob*>(memoJobs.p), (int)all.size(), s), "memo build");
     ck(cudaStreamSynchronize(s), "memo build");   // memos are shared by every stream afterwards
-    m->tab = reinterpret_cast<const int32_t*>(base);
-    m->bits = reinterpret_cast<const uint32_t*>(base + tabBytes + jobBytes);
-    m->words = words;
-    m->slots = (int)jobs.size();
-    memoBytes += m->buf.cap;
-    memos[key] = std::move(m);
-    return memos[key].get();
 }
 
 void Staged::enqueue(Context& c, cudaStream_t s, int instr, int gridCap) {

@@ -5,6 +5,7 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <array>
 #include <climits>
 #include <cstdio>
 #include <memory>
@@ -25,8 +26,7 @@ namespace gr {
 
 size_t engine_smem_bytes(int block);
 cudaError_t engine_configure();
-cudaError_t memo_build(const DevIndex& ix, int p1, int d1, int p2, int d2, const int2* jobs, int nJobs,
-                       uint32_t* bits, int words, cudaStream_t stream);
+cudaError_t memo_build(const DevIndex& ix, const MemoJob* jobs, int nJobs, cudaStream_t stream);
 cudaError_t engine_launch(const DevIndex& ix, const DevPlan* plans, const DevTask* tasks, int nTasks,
                           int* taskCounter, unsigned long long* results, int* status, int grid, int block,
                           cudaStream_t stream, const EngineProfile* prof);
@@ -194,9 +194,14 @@ struct Context {
     double memoGain = 0.25;
     std::unordered_map<uint64_t, std::unique_ptr<SuffixMemo>> memos;
     size_t memoBytes = 0;
-    // The memo for (p1, d1) -> (p2, d2), built (synchronously, on stream s)
-    // on first use; null when no hub row of (p1, d1) is worth one.
-    const SuffixMemo* memo_for(int p1, int d1, int p2, int d2, cudaStream_t s);
+    // Builds the memos of the transitions (p1, d1) -> (p2, d2) in `keys`
+    // that do not exist yet: one kernel over all their hub rows, one
+    // synchronisation of stream s (memos are shared by every stream after).
+    void ensure_memos(const std::vector<std::array<int, 4>>& keys, cudaStream_t s);
+    // The memo of (p1, d1) -> (p2, d2) if built, null when none exists or no
+    // hub row of (p1, d1) is worth one.
+    const SuffixMemo* memo_for(int p1, int d1, int p2, int d2) const;
+    DevBuf memoJobs;
     int serveLanes = 1;        // servers started on this context keep a heavy lane
     int serveHeavyShare = 2;   // the heavy lane launches on grid / serveHeavyShare blocks
     double serveHeavyNs = 5.0e6;

@@ -789,25 +789,25 @@ static void launch_b(const DevIndex& ix, const DevPlan* plans, const DevTask* ta
         engine_kernel<B, 0><<<grid, B, smem, stream>>>(ix, plans, tasks, nTasks, taskCounter, results, status, p);
 }
 
-// Suffix memos (see memo_item): one block per (hub row x, slot) job; warps
-// take the y in N1(x), lanes the h in N2(y).  The first witness of h sets
-// its S1 bit, any later one its S2 bit (atomicOr returns the old word).
-__global__ void memo_build_kernel(DevIndex ix, int p1, int d1, int p2, int d2, const int2* jobs, int nJobs,
-                                  uint32_t* bits, int words) {
+// Suffix memos (see memo_item): one block per job (a hub row x of one
+// transition); warps take the y in N1(x), lanes the h in N2(y).  The first
+// witness of h sets its S1 bit, any later one its S2 bit (atomicOr returns
+// the old word).
+__global__ void memo_build_kernel(DevIndex ix, const MemoJob* jobs, int nJobs) {
     if ((int)blockIdx.x >= nJobs) return;
-    const int2 job = jobs[blockIdx.x];
-    uint32_t* S1 = bits + (long long)job.y * 2 * words;
-    uint32_t* S2 = S1 + words;
+    const MemoJob job = jobs[blockIdx.x];
+    uint32_t* S1 = job.bits;
+    uint32_t* S2 = S1 + job.words;
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nWarps = blockDim.x >> 5;
-    const int b = ix.rowBeg[d1][job.x], e = ix.rowBeg[d1][job.x + 1];
+    const int b = ix.rowBeg[job.d1][job.row], e = ix.rowBeg[job.d1][job.row + 1];
     Meter<false> mt;
     for (int i = b + warp; i < e; i += nWarps) {
-        const int y = __ldg(ix.val[d1] + i);
-        const int2 r = row_lookup(ix, p2, d2, y, mt);
+        const int y = __ldg(ix.val[job.d1] + i);
+        const int2 r = row_lookup(ix, job.p2, job.d2, y, mt);
         for (int j = r.x + lane; j < r.y; j += 32) {
-            if (__ldg(ix.val[d2] + j) == y) continue;
-            const int rank = __ldg(ix.valRank[d2] + j);
-            if (rank < 0 || rank >= (words << 5)) continue;
+            if (__ldg(ix.val[job.d2] + j) == y) continue;
+            const int rank = __ldg(ix.valRank[job.d2] + j);
+            if (rank < 0 || rank >= (job.words << 5)) continue;
             const uint32_t bit = 1u << (rank & 31);
             const uint32_t old = atomicOr(S1 + (rank >> 5), bit);
             if (old & bit) atomicOr(S2 + (rank >> 5), bit);
@@ -815,10 +815,9 @@ __global__ void memo_build_kernel(DevIndex ix, int p1, int d1, int p2, int d2, c
     }
 }
 
-cudaError_t memo_build(const DevIndex& ix, int p1, int d1, int p2, int d2, const int2* jobs, int nJobs,
-                       uint32_t* bits, int words, cudaStream_t stream) {
+cudaError_t memo_build(const DevIndex& ix, const MemoJob* jobs, int nJobs, cudaStream_t stream) {
     if (nJobs <= 0) return cudaSuccess;
-    memo_build_kernel<<<nJobs, 256, 0, stream>>>(ix, p1, d1, p2, d2, jobs, nJobs, bits, words);
+    memo_build_kernel<<<nJobs, 256, 0, stream>>>(ix, jobs, nJobs);
     return cudaGetLastError();
 }
 
