@@ -13,6 +13,7 @@
 
 #include <algorithm>
 #include <climits>
+#include <cmath>
 #include <cstdio>
 #include <cstdlib>
 #include <cstring>
@@ -92,15 +93,30 @@ void Staged::stage(Context& c, std::vector<DevPlan>& plans, const std::vector<co
         cost.insert(cost.end(), pts[i].cost.begin(), pts[i].cost.end());
     }
     if (sortTasks && tasks.size() > 1) {
-        // longest (estimated device time) first, so the tail of the launch is short
-        std::vector<double> t(tasks.size());
-        for (size_t i = 0; i < tasks.size(); ++i) t[i] = cost[i] * pts[tasks[i].plan].scale;
-        std::vector<size_t> ord(tasks.size());
-        std::iota(ord.begin(), ord.end(), 0);
-        std::stable_sort(ord.begin(), ord.end(), [&](size_t a, size_t b) { return t[a] > t[b]; });
+        // longest (estimated device time) first, so the tail of the launch is
+        // short: a stable counting sort by quarter-octaves of the estimate
+        constexpr int kBuckets = 1024;
+        auto bucket = [](double v) {
+            if (!(v > 0.0)) return 0;
+            int e;
+            const double m = std::frexp(v, &e);   // v = m * 2^e, m in [0.5, 1)
+            return std::max(1, std::min(kBuckets - 1, 512 + 4 * e + (int)((m - 0.5) * 8.0)));
+        };
+        std::vector<uint16_t> bk(tasks.size());
+        std::vector<size_t> start(kBuckets + 1, 0);
+        for (size_t i = 0; i < tasks.size(); ++i) {
+            bk[i] = (uint16_t)bucket(cost[i] * pts[tasks[i].plan].scale);
+            ++start[kBuckets - 1 - bk[i]];
+        }
+        size_t acc = 0;
+        for (int b = 0; b <= kBuckets; ++b) { const size_t c = start[b]; start[b] = acc; acc += c; }
         std::vector<DevTask> t2(tasks.size());
         std::vector<double> c2(tasks.size());
-        for (size_t i = 0; i < ord.size(); ++i) { t2[i] = tasks[ord[i]]; c2[i] = cost[ord[i]]; }
+        for (size_t i = 0; i < tasks.size(); ++i) {
+            const size_t at = start[kBuckets - 1 - bk[i]]++;
+            t2[at] = tasks[i];
+            c2[at] = cost[i];
+        }
         tasks.swap(t2);
         cost.swap(c2);
     }
@@ -110,14 +126,14 @@ void Staged::stage(Context& c, std::vector<DevPlan>& plans, const std::vector<co
         int32_t acc = 0;
         for (int i = 0; i < nPlans; ++i) planTaskEnd.push_back(acc += (int32_t)pts[i].tasks.size());
     }
-    hTasks = tasks;
-    hCost = cost;
     size_t planBytes = (size_t)nPlans * sizeof(DevPlan);
     size_t taskBytes = (size_t)nTasks * sizeof(DevTask);
     size_t blob = planBytes + taskBytes;
     hBlob.ensure(blob);
     std::memcpy(hBlob.p, plans.data(), planBytes);
     std::memcpy(static_cast<char*>(hBlob.p) + planBytes, tasks.data(), taskBytes);
+    hTasks = std::move(tasks);   // kept for profiles and task-time learning
+    hCost = std::move(cost);
     dBlob.ensure(blob, as);
     dResults.ensure((size_t)nPlans * sizeof(unsigned long long), as);
     dCtl.ensure(64, as);
@@ -331,7 +347,9 @@ void evaluate_shard(Context& c, const Rule& rule, int shard, int nShards, long l
 }
 
 // Parses and plans n rules and stages their device phases.
-void prepare(Batch& b, Context& c, const char* const* rules, int n, int isJson) {
+// keepPlans: keep a copy of the plans for restaging (prepared batches that
+// may be autotuned); one-shot chunks skip it.
+void prepare(Batch& b, Context& c, const char* const* rules, int n, int isJson, bool keepPlans = true) {
     b.c = &c;
     b.n = n;
     b.owner.clear();
@@ -382,7 +400,8 @@ void prepare(Batch& b, Context& c, const char* const* rules, int n, int isJson) 
     if (!b.stream) ck(cudaStreamCreateWithFlags(&b.stream, cudaStreamNonBlocking), "cudaStreamCreate");
     if (!b.ev0) ck(cudaEventCreate(&b.ev0), "cudaEventCreate");
     if (!b.ev1) ck(cudaEventCreate(&b.ev1), "cudaEventCreate");
-    b.plans0 = plans;
+    if (keepPlans) b.plans0 = plans;
+    else b.plans0.clear();
     b.phases = phases;
     b.st.stage(c, plans, phases, true, b.stream, b.walkBudget);
 }
@@ -545,7 +564,7 @@ int gpu_evaluate_rules_batch(void* ctx, const char* const* rules, int n, int isJ
         for (int k = 0; k < K; ++k) {
             const int lo = (int)((long long)n * k / K), hi = (int)((long long)n * (k + 1) / K);
             Batch& b = *c.pipe[k];
-            prepare(b, c, rules + lo, hi - lo, isJson);
+            prepare(b, c, rules + lo, hi - lo, isJson, false);
             ck(cudaEventRecord(b.ev0, b.stream), "event");
             b.st.enqueue(c, b.stream, 0);
             ck(cudaEventRecord(b.ev1, b.stream), "event");

@@ -64,18 +64,26 @@ uint64_t phase_hash(const PhasePlan& ph) {
 }
 
 const int32_t* TaskBuilder::degrees(int32_t pred, int dir) {
-    auto it = deg_.find(pd_key(pred, dir));
-    if (it != deg_.end()) return it->second.data();
+    {
+        std::shared_lock<std::shared_mutex> lk(cacheMu_);
+        auto it = deg_.find(pd_key(pred, dir));
+        if (it != deg_.end()) return it->second.data();
+    }
     std::vector<int32_t> d((size_t)std::max(ix_.nEnt, 1), 0);
     for (int32_t r = ix_.predRow[dir][pred]; r < ix_.predRow[dir][pred + 1]; ++r)
         d[ix_.rowKey[dir][r]] = ix_.rowBeg[dir][r + 1] - ix_.rowBeg[dir][r];
-    cacheBytes_ += d.size() * 4;
-    return deg_.emplace(pd_key(pred, dir), std::move(d)).first->second.data();
+    std::unique_lock<std::shared_mutex> lk(cacheMu_);
+    auto ins = deg_.emplace(pd_key(pred, dir), std::move(d));
+    if (ins.second) cacheBytes_ += ins.first->second.size() * 4;
+    return ins.first->second.data();
 }
 
 double TaskBuilder::sb_fan(int32_t pred, int dir) {
-    auto it = sbFan_.find(pd_key(pred, dir));
-    if (it != sbFan_.end()) return it->second;
+    {
+        std::shared_lock<std::shared_mutex> lk(cacheMu_);
+        auto it = sbFan_.find(pd_key(pred, dir));
+        if (it != sbFan_.end()) return it->second;
+    }
     double s1 = 0, s2 = 0;
     for (int32_t r = ix_.predRow[dir][pred]; r < ix_.predRow[dir][pred + 1]; ++r) {
         double d = ix_.rowBeg[dir][r + 1] - ix_.rowBeg[dir][r];
@@ -83,7 +91,8 @@ double TaskBuilder::sb_fan(int32_t pred, int dir) {
         s2 += d * d;
     }
     double v = s1 > 0 ? s2 / s1 : 0.0;
-    sbFan_[pd_key(pred, dir)] = v;
+    std::unique_lock<std::shared_mutex> lk(cacheMu_);
+    sbFan_.emplace(pd_key(pred, dir), v);
     return v;
 }
 
@@ -107,8 +116,11 @@ double TaskBuilder::estimate(const PhasePlan& ph, bool hubAware) {
 
 const TaskBuilder::Hop2& TaskBuilder::hop2(int32_t p0, int d0, int32_t p1, int d1) {
     const uint64_t key = ((uint64_t)(uint32_t)p0 << 33) | ((uint64_t)d0 << 32) | ((uint64_t)(uint32_t)p1 << 1) | (uint64_t)d1;
-    auto it = hop2_.find(key);
-    if (it != hop2_.end()) return it->second;
+    {
+        std::shared_lock<std::shared_mutex> lk(cacheMu_);
+        auto it = hop2_.find(key);
+        if (it != hop2_.end()) return it->second;
+    }
     const int32_t* deg = degrees(p1, d1);
     Hop2 h;
     const int32_t r0 = ix_.predRow[d0][p0], r1 = ix_.predRow[d0][p0 + 1];
@@ -119,8 +131,10 @@ const TaskBuilder::Hop2& TaskBuilder::hop2(int32_t p0, int d0, int32_t p1, int d
         h.perRow[r - r0] = (float)acc;
         h.total += acc;
     }
-    cacheBytes_ += h.perRow.size() * sizeof(float);
-    return hop2_.emplace(key, std::move(h)).first->second;
+    std::unique_lock<std::shared_mutex> lk(cacheMu_);
+    auto ins = hop2_.emplace(key, std::move(h));
+    if (ins.second) cacheBytes_ += ins.first->second.perRow.size() * sizeof(float);
+    return ins.first->second;
 }
 
 bool TaskBuilder::chain_shaped(const DevPlan& P) const {
@@ -251,17 +265,18 @@ void TaskBuilder::build(const std::vector<const PhasePlan*>& phases, int blocks,
     std::vector<double> estAvg(n), estHub(n), scale(n, defaultCalib_);
     std::vector<const std::vector<float>*> walked(n, nullptr);
     std::vector<char> forced(n, 0);
-    for (size_t i = 0; i < n; ++i) {
+    const bool learned = !calib_.empty() || !mustWalk_.empty();
+    parallel_for(n, [&](size_t i) {
         estAvg[i] = estimate2(*phases[i]);
         estHub[i] = split ? estimate(*phases[i], true) : estAvg[i];
         out[i].work = estAvg[i];
-        if (!calib_.empty() || !mustWalk_.empty()) {
+        if (learned) {
             const uint64_t sig = signature(*phases[i]);
             auto c = calib_.find(sig);
             if (c != calib_.end()) scale[i] = c->second;
             forced[i] = mustWalk_.count(sig) ? 1 : 0;
         }
-    }
+    }, 128);
     if (split) {
         std::vector<size_t> ord(n);
         std::iota(ord.begin(), ord.end(), 0);

@@ -2,6 +2,7 @@
 #pragma once
 #include <cstdint>
 #include <functional>
+#include <shared_mutex>
 #include <string>
 #include <unordered_map>
 #include <utility>
@@ -106,6 +107,10 @@ private:
     std::unordered_map<uint64_t, bool> mustWalk_;               // phase hash -> walk next time
     double defaultCalib_ = 1.0;
     size_t cacheBytes_ = 0;
+    // guards deg_, sbFan_, hop2_ and cacheBytes_ while the estimates of a
+    // build run on several threads (entries are never erased during a build,
+    // so references handed out stay valid)
+    mutable std::shared_mutex cacheMu_;
 
     const int32_t* degrees(int32_t pred, int dir);
     double sb_fan(int32_t pred, int dir);
