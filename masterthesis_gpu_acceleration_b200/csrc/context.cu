@@ -481,13 +481,17 @@ void* gpu_load_graph(const char* ttlPath) {
     try {
         c = new Context();
         std::vector<int32_t> spo;
-        std::string err;
-        if (!parse_turtle_file(ttlPath, c->ents, c->preds, spo, &err)) {
+        std::string err, text;
+        if (!read_file(ttlPath, text, &err)) {
             set_error("Failed to parse TTL: " + std::string(ttlPath) + " (" + err + ")");
             delete c;
             return nullptr;
         }
-        c->prefixes = scan_rule_prefixes(ttlPath);
+        // one read of the file: the triples (several threads) and the rule
+        // parser's prefix lines come from the same text
+        parse_turtle_text_parallel(text, c->ents, c->preds, spo);
+        c->prefixes = scan_rule_prefixes_text(text);
+        std::string().swap(text);
         // GPU_RULES_MEMO_GAIN overrides the suffix-memo threshold (negative: no memos)
         if (const char* g = std::getenv("GPU_RULES_MEMO_GAIN")) c->memoGain = std::atof(g);
         // GPU_RULES_HUB_MIN_DEGREE overrides the hub-row threshold (0: no hub rows)

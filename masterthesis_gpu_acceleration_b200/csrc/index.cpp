@@ -8,6 +8,7 @@
 // open-addressing table keyed by (predicate, direction, key), so the whole
 // lookup structure of a DBpedia-sized graph stays inside L2.
 #include "index.hpp"
+#include "parallel.hpp"
 
 #include <algorithm>
 #include <numeric>
@@ -24,7 +25,7 @@ inline bool t3_less(const T3& a, const T3& b) {
 }
 
 void build_dir(HostIndex& ix, int d, std::vector<T3>& t) {
-    std::sort(t.begin(), t.end(), t3_less);
+    if (!std::is_sorted(t.begin(), t.end(), t3_less)) parallel_sort(t, t3_less);
     size_t n = t.size();
     auto& val = ix.val[d];
     auto& src = ix.src[d];
@@ -141,7 +142,7 @@ HostIndex build_index(const std::vector<int32_t>& spo, int32_t nEnt, int32_t nPr
     size_t n = spo.size() / 3;
     std::vector<T3> t(n);
     for (size_t i = 0; i < n; ++i) t[i] = {spo[3 * i + 1], spo[3 * i], spo[3 * i + 2]};
-    std::sort(t.begin(), t.end(), t3_less);
+    parallel_sort(t, t3_less);
     t.erase(std::unique(t.begin(), t.end(), [](const T3& a, const T3& b) {
                 return a.p == b.p && a.k == b.k && a.v == b.v;
             }), t.end());
@@ -154,9 +155,10 @@ HostIndex build_index(const std::vector<int32_t>& spo, int32_t nEnt, int32_t nPr
     for (int d = 0; d < 2; ++d) {
         auto& vr = ix.valRank[d];
         vr.resize(ix.val[d].size());
-        for (int32_t p = 0; p < nPred; ++p)
+        parallel_for((size_t)nPred, [&](size_t p) {
             for (int32_t e = ix.predEdge[d][p]; e < ix.predEdge[d][p + 1]; ++e)
-                vr[e] = key_rank(ix, 1 - d, p, ix.val[d][e]);
+                vr[e] = key_rank(ix, 1 - d, (int32_t)p, ix.val[d][e]);
+        }, 1);
     }
     // (pred, dir, key) table at load factor <= 1/2
     size_t rows = ix.rowKey[0].size() + ix.rowKey[1].size();
@@ -164,16 +166,26 @@ HostIndex build_index(const std::vector<int32_t>& spo, int32_t nEnt, int32_t nPr
     while (cap < 2 * rows) cap <<= 1;
     ix.hash.assign(cap, HashSlot{kEmptyTag, 0, 0, 0});
     ix.hashMask = (uint32_t)(cap - 1);
+    // rows are distinct, so threads only need to claim empty slots (the
+    // slot order may differ between runs; lookups do not depend on it)
     for (int d = 0; d < 2; ++d) {
-        for (int32_t p = 0; p < nPred; ++p) {
-            uint32_t tag = (uint32_t)p * 2u + (uint32_t)d;
+        parallel_for((size_t)nPred, [&](size_t p) {
+            const uint32_t tag = (uint32_t)p * 2u + (uint32_t)d;
             for (int32_t r = ix.predRow[d][p]; r < ix.predRow[d][p + 1]; ++r) {
-                uint32_t key = (uint32_t)ix.rowKey[d][r];
+                const uint32_t key = (uint32_t)ix.rowKey[d][r];
                 uint32_t i = slot_hash(tag, key) & ix.hashMask;
-                while (ix.hash[i].tag != kEmptyTag) i = (i + 1) & ix.hashMask;
-                ix.hash[i] = HashSlot{tag, key, (uint32_t)ix.rowBeg[d][r], (uint32_t)ix.rowBeg[d][r + 1]};
+                for (;;) {
+                    uint32_t expect = kEmptyTag;
+                    if (__atomic_compare_exchange_n(&ix.hash[i].tag, &expect, tag, false, __ATOMIC_RELAXED,
+                                                    __ATOMIC_RELAXED))
+                        break;
+                    i = (i + 1) & ix.hashMask;
+                }
+                ix.hash[i].key = key;
+                ix.hash[i].beg = (uint32_t)ix.rowBeg[d][r];
+                ix.hash[i].end = (uint32_t)ix.rowBeg[d][r + 1];
             }
-        }
+        }, 1);
     }
     build_hubs(ix, hubMinDegree);
     return ix;

@@ -46,4 +46,26 @@ void parallel_for(size_t n, Fn fn, size_t grain = 64, unsigned maxThreads = 16) 
     if (err) std::rethrow_exception(err);
 }
 
+// Sorts v with cmp on several threads: chunks are sorted in parallel, then
+// merged pairwise, level by level, in parallel.
+template <class T, class Cmp>
+void parallel_sort(std::vector<T>& v, Cmp cmp, size_t minChunk = size_t(1) << 16) {
+    const unsigned hw = std::max(1u, std::thread::hardware_concurrency());
+    size_t parts = std::min<size_t>(std::min(hw, 16u), v.size() / std::max<size_t>(minChunk, 1));
+    if (parts < 2) {
+        std::sort(v.begin(), v.end(), cmp);
+        return;
+    }
+    std::vector<size_t> b(parts + 1);
+    for (size_t k = 0; k <= parts; ++k) b[k] = v.size() * k / parts;
+    parallel_for(parts, [&](size_t k) { std::sort(v.begin() + b[k], v.begin() + b[k + 1], cmp); }, 1);
+    for (size_t width = 1; width < parts; width *= 2) {
+        const size_t pairs = (parts + 2 * width - 1) / (2 * width);
+        parallel_for(pairs, [&](size_t q) {
+            const size_t lo = 2 * width * q, mid = std::min(parts, lo + width), hi = std::min(parts, lo + 2 * width);
+            if (mid < hi) std::inplace_merge(v.begin() + b[lo], v.begin() + b[mid], v.begin() + b[hi], cmp);
+        }, 1);
+    }
+}
+
 }  // namespace gr

@@ -36,10 +36,20 @@ bool parse_turtle_file(const std::string& path, TermDict& ents, TermDict& preds,
                        std::vector<int32_t>& spo, std::string* err);
 bool parse_turtle_text(const std::string& text, TermDict& ents, TermDict& preds,
                        std::vector<int32_t>& spo);
+// The same result (identical ids and triple order) read by several threads:
+// the text is cut after statement ends into chunks of at least minChunk
+// bytes, each read with the prefixes of the first chunk, and the chunks'
+// dictionaries are merged in file order.  Texts with long literals ("""),
+// anonymous nodes ([ ]) or prefix declarations after the first chunk are
+// read by one reader.
+bool parse_turtle_text_parallel(const std::string& text, TermDict& ents, TermDict& preds,
+                                std::vector<int32_t>& spo, size_t minChunk = size_t(4) << 20);
+bool read_file(const std::string& path, std::string& text, std::string* err);
 
 // Prefix map the rule parser uses: a line-based scan for '@prefix' or
 // 'prefix' lines with a non-empty name and IRI, as
 // CPU_01_nonparallel/RuleParser.cpp:48-93 reads them.
 std::unordered_map<std::string, std::string> scan_rule_prefixes(const std::string& path);
+std::unordered_map<std::string, std::string> scan_rule_prefixes_text(const std::string& text);
 
 }  // namespace gr

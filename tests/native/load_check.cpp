@@ -1,0 +1,48 @@
+// Native check of the graph load path (built and run by tests/test_load_cpu.py):
+//   1. the multi-threaded Turtle read gives the same dictionaries and triples,
+//      in the same order, as one reader over the whole text;
+//   2. in the index built on several threads every row is found through the
+//      lookup table at its own edge range, every triple is found, and every
+//      value rank is the value's row in the other direction.
+// Usage: load_check FILE.ttl MIN_CHUNK_BYTES
+#include <cstdio>
+#include <cstdlib>
+#include <string>
+#include <vector>
+
+#include "../../masterthesis_gpu_acceleration_b200/csrc/index.hpp"
+#include "../../masterthesis_gpu_acceleration_b200/csrc/turtle.hpp"
+
+using namespace gr;
+
+int main(int argc, char** argv) {
+    if (argc < 3) return 2;
+    std::string text, err;
+    if (!read_file(argv[1], text, &err)) { std::fprintf(stderr, "%s\n", err.c_str()); return 2; }
+    TermDict e1, p1, e2, p2;
+    std::vector<int32_t> s1, s2;
+    parse_turtle_text(text, e1, p1, s1);
+    parse_turtle_text_parallel(text, e2, p2, s2, (size_t)std::atol(argv[2]));
+    if (e1.names != e2.names || p1.names != p2.names || s1 != s2) {
+        std::printf("parallel read differs\n");
+        return 1;
+    }
+    HostIndex ix = build_index(s2, (int32_t)e2.size(), (int32_t)p2.size(), 1);
+    long bad = 0;
+    for (int d = 0; d < 2; ++d)
+        for (int32_t p = 0; p < ix.nPred; ++p)
+            for (int32_t r = ix.predRow[d][p]; r < ix.predRow[d][p + 1]; ++r) {
+                auto rr = ix.row_range(p, d, ix.rowKey[d][r]);
+                if (rr.first != ix.rowBeg[d][r] || rr.second != ix.rowBeg[d][r + 1]) ++bad;
+                for (int32_t e = ix.rowBeg[d][r]; e < ix.rowBeg[d][r + 1]; ++e) {
+                    auto back = ix.row_range(p, 1 - d, ix.val[d][e]);
+                    const int32_t row = ix.predRow[1 - d][p] + ix.valRank[d][e];
+                    if (back.first != ix.rowBeg[1 - d][row]) ++bad;
+                }
+            }
+    for (size_t i = 0; i + 2 < s2.size(); i += 3)
+        if (!ix.has_triple(s2[i + 1], s2[i], s2[i + 2])) ++bad;
+    std::printf("triples %zu rows %zu hubs %zu mismatches %ld\n", s2.size() / 3,
+                ix.rowKey[0].size() + ix.rowKey[1].size(), ix.hubOff.size(), bad);
+    return bad == 0 ? 0 : 1;
+}
