@@ -213,6 +213,13 @@ void gpu_serve_stop(void* server);
 /* Number of entities, predicates and distinct triples of a loaded graph. */
 int gpu_graph_stats(void* ctx, long long* entities, long long* predicates, long long* triples);
 
+/* Predicate `index` (0 .. predicates - 1): its IRI into name (at most
+ * capacity - 1 bytes and a terminating 0; name may be NULL to ask for the
+ * length) and its distinct triples into *triples (optional).  Returns the
+ * IRI's length, or -1 for a bad index.  No counterpart in the reference (a
+ * rule miner enumerates head and body predicates with it). */
+int gpu_graph_predicate(void* ctx, long long index, char* name, int capacity, long long* triples);
+
 /* Last error message of the calling thread ("" if none). */
 const char* gpu_last_error(void);
 

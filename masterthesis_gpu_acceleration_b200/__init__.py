@@ -43,6 +43,7 @@ API_SYMBOLS = (
     "gpu_serve_stats",
     "gpu_serve_stop",
     "gpu_graph_stats",
+    "gpu_graph_predicate",
     "gpu_batch_counts",
     "gpu_evaluate_rule_shard",
     "gpu_last_error",
@@ -145,6 +146,9 @@ def load_library(path: os.PathLike | str | None = None) -> ctypes.CDLL:
         [ctypes.POINTER(ctypes.c_double)] * 2
     lib.gpu_serve_stop.restype = None
     lib.gpu_serve_stop.argtypes = [ctypes.c_void_p]
+    lib.gpu_graph_predicate.restype = ctypes.c_int
+    lib.gpu_graph_predicate.argtypes = [ctypes.c_void_p, ctypes.c_longlong, ctypes.c_char_p, ctypes.c_int,
+                                        ctypes.POINTER(ctypes.c_longlong)]
     lib.gpu_graph_stats.restype = ctypes.c_int
     lib.gpu_graph_stats.argtypes = [ctypes.c_void_p] + [ctypes.POINTER(ctypes.c_longlong)] * 3
     lib.gpu_last_error.restype = ctypes.c_char_p
@@ -241,6 +245,20 @@ class GpuRulesLib:
         e, p, t = ctypes.c_longlong(), ctypes.c_longlong(), ctypes.c_longlong()
         self._lib.gpu_graph_stats(self._handle(), ctypes.byref(e), ctypes.byref(p), ctypes.byref(t))
         return {"entities": e.value, "predicates": p.value, "triples": t.value}
+
+    def predicates(self) -> list[tuple[str, int]]:
+        """(IRI, distinct triples) of every predicate of the graph, by id."""
+        out = []
+        n = self.stats()["predicates"]
+        buf = ctypes.create_string_buffer(4096)
+        t = ctypes.c_longlong()
+        for i in range(n):
+            k = self._lib.gpu_graph_predicate(self._handle(), i, None, 0, None)
+            if k >= len(buf):
+                buf = ctypes.create_string_buffer(k + 1)
+            self._lib.gpu_graph_predicate(self._handle(), i, buf, len(buf), ctypes.byref(t))
+            out.append((buf.value.decode(errors="replace"), t.value))
+        return out
 
     def close(self) -> None:
         if getattr(self, "_ctx", None) is not None and self._ctx.value:

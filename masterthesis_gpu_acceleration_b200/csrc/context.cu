@@ -765,6 +765,20 @@ int gpu_graph_stats(void* ctx, long long* entities, long long* predicates, long 
     return 0;
 }
 
+int gpu_graph_predicate(void* ctx, long long index, char* name, int capacity, long long* triples) {
+    if (!ctx) return -1;
+    Context& c = *as_ctx(ctx);
+    if (index < 0 || index >= (long long)c.preds.size()) return -1;
+    const std::string& s = c.preds.names[(size_t)index];
+    if (triples) *triples = (long long)c.hix.pred_size((int32_t)index);
+    if (name && capacity > 0) {
+        const size_t n = std::min(s.size(), (size_t)capacity - 1);
+        std::memcpy(name, s.data(), n);
+        name[n] = 0;
+    }
+    return (int)s.size();
+}
+
 }  // extern "C"
 
 // ---------------------------------------------------------------------------
