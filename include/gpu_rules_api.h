@@ -150,11 +150,16 @@ void gpu_batch_free(void* batch);
 int gpu_evaluate_rule_noalloc(void* ctx, const char* ruleText, GpuRuleResult* out);
 
 /* Engine option for later calls on this context.  "block": threads per
- * block of the engine kernel, 128, 256 or 512 (default 512; the environment
+ * block of the engine kernel, 128, 256 or 512 (default 256; the environment
  * variable GPU_RULES_BLOCK sets it at load).  "task_target": fixed work per
  * task in candidate bindings (0 = automatic balancing).  "walk_threshold":
  * estimated work above which a phase's roots are measured one by one before
- * splitting (default 200000).  Servers started afterwards: "serve_lanes"
+ * splitting (default 200000).  "rule_block": block size the plain per-rule
+ * calls launch on (default 512; 0, or a size not above "block", = "block");
+ * their plans keep the layout of "block", so they reuse what batches learnt.
+ * "rule_walk_budget": per-root measurement allowed per per-rule call.
+ * "batch_chunks": pipelined chunks of gpu_evaluate_rules_batch (0 =
+ * automatic).  Servers started afterwards: "serve_lanes"
  * (1: keep a heavy lane, default; 0: all slots alike), "serve_heavy_share"
  * (the heavy lane launches on 1/share of the blocks, default 2) and
  * "serve_heavy_us" (expected device time in microseconds above which a

@@ -159,7 +159,7 @@ struct DevTask {
 // its frontier levels and its dedup bitmap, so 1024 / B blocks stay
 // resident per SM.
 struct Geom {
-    int block = 512;
+    int block = 256;
     static constexpr int pool_for(int b) { return 48 * b; }
     int poolInts() const { return pool_for(block); }
 };

@@ -123,8 +123,23 @@ void Staged::stage(Context& c, std::vector<DevPlan>& plans, const std::vector<co
     nTasks = (int)tasks.size();
     planTaskEnd.clear();
     if (!sortTasks) {
+        // one launch per plan: each plan's tasks stay contiguous, longest
+        // first within the plan
         int32_t acc = 0;
-        for (int i = 0; i < nPlans; ++i) planTaskEnd.push_back(acc += (int32_t)pts[i].tasks.size());
+        std::vector<int32_t> ord;
+        for (int i = 0; i < nPlans; ++i) {
+            const int32_t b = acc, e = acc + (int32_t)pts[i].tasks.size();
+            ord.resize((size_t)(e - b));
+            std::iota(ord.begin(), ord.end(), b);
+            std::stable_sort(ord.begin(), ord.end(), [&](int32_t x, int32_t y) { return cost[x] > cost[y]; });
+            for (int32_t k = b; k < e; ++k) {
+                pts[i].tasks[k - b] = tasks[ord[k - b]];
+                pts[i].cost[k - b] = cost[ord[k - b]];
+            }
+            std::copy(pts[i].tasks.begin(), pts[i].tasks.end(), tasks.begin() + b);
+            std::copy(pts[i].cost.begin(), pts[i].cost.end(), cost.begin() + b);
+            planTaskEnd.push_back(acc = e);
+        }
     }
     size_t planBytes = (size_t)nPlans * sizeof(DevPlan);
     size_t taskBytes = (size_t)nTasks * sizeof(DevTask);
@@ -292,6 +307,22 @@ int64_t run_one_phase(Context& c, const PhasePlan& ph, float* ms) {
     return (int64_t)c.one.counts()[0];
 }
 
+// Runs fn with the context's launch block size and grid switched to the
+// per-rule block size, restoring them afterwards (also when fn throws).
+// Only launches run under it: plans keep the batch geometry, whose shared
+// pool is a prefix of the larger block's, so per-rule calls share the
+// batch's cached walks and learnt costs (both keyed by plan signature).
+template <class Fn>
+void with_rule_block(Context& c, Fn fn) {
+    struct Restore {
+        Context& c;
+        int block, grid;
+        ~Restore() { c.geom.block = block; c.grid = grid; }
+    } restore{c, c.geom.block, c.grid};
+    if (c.ruleBlock > c.geom.block) c.set_block(c.ruleBlock);
+    fn();
+}
+
 // Both phases of one rule, each in its own launch timed by its own events,
 // issued back to back with one host synchronisation.
 int evaluate_parsed(Context& c, const Rule& rule, GpuRuleResult* out) {
@@ -307,7 +338,7 @@ int evaluate_parsed(Context& c, const Rule& rule, GpuRuleResult* out) {
     if (!plans.empty()) {
         // one upload, one launch per phase (each timed on the device), one download
         c.one.stage(c, plans, phases, false, c.stream, c.ruleWalkBudget, true);
-        c.one.enqueue_per_plan(c, c.stream);
+        with_rule_block(c, [&] { c.one.enqueue_per_plan(c, c.stream); });
         c.one.download_spans(c.stream);
         ck(cudaStreamSynchronize(c.stream), "engine");
         if (static_cast<const int*>(c.one.hCtl.p)[2] != 0)
@@ -747,6 +778,10 @@ int gpu_set_option(void* ctx, const char* name, long long value) {
     if (n == "serve_lanes" && (value == 0 || value == 1)) { c.serveLanes = (int)value; return 0; }
     if (n == "rule_walk_budget" && value >= 0) { c.ruleWalkBudget = (double)value; return 0; }
     if (n == "batch_chunks" && value >= 0 && value <= 16) { c.batchChunks = (int)value; return 0; }
+    if (n == "rule_block" && (value == 0 || value == 128 || value == 256 || value == 512)) {
+        c.ruleBlock = (int)value;
+        return 0;
+    }
     if (n == "serve_heavy_share" && value >= 1 && value <= 16) { c.serveHeavyShare = (int)value; return 0; }
     if (n == "serve_heavy_us" && value >= 0) { c.serveHeavyNs = 1e3 * (double)value; return 0; }
     return -1;

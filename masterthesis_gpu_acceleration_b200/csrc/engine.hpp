@@ -282,6 +282,10 @@ struct Context {
         grid = sms * (1024 / b);
         return true;
     }
+    // Plain per-rule calls launch on 512-thread blocks: one rule has few
+    // tasks, which finish sooner on larger blocks.  Their plans keep the
+    // layout of geom.block.  0 (or a size not above geom.block): geom.block.
+    int ruleBlock = 512;
 
     void init_device() {
         ck(cudaGetDevice(&device), "cudaGetDevice");

@@ -245,9 +245,17 @@ const TaskBuilder::Walk& TaskBuilder::walk(const PhasePlan& ph, uint64_t sig) {
             for (int32_t e = seg.first; e < seg.second; ++e) acc += child_work(P, vals, e, deg2, tail);
         w[r - ph.rootBeg] = (float)acc;
     }
-    cacheBytes_ += w.size() * sizeof(float) + sizeof(Walk);
     Walk entry;
     for (float x : w) entry.sum += x;
+    const size_t nb = w.size() / kWalkBlock;
+    entry.bsum.assign(nb, 0.0);
+    entry.bmax.assign(nb, 0.f);
+    for (size_t b = 0; b < nb; ++b)
+        for (size_t k = b * kWalkBlock; k < (b + 1) * kWalkBlock; ++k) {
+            entry.bsum[b] += w[k];
+            entry.bmax[b] = std::max(entry.bmax[b], w[k]);
+        }
+    cacheBytes_ += w.size() * sizeof(float) + nb * (sizeof(double) + sizeof(float)) + sizeof(Walk);
     entry.w = std::move(w);
     return walks_.emplace(sig, std::move(entry)).first->second;
 }
@@ -263,7 +271,7 @@ void TaskBuilder::build(const std::vector<const PhasePlan*>& phases, int blocks,
         cacheBytes_ = 0;
     }
     std::vector<double> estAvg(n), estHub(n), scale(n, defaultCalib_);
-    std::vector<const std::vector<float>*> walked(n, nullptr);
+    std::vector<const Walk*> walked(n, nullptr);
     std::vector<char> forced(n, 0);
     const bool learned = !calib_.empty() || !mustWalk_.empty();
     parallel_for(n, [&](size_t i) {
@@ -303,7 +311,7 @@ void TaskBuilder::build(const std::vector<const PhasePlan*>& phases, int blocks,
             if (costAware && !cached && estAvg[i] * scale[i] < kWalkNsPerEdge * edges) continue;
             if (!cached) used += edges;   // cached walks cost nothing
             const Walk& wk = walk(ph, sig);
-            walked[i] = &wk.w;
+            walked[i] = &wk;
             out[i].work = wk.sum;
         }
     }
@@ -329,8 +337,8 @@ void TaskBuilder::build(const std::vector<const PhasePlan*>& phases, int blocks,
         if (ph.needsGlobalBitmap) g = std::min(P.cap, 512);
         const int32_t R = ph.rootEnd - ph.rootBeg;
         const double uniform = R > 0 ? std::max(1.0, pt.work / R) : 1.0;
-        const std::vector<float>* w = walked[i];
-        if (!w) {
+        const Walk* wk = walked[i];
+        if (!wk) {
             // uniform cost per root: fixed-size chunks, no per-root pass
             const double per = uniform * sc;
             int32_t chunk = g;
@@ -353,19 +361,40 @@ void TaskBuilder::build(const std::vector<const PhasePlan*>& phases, int blocks,
             acc = 0;
             accUnits = 0;
         };
+        const std::vector<float>& w = wk->w;
+        const bool canSplit = split && P.m >= 1;
+        // Roots heavier than splitAt are cut into slices of `target`.  A
+        // launch of one rule (costAware) cuts only roots above a block's fair
+        // share of the phase: lighter ones cannot hold up its end, and each
+        // cut costs host time per first-segment edge.
+        const double splitAt = costAware ? std::max(target, pt.work * sc / std::max(blocks, 1)) : target;
+        double tail = 1.0;
+        for (int s = 2; s < P.m; ++s) tail *= std::max(1.0, avg_fan(P.steps[s]));
+        const int32_t* deg2 =
+            (canSplit && P.m >= 2 && P.steps[1].kind == kExpand) ? degrees(P.steps[1].pred, P.steps[1].dir) : nullptr;
         for (int32_t r = ph.rootBeg; r < ph.rootEnd; ++r) {
-            const double wu = w ? (double)(*w)[r - ph.rootBeg] : uniform;
+            const int32_t o = r - ph.rootBeg;
+            if (o % kWalkBlock == 0 && (size_t)(o / kWalkBlock) < wk->bsum.size()) {
+                // a whole block that neither holds a heavy root nor ends the
+                // current task (roots below exceed neither bound one by one)
+                const size_t b = (size_t)(o / kWalkBlock);
+                const double bs = wk->bsum[b];
+                if ((!canSplit || (double)wk->bmax[b] * sc <= splitAt) && acc + bs * sc <= target &&
+                    r + kWalkBlock - 1 - gb < g) {
+                    acc += bs * sc;
+                    accUnits += bs;
+                    r += kWalkBlock - 1;
+                    continue;
+                }
+            }
+            const double wu = (double)w[o];
             const double wr = wu * sc;
-            if (split && w && wr > target && P.m >= 1) {
+            if (canSplit && wr > splitAt) {
                 // a heavy root: slices of its first segment, one task each
                 flush(r);
                 int32_t vals[2];
                 root_vals(P, r, vals);
                 auto seg = first_segment(P, r, vals);
-                double tail = 1.0;
-                for (int s = 2; s < P.m; ++s) tail *= std::max(1.0, avg_fan(P.steps[s]));
-                const int32_t* deg2 =
-                    (P.m >= 2 && P.steps[1].kind == kExpand) ? degrees(P.steps[1].pred, P.steps[1].dir) : nullptr;
                 size_t first = pt.tasks.size();
                 int32_t s0 = 0;
                 double sa = 0;

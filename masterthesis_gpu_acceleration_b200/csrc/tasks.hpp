@@ -51,7 +51,8 @@ public:
     // walkBudget: first-segment edges that may be newly walked (cached
     // walks and phases marked by learn() are not counted).
     // costAware: walk a phase only when its expected device time exceeds
-    // the walk's own host time (per-rule launches, where nothing overlaps).
+    // the walk's own host time, and cut only roots above a block's fair
+    // share of their phase (per-rule launches, where nothing overlaps).
     void build(const std::vector<const PhasePlan*>& phases, int blocks, bool split,
                std::vector<PhaseTasks>& out, double walkBudget = 4.0e6, bool costAware = false);
 
@@ -93,8 +94,14 @@ private:
     const HostIndex& ix_;
     std::unordered_map<int64_t, std::vector<int32_t>> deg_;      // (pred, dir) -> degree by entity
     std::unordered_map<int64_t, double> sbFan_;                  // (pred, dir) -> size-biased fan-out
+    // Per-root work, and its sum and maximum over blocks of kWalkBlock
+    // roots, so that task building steps over runs of light roots a block
+    // at a time.
+    static constexpr int kWalkBlock = 16;
     struct Walk {
-        std::vector<float> w;   // per-root work
+        std::vector<float> w;      // per-root work
+        std::vector<double> bsum;  // per block of kWalkBlock roots (full blocks only)
+        std::vector<float> bmax;
         double sum = 0.0;
     };
     std::unordered_map<uint64_t, Walk> walks_;                   // phase hash -> per-root work

@@ -162,7 +162,7 @@ def test_prepared_batch_replays_exactly(tmp_path):
 
 
 @pytest.mark.parametrize("name", ["fuzz_0.json", "fuzz_2.json", "fuzz_5.json"])
-@pytest.mark.parametrize("block", [128, 512])
+@pytest.mark.parametrize("block", [128, 256, 512])
 def test_fuzz_forced_splitting(name, block, tmp_path):
     """Every root is measured and every root with more than a few candidates
     is split into first-segment slices deduplicated in global rows."""
@@ -175,7 +175,12 @@ def test_fuzz_forced_splitting(name, block, tmp_path):
         lib.set_option("task_target", 3)
         res, st, _ = lib.evaluate_rules_batch(fx["rules"])
         _check(res, fx["expected"], f"batch split block={block}")
-        _check([lib.evaluate_rule(t) for t in fx["rules"][:60]], fx["expected"][:60], "per-rule split")
+        # per-rule launches on the batch block size, then on 512-thread
+        # blocks with plans laid out for the batch block size
+        for rule_block in (0, 512):
+            lib.set_option("rule_block", rule_block)
+            _check([lib.evaluate_rule(t) for t in fx["rules"][:60]], fx["expected"][:60],
+                   f"per-rule split block={block} rule_block={rule_block}")
 
 
 @pytest.mark.parametrize("hub_min,memo_gain", [("1", "0"), ("1", "-1"), ("0", "8")])
