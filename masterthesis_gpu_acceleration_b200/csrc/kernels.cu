@@ -188,12 +188,15 @@ __device__ __forceinline__ unsigned long long block_sum(unsigned long long x, Bl
 // y0 lies in N1(x) (injectivity on y), the h in N2(y0) that have no witness
 // but y0 (those outside S2).  Ranks within a row ascend with the values, so
 // each lane merges its own run of words with N2(y0)'s sorted ranks.  The
-// whole warp calls this; new pair bits are counted on insertion.
+// whole warp calls this; new pair bits are counted on insertion and
+// returned (per lane).  Steps come by value and counts go back as the
+// result, so that the caller's loop state never needs an address.
 template <bool kC>
-__device__ __noinline__ void memo_item(const DevPlan& P, const DevIndex& ix, const DevStep& stA,
-                                          const DevStep& stB, const int* par, int lenK, int slot, uint32_t* dst,
-                                          int words, int* ex, int lane, unsigned long long& myNew, Meter<kC>& mt,
-                                          bool sharedDst) {
+__device__ __noinline__ unsigned long long memo_item(const DevPlan& P, const DevIndex& ix, const DevStep stA,
+                                                     const DevStep stB, const int* par, int lenK, int slot,
+                                                     uint32_t* dst, int words, int* ex, int lane, Meter<kC>& mt,
+                                                     bool sharedDst) {
+    unsigned long long myNew = 0;
     const int nEx = lenK - kTupleHead;
     const int exDir = 1 - stB.dir;
     const int segBeg = par[lenK], segLen = par[lenK + 1];
@@ -253,6 +256,7 @@ __device__ __noinline__ void memo_item(const DevPlan& P, const DevIndex& ix, con
         }
     }
     __syncwarp();
+    return myNew;
 }
 
 // kExist counterpart of memo_item: the item's last step expands a hub row x
@@ -262,7 +266,7 @@ __device__ __noinline__ void memo_item(const DevPlan& P, const DevIndex& ix, con
 // bit of h, with one the S2 bit; with more the item is left to enumeration.
 // Returns 1 (a grounding exists), 0 (none) or -1 (undecided).
 template <bool kC>
-__device__ __noinline__ int memo_exists(const DevPlan& P, const DevIndex& ix, const DevStep& stA, const int* it,
+__device__ __noinline__ int memo_exists(const DevPlan& P, const DevIndex& ix, const DevStep stA, const int* it,
                                         int lenK, int segBeg, int segLen, int slot, Meter<kC>& mt) {
     const int h = it[P.memoH];
     const int dDom = 1 - P.memoD2;
@@ -286,14 +290,15 @@ __device__ __noinline__ int memo_exists(const DevPlan& P, const DevIndex& ix, co
 // whole hub row (returns the hub index); 2: an item at the memo level whose
 // segment is a memoised hub row with at most one bound value among its
 // neighbours (returns the memo slot); 3: a kExist leaf item decided by the
-// existence memo (returns -3, its found bit set).  -1: enumerate as usual.
+// existence memo (returns -3, its found bit set; -4 when the bit is new and
+// the task counts on insertion).  -1: enumerate as usual.
 template <bool kC>
-__device__ __noinline__ int classify_item(const DevPlan& P, const DevIndex& ix, const DevStep& stp, const int* it,
+__device__ __noinline__ int classify_item(const DevPlan& P, const DevIndex& ix, const DevStep stp, const int* it,
                                           int lenK, int kind, int segBeg, int segLen, uint32_t* fb, bool heavy,
-                                          unsigned long long* myNew, Meter<kC>* mt) {
+                                          Meter<kC>& mt) {
     const int row = __ldg(ix.predRow[stp.dir] + stp.pred) + __ldg(ix.srcRank[stp.dir] + segBeg);
     const int h = __ldg(ix.hubOf[stp.dir] + row);
-    mt->add(12);
+    mt.add(12);
     if (h < 0 || __ldg(ix.rowBeg[stp.dir] + row) != segBeg || __ldg(ix.rowBeg[stp.dir] + row + 1) - segBeg != segLen)
         return -1;
     if (kind == 1) return h;
@@ -304,16 +309,19 @@ __device__ __noinline__ int classify_item(const DevPlan& P, const DevIndex& ix, 
         // memo must not count; one is corrected exactly, more enumerate
         int nR = 0;
         for (int q = kTupleHead; q < lenK && nR < 2; ++q)
-            nR += seg_has(ix.val[stp.dir], segBeg, segLen, it[q], *mt) ? 1 : 0;
+            nR += seg_has(ix.val[stp.dir], segBeg, segLen, it[q], mt) ? 1 : 0;
         return nR <= 1 ? slot : -1;
     }
-    const int res = memo_exists(P, ix, stp, it, lenK, segBeg, segLen, slot, *mt);
+    const int res = memo_exists(P, ix, stp, it, lenK, segBeg, segLen, slot, mt);
     if (res < 0) return -1;
     if (res == 1) {
         const int root = it[0];
         const uint32_t mask = 1u << (root & 31);
         const uint32_t old = atomicOr(&fb[root >> 5], mask);
-        if (heavy) { mt->add(8); *myNew += (old & mask) ? 0ull : 1ull; }
+        if (heavy) {
+            mt.add(8);
+            if (!(old & mask)) return -4;
+        }
     }
     return -3;
 }
@@ -471,8 +479,11 @@ __device__ __forceinline__ void run_task(Smem<B>& sm, const DevIndex& ix, const 
                     myLen = it[lenK + 1];
                     const int pathKind = hubPath ? 1 : (memoPath ? 2 : (existMemo ? 3 : 0));
                     if (pathKind && myLen > 0 && !(tid == 0 && S.curOff[k] != 0)) {
-                        const int code = classify_item(P, ix, stp, it, lenK, pathKind, myBeg, (int)myLen, fb, heavy,
-                                                       &myNew, &mt);
+                        int code = classify_item(P, ix, stp, it, lenK, pathKind, myBeg, (int)myLen, fb, heavy, mt);
+                        if (code == -4) {
+                            myNew += 1;          // a new found bit of a split root
+                            code = -3;
+                        }
                         if (code >= 0) {
                             isHub = true;
                             myBeg = -2 - code;   // marks the item for the hub or memo pass; no candidates
@@ -628,9 +639,9 @@ __device__ __forceinline__ void run_task(Smem<B>& sm, const DevIndex& ix, const 
                         if (perWarp && mine % kWarps != warp) continue;
                         const int* par = baseK + (w0 + item) * strideK;
                         if (!leaf) {
-                            memo_item(P, ix, stp, P.steps[k + 1], par, lenK, -2 - sm.wBeg[item],
-                                      bm + (rowBase + par[0]) * (long long)words, words, S.exRank[warp], lane,
-                                      myNew, mt, shared);
+                            myNew += memo_item(P, ix, stp, P.steps[k + 1], par, lenK, -2 - sm.wBeg[item],
+                                               bm + (rowBase + par[0]) * (long long)words, words, S.exRank[warp],
+                                               lane, mt, shared);
                             continue;
                         }
                         // hO must differ from every bound value: their ranks in hO's domain
@@ -708,7 +719,7 @@ __device__ __forceinline__ unsigned long long global_ns() {
 // the algorithmic bytes.
 template <int B, int kI>
 __global__ void __launch_bounds__(B, 1024 / B)
-engine_kernel(DevIndex ix, const DevPlan* __restrict__ plans, const DevTask* __restrict__ tasks,
+engine_kernel(const __grid_constant__ DevIndex ix, const DevPlan* __restrict__ plans, const DevTask* __restrict__ tasks,
               int nTasks, int* taskCounter, unsigned long long* results, int* status, EngineProfile prof) {
     constexpr bool kC = kI == 2;
     extern __shared__ __align__(16) unsigned char smem_raw[];
