@@ -386,6 +386,7 @@ void prepare(Batch& b, Context& c, const char* const* rules, int n, int isJson, 
     b.owner.clear();
     b.shared.clear();
     std::unordered_multimap<uint64_t, int> seen;
+    seen.reserve(2 * (size_t)n);
     if (b.exec) { cudaGraphExecDestroy(b.exec); b.exec = nullptr; }
     if (b.graph) { cudaGraphDestroy(b.graph); b.graph = nullptr; }
     b.rps.assign(n, RulePlan{});
@@ -393,12 +394,18 @@ void prepare(Batch& b, Context& c, const char* const* rules, int n, int isJson, 
     std::vector<DevPlan> plans;
     std::vector<const PhasePlan*> phases;
     plans.reserve(2 * (size_t)n);
-    // parsing and planning only read the graph and the dictionaries: in parallel
+    std::vector<uint64_t> hash(2 * (size_t)n, 0);   // per rule: support and body phase hashes
+    // parsing, planning and hashing only read the graph and the
+    // dictionaries: in parallel
     parallel_for((size_t)n, [&](size_t i) {
         if (!rules[i]) { b.parseStatus[i] = -1; return; }
         try {
             Rule r = isJson ? c.parser->parse_json(rules[i]) : c.parser->parse_text(rules[i]);
             b.rps[i] = plan_rule(r, c.hix, c.geom);
+            if (b.rps[i].status == kRuleOk) {
+                if (b.rps[i].support.how == kDevice) hash[2 * i] = phase_hash(b.rps[i].support);
+                if (b.rps[i].body.how == kDevice) hash[2 * i + 1] = phase_hash(b.rps[i].body);
+            }
         } catch (const RuleError&) {
             b.parseStatus[i] = -1;
         }
@@ -414,15 +421,16 @@ void prepare(Batch& b, Context& c, const char* const* rules, int n, int isJson, 
             // several heads) run once; the others share the count
             // keyed by hash, confirmed by the full signature (plans are
             // zero-initialised, so equal signatures mean equal computations)
-            auto range = seen.equal_range(phase_hash(ph));
+            const uint64_t h = hash[2 * (size_t)i + k];
+            auto range = seen.equal_range(h);
             int same = -1;
             for (auto it = range.first; it != range.second && same < 0; ++it)
-                if (phase_signature(*phases[it->second]) == phase_signature(ph)) same = it->second;
+                if (phase_equal(*phases[it->second], ph)) same = it->second;
             if (same >= 0) {
                 b.shared.emplace_back(2 * i + k, same);
                 continue;
             }
-            seen.emplace(phase_hash(ph), (int)plans.size());
+            seen.emplace(h, (int)plans.size());
             plans.push_back(ph.plan);
             phases.push_back(&ph);
             b.owner.push_back(2 * i + k);

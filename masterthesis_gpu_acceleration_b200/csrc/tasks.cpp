@@ -47,6 +47,12 @@ std::string phase_signature(const PhasePlan& ph) {
     return s;
 }
 
+bool phase_equal(const PhasePlan& a, const PhasePlan& b) {
+    if (a.rootBeg != b.rootBeg || a.rootEnd != b.rootEnd) return false;
+    const DevPlan pa = plan_identity(a), pb = plan_identity(b);
+    return std::memcmp(&pa, &pb, sizeof(DevPlan)) == 0;
+}
+
 uint64_t phase_hash(const PhasePlan& ph) {
     static_assert(sizeof(DevPlan) % 8 == 0, "plan hashed in 8-byte words");
     const DevPlan p = plan_identity(ph);
@@ -209,6 +215,15 @@ double TaskBuilder::child_work(const DevPlan& P, const int32_t* vals, int32_t e,
 const TaskBuilder::Walk& TaskBuilder::walk(const PhasePlan& ph, uint64_t sig) {
     auto it = walks_.find(sig);
     if (it != walks_.end()) return it->second;
+    return keep_walk(sig, compute_walk(ph));
+}
+
+const TaskBuilder::Walk& TaskBuilder::keep_walk(uint64_t sig, Walk&& wk) {
+    cacheBytes_ += wk.w.size() * sizeof(float) + wk.bsum.size() * (sizeof(double) + sizeof(float)) + sizeof(Walk);
+    return walks_.emplace(sig, std::move(wk)).first->second;
+}
+
+TaskBuilder::Walk TaskBuilder::compute_walk(const PhasePlan& ph) {
     const DevPlan& P = ph.plan;
     double tail = 1.0;
     for (int s = 2; s < P.m; ++s) tail *= std::max(1.0, avg_fan(P.steps[s]));
@@ -255,9 +270,8 @@ const TaskBuilder::Walk& TaskBuilder::walk(const PhasePlan& ph, uint64_t sig) {
             entry.bsum[b] += w[k];
             entry.bmax[b] = std::max(entry.bmax[b], w[k]);
         }
-    cacheBytes_ += w.size() * sizeof(float) + nb * (sizeof(double) + sizeof(float)) + sizeof(Walk);
     entry.w = std::move(w);
-    return walks_.emplace(sig, std::move(entry)).first->second;
+    return entry;
 }
 
 void TaskBuilder::build(const std::vector<const PhasePlan*>& phases, int blocks, bool split,
@@ -294,6 +308,8 @@ void TaskBuilder::build(const std::vector<const PhasePlan*>& phases, int blocks,
             return estHub[a] > estHub[b];
         });
         double used = 0;
+        std::vector<size_t> sel;          // phases that get a walk
+        std::vector<uint64_t> sig(n, 0);
         for (size_t i : ord) {
             if (!forced[i] && estHub[i] < walkThreshold) break;
             const PhasePlan& ph = *phases[i];
@@ -303,14 +319,30 @@ void TaskBuilder::build(const std::vector<const PhasePlan*>& phases, int blocks,
             double edges = chain_shaped(ph.plan) ? (double)(ph.rootEnd - ph.rootBeg)
                          : (double)(ph.rootEnd - ph.rootBeg) *
                            (s0.kind == kExpand ? std::max(1.0, ix_.avg_degree(s0.pred, s0.dir)) : (double)ix_.pred_size(s0.pred));
-            const uint64_t sig = signature(ph);
-            const bool cached = walks_.count(sig) != 0;
+            sig[i] = signature(ph);
+            const bool cached = walks_.count(sig[i]) != 0;
             if (!forced[i] && !cached && used + edges > walkBudget) continue;
             // a walk whose own cost exceeds the phase's expected device time
             // cannot pay for itself (a single rule on the whole GPU)
             if (costAware && !cached && estAvg[i] * scale[i] < kWalkNsPerEdge * edges) continue;
             if (!cached) used += edges;   // cached walks cost nothing
-            const Walk& wk = walk(ph, sig);
+            sel.push_back(i);
+        }
+        // the new walks, one per distinct signature, on host threads (a walk
+        // only reads the index and the shared estimate caches)
+        std::vector<size_t> fresh;
+        {
+            std::unordered_map<uint64_t, char> pending;
+            for (size_t i : sel)
+                if (!walks_.count(sig[i]) && pending.emplace(sig[i], 1).second) fresh.push_back(i);
+        }
+        std::vector<Walk> made(fresh.size());
+        // threads only pay for themselves on large walks (~0.1 ms and up)
+        parallel_for(fresh.size(), [&](size_t k) { made[k] = compute_walk(*phases[fresh[k]]); },
+                     used > 1.0e5 ? 1 : fresh.size() + 1);
+        for (size_t k = 0; k < fresh.size(); ++k) keep_walk(sig[fresh[k]], std::move(made[k]));
+        for (size_t i : sel) {
+            const Walk& wk = walks_.find(sig[i])->second;
             walked[i] = &wk;
             out[i].work = wk.sum;
         }

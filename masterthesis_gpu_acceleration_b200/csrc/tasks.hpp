@@ -39,6 +39,8 @@ constexpr double kWalkNsPerEdge = 8.0;
 // per-launch fields, and its root range.  Phases with equal signatures
 // produce equal counts.
 std::string phase_signature(const PhasePlan& ph);
+// Whether two phases have equal signatures (without building them).
+bool phase_equal(const PhasePlan& a, const PhasePlan& b);
 // 64-bit hash of phase_signature (keys of the task builder's caches).
 uint64_t phase_hash(const PhasePlan& ph);
 
@@ -133,6 +135,10 @@ private:
     // the average-fan-out estimate.
     double estimate2(const PhasePlan& ph);
     const Walk& walk(const PhasePlan& ph, uint64_t sig);
+    // The per-root walk of a phase (thread-safe: reads the index and the
+    // lock-guarded estimate caches), and its insertion into the cache.
+    Walk compute_walk(const PhasePlan& ph);
+    const Walk& keep_walk(uint64_t sig, Walk&& wk);
     const Walk& walk(const PhasePlan& ph) { return walk(ph, phase_hash(ph)); }
     double child_work(const DevPlan& P, const int32_t* rootVals, int32_t e, const int32_t* deg2, double tail) const;
     int root_vals(const DevPlan& P, int32_t r, int32_t* vals) const;
