@@ -34,6 +34,13 @@ __host__ __device__ inline uint32_t slot_hash(uint32_t tag, uint32_t key) {
     return (uint32_t)x;
 }
 
+// Bit of (pred, dir) in an entity's row signature: the signature of an
+// entity has the bits of every (pred, dir) under which it keys a row, so a
+// clear bit proves that the row is absent (a set bit may be a collision).
+__host__ __device__ inline int sig_bit(int32_t pred, int dir) {
+    return (int)(((uint32_t)pred * 2u + (uint32_t)dir) * 0x9E3779B1u >> 26);
+}
+
 // Device-resident graph index.  Triples are stored once per direction:
 // dir 0 (SPO) keys edges by subject and stores objects as values, dir 1
 // (POS) keys them by object and stores subjects.  Within a direction edges
@@ -58,6 +65,8 @@ struct DevIndex {
     const int32_t* hubOf[2];     // per row: hub index or -1
     const int64_t* hubOff;       // per hub: first word in hubBits
     const uint32_t* hubBits;
+    // per direction, per edge: the row signature of the edge's value
+    const uint64_t* valSig[2];
     int32_t nHub;
     uint32_t hashMask;
     int32_t nPred;

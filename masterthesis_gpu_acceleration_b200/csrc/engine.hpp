@@ -237,6 +237,8 @@ struct Context {
         add(h.hubOf[1].data(), h.hubOf[1].size() * 4);
         add(h.hubOff.data(), h.hubOff.size() * 8);
         add(h.hubBits.data(), h.hubBits.size() * 4);
+        add(h.valSig[0].data(), h.valSig[0].size() * 8);
+        add(h.valSig[1].data(), h.valSig[1].size() * 8);
         size_t total = 0;
         std::vector<size_t> off;
         for (auto& pp : parts) {
@@ -269,6 +271,8 @@ struct Context {
         dix.hubOf[1] = reinterpret_cast<const int32_t*>(base + off[k++]);
         dix.hubOff = reinterpret_cast<const int64_t*>(base + off[k++]);
         dix.hubBits = reinterpret_cast<const uint32_t*>(base + off[k++]);
+        dix.valSig[0] = reinterpret_cast<const uint64_t*>(base + off[k++]);
+        dix.valSig[1] = reinterpret_cast<const uint64_t*>(base + off[k++]);
         dix.nHub = (int32_t)h.hubOff.size();
         dix.hashMask = h.hashMask;
         dix.nPred = h.nPred;

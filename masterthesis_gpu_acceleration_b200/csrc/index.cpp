@@ -187,6 +187,22 @@ HostIndex build_index(const std::vector<int32_t>& spo, int32_t nEnt, int32_t nPr
             }
         }, 1);
     }
+    // row signatures: per entity, then copied beside every edge's value
+    std::vector<uint64_t> entSig((size_t)std::max(nEnt, 1), 0);
+    for (int d = 0; d < 2; ++d)
+        parallel_for((size_t)nPred, [&](size_t p) {
+            const uint64_t bit = 1ull << sig_bit((int32_t)p, d);
+            for (int32_t r = ix.predRow[d][p]; r < ix.predRow[d][p + 1]; ++r)
+                __atomic_fetch_or(&entSig[(size_t)ix.rowKey[d][r]], bit, __ATOMIC_RELAXED);
+        }, 1);
+    for (int d = 0; d < 2; ++d) {
+        const size_t nE = ix.val[d].size();
+        ix.valSig[d].resize(nE);
+        parallel_for((nE + 65535) / 65536, [&](size_t c) {
+            const size_t e1 = std::min(nE, (c + 1) * 65536);
+            for (size_t e = c * 65536; e < e1; ++e) ix.valSig[d][e] = entSig[(size_t)ix.val[d][e]];
+        }, 1);
+    }
     build_hubs(ix, hubMinDegree);
     return ix;
 }

@@ -23,6 +23,10 @@ struct HostIndex {
     std::vector<int32_t> hubOf[2];
     std::vector<int64_t> hubOff;
     std::vector<uint32_t> hubBits;
+    // Per direction, per edge: the row signature (sig_bit) of the edge's
+    // value, read beside the value so that an expansion can drop a
+    // candidate whose next row does not exist without looking it up.
+    std::vector<uint64_t> valSig[2];
 
     int64_t pred_size(int32_t p) const {
         return (p < 0 || p >= nPred) ? 0 : predEdge[0][p + 1] - predEdge[0][p];

@@ -573,9 +573,17 @@ __device__ __forceinline__ void run_task(Smem<B>& sm, const DevIndex& ix, const 
             const int* rbase = stp.kind == kExpand ? ix.valRank[stp.dir]
                                                    : (stp.hoWhich == 1 ? ix.srcRank[0] : ix.valRank[0]);
             const bool wantRank = pairs && stp.hoWhich;
+            // When the next step expands from the value this step binds,
+            // that value's row signature (stored beside it) drops most
+            // candidates whose next row is absent before any lookup.
+            const bool sigTest = !leaf && stp.kind == kExpand && P.steps[k + 1].kind == kExpand &&
+                                 P.steps[k + 1].keyRef == lenK;
+            const int sigBit = sig_bit(P.steps[k + 1 < P.m ? k + 1 : k].pred, P.steps[k + 1 < P.m ? k + 1 : k].dir);
+            const uint32_t* sigWords = reinterpret_cast<const uint32_t*>(ix.valSig[stp.dir]) + (sigBit >> 5);
             int hint = 0;
             for (long long jb = tid; jb < take; jb += (long long)B * kU) {
                 int lo_[kU], e_[kU], n0_[kU], n1_[kU], rk_[kU];
+                uint32_t sw_[kU];
 #pragma unroll
                 for (int u = 0; u < kU; ++u) {
                     const long long j = jb + (long long)u * B;
@@ -602,14 +610,16 @@ __device__ __forceinline__ void run_task(Smem<B>& sm, const DevIndex& ix, const 
 #pragma unroll
                 for (int u = 0; u < kU; ++u) {
                     n0_[u] = n1_[u] = rk_[u] = 0;
+                    sw_[u] = ~0u;
                     if (lo_[u] < 0) continue;
+                    if (sigTest) { sw_[u] = __ldg(sigWords + 2 * (long long)e_[u]); mt.add(4); }
                     n0_[u] = __ldg(vbase + e_[u]);
                     if (stp.kind == kScan) { n1_[u] = __ldg(ix.val[0] + e_[u]); mt.add(8); } else mt.add(4);
                     if (wantRank) { rk_[u] = __ldg(rbase + e_[u]); mt.add(4); }
                 }
 #pragma unroll
                 for (int u = 0; u < kU; ++u)
-                    if (lo_[u] >= 0) eval(lo_[u], e_[u], n0_[u], n1_[u], rk_[u]);
+                    if (lo_[u] >= 0 && ((sw_[u] >> (sigBit & 31)) & 1u)) eval(lo_[u], e_[u], n0_[u], n1_[u], rk_[u]);
             }
             if (anyHub) {
                 // hub items of the consumed part of the window: [0, cut)
