@@ -65,8 +65,10 @@ struct DevIndex {
     const int32_t* hubOf[2];     // per row: hub index or -1
     const int64_t* hubOff;       // per hub: first word in hubBits
     const uint32_t* hubBits;
-    // per direction, per edge: the row signature of the edge's value
+    // per direction, per edge: the row signature of the edge's value, and
+    // the union of those signatures from the edge to the end of its row
     const uint64_t* valSig[2];
+    const uint64_t* sufSig[2];
     int32_t nHub;
     uint32_t hashMask;
     int32_t nPred;

@@ -239,6 +239,8 @@ struct Context {
         add(h.hubBits.data(), h.hubBits.size() * 4);
         add(h.valSig[0].data(), h.valSig[0].size() * 8);
         add(h.valSig[1].data(), h.valSig[1].size() * 8);
+        add(h.sufSig[0].data(), h.sufSig[0].size() * 8);
+        add(h.sufSig[1].data(), h.sufSig[1].size() * 8);
         size_t total = 0;
         std::vector<size_t> off;
         for (auto& pp : parts) {
@@ -273,6 +275,8 @@ struct Context {
         dix.hubBits = reinterpret_cast<const uint32_t*>(base + off[k++]);
         dix.valSig[0] = reinterpret_cast<const uint64_t*>(base + off[k++]);
         dix.valSig[1] = reinterpret_cast<const uint64_t*>(base + off[k++]);
+        dix.sufSig[0] = reinterpret_cast<const uint64_t*>(base + off[k++]);
+        dix.sufSig[1] = reinterpret_cast<const uint64_t*>(base + off[k++]);
         dix.nHub = (int32_t)h.hubOff.size();
         dix.hashMask = h.hashMask;
         dix.nPred = h.nPred;

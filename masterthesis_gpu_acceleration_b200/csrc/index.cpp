@@ -202,6 +202,14 @@ HostIndex build_index(const std::vector<int32_t>& spo, int32_t nEnt, int32_t nPr
             const size_t e1 = std::min(nE, (c + 1) * 65536);
             for (size_t e = c * 65536; e < e1; ++e) ix.valSig[d][e] = entSig[(size_t)ix.val[d][e]];
         }, 1);
+        ix.sufSig[d].resize(nE);
+        parallel_for((size_t)nPred, [&](size_t p) {
+            for (int32_t r = ix.predRow[d][p]; r < ix.predRow[d][p + 1]; ++r) {
+                uint64_t acc = 0;
+                for (int32_t e = ix.rowBeg[d][r + 1] - 1; e >= ix.rowBeg[d][r]; --e)
+                    ix.sufSig[d][(size_t)e] = acc |= ix.valSig[d][(size_t)e];
+            }
+        }, 1);
     }
     build_hubs(ix, hubMinDegree);
     return ix;

@@ -27,6 +27,10 @@ struct HostIndex {
     // value, read beside the value so that an expansion can drop a
     // candidate whose next row does not exist without looking it up.
     std::vector<uint64_t> valSig[2];
+    // Per direction, per edge: the union of valSig from the edge to the end
+    // of its row, so that an item whose whole segment cannot continue is
+    // never stored.
+    std::vector<uint64_t> sufSig[2];
 
     int64_t pred_size(int32_t p) const {
         return (p < 0 || p >= nPred) ? 0 : predEdge[0][p + 1] - predEdge[0][p];

@@ -512,6 +512,14 @@ __device__ __forceinline__ void run_task(Smem<B>& sm, const DevIndex& ix, const 
             const int strideN = lenN + 2;
             int* baseN = leaf ? nullptr : items + S.levelOff[k + 1];
 
+            // A new item of level k + 1 whose segment holds no value with a
+            // row under step k + 2 (keyed on that value) is not stored.
+            const bool lookTest = k + 2 < P.m && P.steps[k + 1].kind == kExpand && P.steps[k + 2].kind == kExpand &&
+                                  P.steps[k + 2].keyRef == P.tupleLen[k + 1];
+            const int lookBit = lookTest ? sig_bit(P.steps[k + 2].pred, P.steps[k + 2].dir) : 0;
+            const uint32_t* lookWords =
+                reinterpret_cast<const uint32_t*>(ix.sufSig[lookTest ? P.steps[k + 1].dir : 0]) + (lookBit >> 5);
+
             // One candidate: its parent item `lo`, edge `e`, new value(s)
             // n0/n1 and (when this step binds hO) the loaded rank.
             auto eval = [&](int lo, int e, int n0, int n1, int rankLoaded) {
@@ -553,6 +561,10 @@ __device__ __forceinline__ void run_task(Smem<B>& sm, const DevIndex& ix, const 
                 } else {
                     const int2 seg = step_segment(P, ix, k + 1, mt, valN);
                     if (seg.y <= seg.x) return;
+                    if (lookTest) {
+                        mt.add(4);
+                        if (!((__ldg(lookWords + 2 * (long long)seg.x) >> (lookBit & 31)) & 1u)) return;
+                    }
                     const int slot = atomicAdd(&S.count[k + 1], 1);
                     if (slot >= P.cap) { atomicOr(status, 8); return; }
                     int* dst = baseN + slot * strideN;
