@@ -371,6 +371,13 @@ __device__ __forceinline__ void run_task(Smem<B>& sm, const DevIndex& ix, const 
     {
         const int len0 = P.tupleLen[0];
         const int stride0 = P.m > 0 ? len0 + 2 : len0;
+        // as for deeper items: a root whose segment has no value able to
+        // take step 2 (keyed on that value) is not stored
+        const bool lookTest0 = P.m >= 2 && P.steps[0].kind == kExpand && P.steps[1].kind == kExpand &&
+                               P.steps[1].keyRef == len0;
+        const int lookBit0 = lookTest0 ? sig_bit(P.steps[1].pred, P.steps[1].dir) : 0;
+        const uint32_t* lookWords0 =
+            reinterpret_cast<const uint32_t*>(ix.sufSig[lookTest0 ? P.steps[0].dir : 0]) + (lookBit0 >> 5);
         for (int i = tid; i < G; i += B) {
             const int r = task.beg + i;
             int tv[kTupleHead + 2];
@@ -403,6 +410,10 @@ __device__ __forceinline__ void run_task(Smem<B>& sm, const DevIndex& ix, const 
                     seg.y = min(seg.y, b0 + task.sub1);
                 }
                 ok = seg.y > seg.x;
+                if (ok && lookTest0) {
+                    mt.add(4);
+                    ok = (__ldg(lookWords0 + 2 * (long long)seg.x) >> (lookBit0 & 31)) & 1u;
+                }
             }
             if (ok) {
                 const int slot = atomicAdd(&S.count[0], 1);
