@@ -2,7 +2,6 @@
 #include "rules.hpp"
 
 #include <cctype>
-#include <sstream>
 
 namespace gr {
 namespace {
@@ -12,6 +11,23 @@ std::string trim(const std::string& s) {
     while (b < e && std::isspace((unsigned char)s[b])) ++b;
     while (e > b && std::isspace((unsigned char)s[e - 1])) --e;
     return s.substr(b, e - b);
+}
+
+// The first three whitespace-separated tokens of s, as
+// `istringstream(s) >> a >> b >> c` reads them (RuleParser.cpp reads an atom
+// that way): leading whitespace skipped, missing tokens left empty, anything
+// after the third ignored.
+void three_tokens(const std::string& s, std::string& a, std::string& b, std::string& c) {
+    std::string* out[3] = {&a, &b, &c};
+    size_t i = 0;
+    const size_t n = s.size();
+    for (std::string* t : out) {
+        while (i < n && std::isspace((unsigned char)s[i])) ++i;
+        size_t j = i;
+        while (j < n && !std::isspace((unsigned char)s[j])) ++j;
+        t->assign(s, i, j - i);
+        i = j;
+    }
 }
 
 // Splits the body on '^' outside parentheses (RuleParser.cpp:155-184).
@@ -86,10 +102,10 @@ std::string RuleParser::expand(const std::string& token) const {
 Term RuleParser::var_term(const std::string& name, Scope& sc) const {
     Term t;
     t.isVar = true;
-    auto it = sc.vars.find(name);
-    if (it != sc.vars.end()) { t.id = it->second; return t; }
+    for (const auto& v : sc.vars)
+        if (v.first == name) { t.id = v.second; return t; }
     t.id = sc.nextVar++;
-    sc.vars.emplace(name, t.id);
+    sc.vars.emplace_back(name, t.id);
     return t;
 }
 
@@ -98,10 +114,10 @@ Term RuleParser::const_term(const std::string& spelled, Scope& sc) const {
     t.isVar = false;
     int32_t id = ents_.find(spelled);
     if (id >= 0) { t.id = id; return t; }
-    auto it = sc.unknown.find(spelled);
-    if (it != sc.unknown.end()) { t.id = it->second; return t; }
+    for (const auto& u : sc.unknown)
+        if (u.first == spelled) { t.id = u.second; return t; }
     t.id = -1 - (int32_t)sc.unknown.size();
-    sc.unknown.emplace(spelled, t.id);
+    sc.unknown.emplace_back(spelled, t.id);
     return t;
 }
 
@@ -130,10 +146,8 @@ Rule RuleParser::parse_text(const std::string& line) const {
     auto atom_of = [&](const std::string& raw, const char* what) {
         std::string s = trim(raw);
         if (s.empty() || s.front() != '(' || s.back() != ')') throw RuleError(std::string("Invalid ") + what + ": " + raw);
-        s = trim(s.substr(1, s.size() - 2));
-        std::istringstream iss(s);
         std::string st, pt, ot;
-        iss >> st >> pt >> ot;
+        three_tokens(s.substr(1, s.size() - 2), st, pt, ot);
         if (st.empty() || pt.empty() || ot.empty()) throw RuleError(std::string("Invalid ") + what + ": " + raw);
         Atom a;
         a.s = text_term(st, sc);

@@ -52,9 +52,10 @@ private:
     std::unordered_map<std::string, std::string> prefixes_;
 
     std::string expand(const std::string& token) const;
+    // Names seen in one rule: a handful, so searched linearly.
     struct Scope {
-        std::unordered_map<std::string, int32_t> vars;
-        std::unordered_map<std::string, int32_t> unknown;
+        std::vector<std::pair<std::string, int32_t>> vars;
+        std::vector<std::pair<std::string, int32_t>> unknown;
         int32_t nextVar = 0;
     };
     Term var_term(const std::string& name, Scope& sc) const;

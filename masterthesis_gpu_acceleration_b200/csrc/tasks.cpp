@@ -288,16 +288,21 @@ void TaskBuilder::build(const std::vector<const PhasePlan*>& phases, int blocks,
     std::vector<const Walk*> walked(n, nullptr);
     std::vector<char> forced(n, 0);
     const bool learned = !calib_.empty() || !mustWalk_.empty();
+    // signatures and cached-walk flags too: the walk cache only changes
+    // after this loop
+    std::vector<uint64_t> sig(n, 0);
+    std::vector<char> cached(n, 0);
     parallel_for(n, [&](size_t i) {
         estAvg[i] = estimate2(*phases[i]);
         estHub[i] = split ? estimate(*phases[i], true) : estAvg[i];
         out[i].work = estAvg[i];
+        if (learned || split) sig[i] = signature(*phases[i]);
         if (learned) {
-            const uint64_t sig = signature(*phases[i]);
-            auto c = calib_.find(sig);
+            auto c = calib_.find(sig[i]);
             if (c != calib_.end()) scale[i] = c->second;
-            forced[i] = mustWalk_.count(sig) ? 1 : 0;
+            forced[i] = mustWalk_.count(sig[i]) ? 1 : 0;
         }
+        if (split) cached[i] = walks_.count(sig[i]) ? 1 : 0;
     }, 128);
     if (split) {
         std::vector<size_t> ord(n);
@@ -309,7 +314,6 @@ void TaskBuilder::build(const std::vector<const PhasePlan*>& phases, int blocks,
         });
         double used = 0;
         std::vector<size_t> sel;          // phases that get a walk
-        std::vector<uint64_t> sig(n, 0);
         for (size_t i : ord) {
             if (!forced[i] && estHub[i] < walkThreshold) break;
             const PhasePlan& ph = *phases[i];
@@ -319,13 +323,11 @@ void TaskBuilder::build(const std::vector<const PhasePlan*>& phases, int blocks,
             double edges = chain_shaped(ph.plan) ? (double)(ph.rootEnd - ph.rootBeg)
                          : (double)(ph.rootEnd - ph.rootBeg) *
                            (s0.kind == kExpand ? std::max(1.0, ix_.avg_degree(s0.pred, s0.dir)) : (double)ix_.pred_size(s0.pred));
-            sig[i] = signature(ph);
-            const bool cached = walks_.count(sig[i]) != 0;
-            if (!forced[i] && !cached && used + edges > walkBudget) continue;
+            if (!forced[i] && !cached[i] && used + edges > walkBudget) continue;
             // a walk whose own cost exceeds the phase's expected device time
             // cannot pay for itself (a single rule on the whole GPU)
-            if (costAware && !cached && estAvg[i] * scale[i] < kWalkNsPerEdge * edges) continue;
-            if (!cached) used += edges;   // cached walks cost nothing
+            if (costAware && !cached[i] && estAvg[i] * scale[i] < kWalkNsPerEdge * edges) continue;
+            if (!cached[i]) used += edges;   // cached walks cost nothing
             sel.push_back(i);
         }
         // the new walks, one per distinct signature, on host threads (a walk

@@ -3,7 +3,11 @@
 //      in the same order, as one reader over the whole text;
 //   2. in the index built on several threads every row is found through the
 //      lookup table at its own edge range, every triple is found, and every
-//      value rank is the value's row in the other direction.
+//      value rank is the value's row in the other direction;
+//   3. row signatures have no false negatives: every edge's value signature
+//      holds the bit of every (pred, dir) under which the value keys a row,
+//      and every suffix signature is the union of the value signatures from
+//      its edge to the end of its row.
 // Usage: load_check FILE.ttl MIN_CHUNK_BYTES
 #include <cstdio>
 #include <cstdlib>
@@ -42,7 +46,27 @@ int main(int argc, char** argv) {
             }
     for (size_t i = 0; i + 2 < s2.size(); i += 3)
         if (!ix.has_triple(s2[i + 1], s2[i], s2[i + 2])) ++bad;
-    std::printf("triples %zu rows %zu hubs %zu mismatches %ld\n", s2.size() / 3,
-                ix.rowKey[0].size() + ix.rowKey[1].size(), ix.hubOff.size(), bad);
+    // the signature each entity must carry, rebuilt here row by row
+    std::vector<uint64_t> want((size_t)ix.nEnt, 0);
+    for (int d = 0; d < 2; ++d)
+        for (int32_t p = 0; p < ix.nPred; ++p)
+            for (int32_t r = ix.predRow[d][p]; r < ix.predRow[d][p + 1]; ++r)
+                want[(size_t)ix.rowKey[d][r]] |= 1ull << sig_bit(p, d);
+    long badSig = 0;
+    for (int d = 0; d < 2; ++d) {
+        if (ix.valSig[d].size() != ix.val[d].size() || ix.sufSig[d].size() != ix.val[d].size()) { ++badSig; continue; }
+        for (int32_t p = 0; p < ix.nPred; ++p)
+            for (int32_t r = ix.predRow[d][p]; r < ix.predRow[d][p + 1]; ++r) {
+                uint64_t acc = 0;
+                for (int32_t e = ix.rowBeg[d][r + 1] - 1; e >= ix.rowBeg[d][r]; --e) {
+                    if (ix.valSig[d][e] != want[(size_t)ix.val[d][e]]) ++badSig;
+                    acc |= ix.valSig[d][e];
+                    if (ix.sufSig[d][e] != acc) ++badSig;
+                }
+            }
+    }
+    bad += badSig;
+    std::printf("triples %zu rows %zu hubs %zu mismatches %ld (signatures %ld)\n", s2.size() / 3,
+                ix.rowKey[0].size() + ix.rowKey[1].size(), ix.hubOff.size(), bad, badSig);
     return bad == 0 ? 0 : 1;
 }
