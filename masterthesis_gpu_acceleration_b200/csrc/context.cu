@@ -251,10 +251,10 @@ void Staged::enqueue(Context& c, cudaStream_t s, int instr, int gridCap) {
 void Staged::enqueue_per_plan(Context& c, cudaStream_t s) {
     if (!nPlans) return;
     if (nPlans > kMaxPerPlan || (int)planTaskEnd.size() != nPlans) throw CudaError("bad per-plan staging");
-    // control words: [0..1] task counters, [2] status (int), then per plan
-    // two u64 span words at byte 16 + 16 * i; all start at zero
-    ck(cudaMemsetAsync(dResults.p, 0, (size_t)nPlans * sizeof(unsigned long long), s), "memset results");
-    ck(cudaMemsetAsync(dCtl.p, 0, 16 + 16 * kMaxPerPlan, s), "memset ctl");
+    // control words: [0..1] task counters, [2] status (int), per plan two
+    // u64 span words at byte 16 + 16 * i and its u64 result at
+    // kPerPlanResults + 8 * i; all start at zero
+    ck(cudaMemsetAsync(dCtl.p, 0, 64, s), "memset ctl");
     if (bitmapWords) ck(cudaMemsetAsync(dBitmap.p, 0, bitmapWords * 4, s), "memset bitmap");
     if (heavyWords) ck(cudaMemsetAsync(dHeavy.p, 0, heavyWords * 4, s), "memset heavy rows");
     int* ctl = static_cast<int*>(dCtl.p);
@@ -263,17 +263,16 @@ void Staged::enqueue_per_plan(Context& c, cudaStream_t s) {
         EngineProfile prof;
         prof.span = reinterpret_cast<unsigned long long*>(static_cast<char*>(dCtl.p) + 16 + 16 * i);
         const int grid = std::max(1, std::min(e - b, c.grid));
-        ck(engine_launch(c.dix, dPlans, dTasks + b, e - b, ctl + i, static_cast<unsigned long long*>(dResults.p),
-                         ctl + 2, grid, c.geom.block, s, &prof),
+        ck(engine_launch(c.dix, dPlans, dTasks + b, e - b, ctl + i,
+                         reinterpret_cast<unsigned long long*>(static_cast<char*>(dCtl.p) + kPerPlanResults), ctl + 2,
+                         grid, c.geom.block, s, &prof),
            "engine launch");
     }
 }
 
 void Staged::download_spans(cudaStream_t s) {
     if (!nPlans) return;
-    ck(cudaMemcpyAsync(hResults.p, dResults.p, nPlans * sizeof(unsigned long long), cudaMemcpyDeviceToHost, s),
-       "D2H results");
-    ck(cudaMemcpyAsync(hCtl.p, dCtl.p, 16 + 16 * kMaxPerPlan, cudaMemcpyDeviceToHost, s), "D2H status");
+    ck(cudaMemcpyAsync(hCtl.p, dCtl.p, 64, cudaMemcpyDeviceToHost, s), "D2H control words");
 }
 
 void compose(const RulePlan& rp, int64_t sup, int64_t body, double supMs, double confMs, GpuRuleResult* out) {
@@ -344,8 +343,8 @@ int evaluate_parsed(Context& c, const Rule& rule, GpuRuleResult* out) {
         if (static_cast<const int*>(c.one.hCtl.p)[2] != 0)
             throw CudaError("engine reported internal status " + std::to_string(static_cast<const int*>(c.one.hCtl.p)[2]));
         int k = 0;
-        if (runS) { sup = (int64_t)c.one.counts()[k]; supMs = (float)c.one.span_ms(k); ++k; }
-        if (runB) { body = (int64_t)c.one.counts()[k]; confMs = (float)c.one.span_ms(k); }
+        if (runS) { sup = (int64_t)c.one.per_plan_count(k); supMs = (float)c.one.span_ms(k); ++k; }
+        if (runB) { body = (int64_t)c.one.per_plan_count(k); confMs = (float)c.one.span_ms(k); }
     }
     compose(rp, sup, body, supMs, confMs, out);
     return 0;

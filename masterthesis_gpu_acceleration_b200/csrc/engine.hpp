@@ -121,12 +121,20 @@ struct Staged {
     // share of the SMs).
     void enqueue(Context& c, cudaStream_t s, int instr, int gridCap = 0);
     // One launch per plan of an unsorted staging (at most kMaxPerPlan plans),
-    // each with its own task counter and launch span in the control words;
-    // download_spans then brings results, status and spans back in two
-    // copies.  The plain per-rule form: support and body size of one rule.
+    // each with its own task counter, launch span and result in the 64
+    // control bytes (counters and status at 0, spans at 16, results at
+    // kPerPlanResults), cleared by one memset; download_spans brings them
+    // back in one copy.  The plain per-rule form: support and body size of
+    // one rule.
     static constexpr int kMaxPerPlan = 2;
+    static constexpr int kPerPlanResults = 16 + 16 * kMaxPerPlan;
+    static_assert(kPerPlanResults + 8 * kMaxPerPlan <= 64, "per-plan control words fit the 64 control bytes");
     void enqueue_per_plan(Context& c, cudaStream_t s);
     void download_spans(cudaStream_t s);
+    // Count of plan i after download_spans and a sync.
+    unsigned long long per_plan_count(int i) const {
+        return reinterpret_cast<const unsigned long long*>(static_cast<const char*>(hCtl.p) + kPerPlanResults)[i];
+    }
     // Device span (ms) of plan i's launch after download_spans and a sync.
     double span_ms(int i) const {
         const unsigned long long* w = static_cast<const unsigned long long*>(hCtl.p) + 2 + 2 * i;
