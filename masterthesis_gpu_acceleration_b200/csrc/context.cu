@@ -175,49 +175,76 @@ const SuffixMemo* Context::memo_for(int p1, int d1, int p2, int d2) const {
 void Context::ensure_memos(const std::vector<std::array<int, 4>>& keys, cudaStream_t s) {
     const HostIndex& h = hix;
     const int nHub = (int)h.hubOff.size();
-    std::vector<MemoJob> all;
+    std::vector<std::array<int, 4>> fresh;
     for (const auto& k : keys) {
         const int p1 = k[0], d1 = k[1], p2 = k[2], d2 = k[3];
         const uint64_t key = memo_key(p1, d1, p2, d2);
         if (memos.count(key)) continue;
         memos[key] = nullptr;
         if (memoGain < 0 || nHub == 0 || p1 < 0 || p2 < 0 || p1 >= h.nPred || p2 >= h.nPred) continue;
+        fresh.push_back(k);
+    }
+    if (fresh.empty()) return;
+    // the hub rows of (p1, d1) worth a memo, per new transition, on host
+    // threads: a row's suffix candidates are the second-step degrees of its
+    // values summed
+    std::vector<std::vector<int32_t>> rowsOf(fresh.size());
+    parallel_for(fresh.size(), [&](size_t i) {
+        const int p1 = fresh[i][0], d1 = fresh[i][1], p2 = fresh[i][2], d2 = fresh[i][3];
         const int words = (int)((h.pred_rows(p2, 1 - d2) + 31) / 32);
-        std::vector<int32_t> rows;
-        std::vector<int32_t> tab(nHub, -1);
+        const int32_t* deg = tasks->degrees(p2, d2);
         for (int32_t r = h.predRow[d1][p1]; r < h.predRow[d1][p1 + 1]; ++r) {
-            const int32_t hub = h.hubOf[d1][r];
-            if (hub < 0) continue;
-            double cand = 0;   // suffix candidates of this row: sum of the second-step degrees
-            for (int32_t e = h.rowBeg[d1][r]; e < h.rowBeg[d1][r + 1]; ++e) {
-                auto rr = h.row_range(p2, d2, h.val[d1][e]);
-                cand += rr.second - rr.first;
-            }
-            if (cand < memoGain * words) continue;
-            tab[hub] = (int32_t)rows.size();
-            rows.push_back(r);
+            if (h.hubOf[d1][r] < 0) continue;
+            double cand = 0;
+            for (int32_t e = h.rowBeg[d1][r]; e < h.rowBeg[d1][r + 1]; ++e) cand += deg[h.val[d1][e]];
+            if (cand >= memoGain * words) rowsOf[i].push_back(r);
         }
-        const size_t tabBytes = ((size_t)nHub * 4 + 255) & ~size_t(255);
-        const size_t bitBytes = rows.size() * 2 * (size_t)words * 4;
-        if (rows.empty() || memoBytes + bitBytes > kMemoBudgetBytes) continue;
+    }, 1);
+    // within the memory budget, in key order: one device allocation holding
+    // every new memo's hub table, then every new memo's bits
+    const size_t tabBytes = ((size_t)nHub * 4 + 255) & ~size_t(255);
+    std::vector<size_t> take, bitOff;
+    size_t bitTotal = 0;
+    for (size_t i = 0; i < fresh.size(); ++i) {
+        const int words = (int)((h.pred_rows(fresh[i][2], 1 - fresh[i][3]) + 31) / 32);
+        const size_t bytes = tabBytes + rowsOf[i].size() * 2 * (size_t)words * 4;
+        if (rowsOf[i].empty() || memoBytes + bytes > kMemoBudgetBytes) continue;
+        memoBytes += bytes;
+        take.push_back(i);
+        bitOff.push_back(bitTotal);
+        bitTotal += rowsOf[i].size() * 2 * (size_t)words * 4;
+    }
+    if (take.empty()) return;
+    const size_t tabTotal = tabBytes * take.size();
+    memoChunks.emplace_back(new DevBuf());
+    DevBuf& chunk = *memoChunks.back();
+    ck(cudaMalloc(&chunk.p, tabTotal + bitTotal), "cudaMalloc(memos)");   // exact: never resized
+    chunk.cap = tabTotal + bitTotal;
+    char* base = static_cast<char*>(chunk.p);
+    std::vector<int32_t> tabs(tabTotal / 4, -1);
+    std::vector<MemoJob> all;
+    for (size_t t = 0; t < take.size(); ++t) {
+        const size_t i = take[t];
+        const int p1 = fresh[i][0], d1 = fresh[i][1], p2 = fresh[i][2], d2 = fresh[i][3];
+        const int words = (int)((h.pred_rows(p2, 1 - d2) + 31) / 32);
+        int32_t* tab = tabs.data() + t * (tabBytes / 4);
+        uint32_t* bits = reinterpret_cast<uint32_t*>(base + tabTotal + bitOff[t]);
         auto m = std::make_unique<SuffixMemo>();
         m->rowHasMemo.assign((size_t)h.pred_rows(p1, d1), 0);
-        for (int32_t r : rows) m->rowHasMemo[(size_t)(r - h.predRow[d1][p1])] = 1;
-        m->buf.ensure(tabBytes + bitBytes);
-        char* base = static_cast<char*>(m->buf.p);
-        ck(cudaMemcpyAsync(base, tab.data(), (size_t)nHub * 4, cudaMemcpyHostToDevice, s), "H2D memo table");
-        ck(cudaMemsetAsync(base + tabBytes, 0, bitBytes, s), "clear memo bits");
-        m->tab = reinterpret_cast<const int32_t*>(base);
-        m->bits = reinterpret_cast<const uint32_t*>(base + tabBytes);
+        const std::vector<int32_t>& rows = rowsOf[i];
+        for (size_t j = 0; j < rows.size(); ++j) {
+            tab[h.hubOf[d1][rows[j]]] = (int32_t)j;
+            m->rowHasMemo[(size_t)(rows[j] - h.predRow[d1][p1])] = 1;
+            all.push_back(MemoJob{p1, d1, p2, d2, rows[j], words, bits + j * 2 * (size_t)words});
+        }
+        m->tab = reinterpret_cast<const int32_t*>(base + t * tabBytes);
+        m->bits = bits;
         m->words = words;
         m->slots = (int)rows.size();
-        for (size_t i = 0; i < rows.size(); ++i)
-            all.push_back(MemoJob{p1, d1, p2, d2, rows[i], words,
-                                  reinterpret_cast<uint32_t*>(base + tabBytes) + i * 2 * (size_t)words});
-        memoBytes += m->buf.cap;
-        memos[key] = std::move(m);
+        memos[memo_key(p1, d1, p2, d2)] = std::move(m);
     }
-    if (all.empty()) return;
+    ck(cudaMemcpyAsync(base, tabs.data(), tabTotal, cudaMemcpyHostToDevice, s), "H2D memo tables");
+    ck(cudaMemsetAsync(base + tabTotal, 0, bitTotal, s), "clear memo bits");
     memoJobs.ensure(all.size() * sizeof(MemoJob));
     ck(cudaMemcpyAsync(memoJobs.p, all.data(), all.size() * sizeof(MemoJob), cudaMemcpyHostToDevice, s),
        "H2D memo jobs");

@@ -173,8 +173,7 @@ struct Staged {
 // memo_item in kernels.cu).  Built once per context, never moved.
 constexpr size_t kMemoBudgetBytes = size_t(1) << 30;   // all suffix memos of a context
 
-struct SuffixMemo {
-    DevBuf buf;
+struct SuffixMemo {   // its table and bits live in one of Context::memoChunks
     const int32_t* tab = nullptr;
     const uint32_t* bits = nullptr;
     int words = 0;
@@ -201,6 +200,7 @@ struct Context {
     // least memoGain x the memo's words (negative: no memos)
     double memoGain = 0.25;
     std::unordered_map<uint64_t, std::unique_ptr<SuffixMemo>> memos;
+    std::vector<std::unique_ptr<DevBuf>> memoChunks;   // one allocation per ensure_memos call
     size_t memoBytes = 0;
     // Builds the memos of the transitions (p1, d1) -> (p2, d2) in `keys`
     // that do not exist yet: one kernel over all their hub rows, one

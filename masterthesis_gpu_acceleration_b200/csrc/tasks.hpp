@@ -60,6 +60,10 @@ public:
 
     size_t cache_bytes() const { return cacheBytes_; }
 
+    // Row length of every entity under (pred, dir), indexed by entity
+    // (cached; safe to call from several threads).
+    const int32_t* degrees(int32_t pred, int dir);
+
     // Estimated device time of a phase: learned ns per unit for plans seen
     // by learn(), otherwise the work estimate times the learned default
     // (1 ns per unit before any learning).
@@ -121,7 +125,6 @@ private:
     // so references handed out stay valid)
     mutable std::shared_mutex cacheMu_;
 
-    const int32_t* degrees(int32_t pred, int dir);
     double sb_fan(int32_t pred, int dir);
     double avg_fan(const DevStep& st) const;
     double estimate(const PhasePlan& ph, bool hubAware);
