@@ -330,7 +330,9 @@ template <int B, bool kC>
 __device__ __forceinline__ void run_task(Smem<B>& sm, const DevIndex& ix, const DevTask& task,
                                          unsigned long long* results, int* status, Meter<kC>& mt) {
     constexpr int kLeafChunk = 16 * B;
-    constexpr int kU = 4;
+    // candidates per thread per group (1, 2 and 4 measured on c3: 44.96,
+    // 45.22 and 46.92 ms per launch; 8 makes compilation impractical)
+    constexpr int kU = 1;
     const DevPlan& P = sm.plan;
     BlockState<B>& S = sm.st;
     const int tid = threadIdx.x;
@@ -591,7 +593,7 @@ __device__ __forceinline__ void run_task(Smem<B>& sm, const DevIndex& ix, const 
 
             // Candidates j = tid, tid + B, ... in groups of kU per thread: all
             // group members are located first, then their loads are issued
-            // together, then they are evaluated (memory-level parallelism).
+            // together, then they are evaluated.
             const int* vbase = stp.kind == kExpand ? ix.val[stp.dir] : ix.src[0];
             const int* rbase = stp.kind == kExpand ? ix.valRank[stp.dir]
                                                    : (stp.hoWhich == 1 ? ix.srcRank[0] : ix.valRank[0]);
