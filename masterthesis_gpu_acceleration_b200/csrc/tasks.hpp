@@ -144,6 +144,10 @@ private:
     const Walk& keep_walk(uint64_t sig, Walk&& wk);
     const Walk& walk(const PhasePlan& ph) { return walk(ph, phase_hash(ph)); }
     double child_work(const DevPlan& P, const int32_t* rootVals, int32_t e, const int32_t* deg2, double tail) const;
+
+public:
+    // The bound values of root r and the edge range of its first step: the
+    // range a split root's slices [sub0, sub1) partition.
     int root_vals(const DevPlan& P, int32_t r, int32_t* vals) const;
     std::pair<int32_t, int32_t> first_segment(const DevPlan& P, int32_t r, const int32_t* vals) const;
 };

@@ -1,0 +1,45 @@
+"""The task builder's output on CPU (tests/native/tasks_check.cpp, compiled
+here with g++): for every device phase of the fuzz, edge-case and
+synthetic rule sets, in batch, tiny-task and per-rule modes, the tasks cover
+every root exactly once, split roots' slices partition their first segment
+in order, plain tasks stay within the plan's group size and every split root
+has its own global row.  The engine's counts rely on all four."""
+import subprocess
+
+import pytest
+
+from conftest import ROOT, fuzz_names, load_fixture
+from masterthesis_gpu_acceleration_b200 import synth
+
+CSRC = ROOT / "masterthesis_gpu_acceleration_b200" / "csrc"
+
+
+@pytest.fixture(scope="module")
+def checker(tmp_path_factory):
+    out = tmp_path_factory.mktemp("native") / "tasks_check"
+    subprocess.run(["g++", "-O2", "-std=c++17", "-pthread", "-o", str(out),
+                    str(ROOT / "tests" / "native" / "tasks_check.cpp")] +
+                   [str(CSRC / f) for f in ("turtle.cpp", "index.cpp", "rules.cpp", "planner.cpp", "tasks.cpp")],
+                   check=True)
+    return out
+
+
+def _run(checker, ttl, rules):
+    r = subprocess.run([str(checker), str(ttl), str(rules)], capture_output=True, text=True, timeout=600)
+    assert r.returncode == 0, r.stdout + r.stderr
+
+
+def test_tasks_cover_roots_fixtures(checker, tmp_path):
+    for name in fuzz_names() + ["edge_cases.json"]:
+        fx = load_fixture(name)
+        ttl, rules = tmp_path / f"{name}.ttl", tmp_path / f"{name}.txt"
+        ttl.write_text(fx["ttl"])
+        texts = fx["rules"] if "rules" in fx else [c["rule"] for c in fx["cases"]]
+        rules.write_text("\n".join(texts) + "\n")
+        _run(checker, ttl, rules)
+
+
+@pytest.mark.parametrize("cfg", ["c2s", "c4s"])
+def test_tasks_cover_roots_synthetic(checker, data_dir, cfg):
+    d = synth.generate(cfg, data_dir / f"{cfg}_tasks", seed=0)
+    _run(checker, d / "graph.ttl", d / "rules.txt")
