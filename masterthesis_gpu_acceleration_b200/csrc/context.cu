@@ -627,8 +627,10 @@ int gpu_evaluate_rules_batch(void* ctx, const char* const* rules, int n, int isJ
         cudaSetDevice(c.device);
         // Pipelined: chunk k+1 is parsed, planned and staged on the host
         // while chunk k runs on the device (each chunk on its own stream).
+        // automatic: up to 8 chunks of at least 1,250 rules (c3, 10,000 rules:
+        // 2, 4, 8 and 16 chunks measured 149k, 164k, 169k and 160k rules/s)
         const int K = c.batchChunks > 0 ? std::max(1, std::min(c.batchChunks, std::max(n, 1)))
-                                        : std::max(1, std::min(4, (n + 2499) / 2500));
+                                        : std::max(1, std::min(8, (n + 1249) / 1250));
         while ((int)c.pipe.size() < K) c.pipe.push_back(new Batch());
         for (int k = 0; k < K; ++k) {
             const int lo = (int)((long long)n * k / K), hi = (int)((long long)n * (k + 1) / K);

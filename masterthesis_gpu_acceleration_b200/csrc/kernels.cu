@@ -144,7 +144,7 @@ __device__ __forceinline__ int2 step_segment(const DevPlan& P, const DevIndex& i
 // Inclusive block scan of one 64-bit value per thread.
 template <int B>
 __device__ __forceinline__ long long block_scan(long long x, BlockState<B>& st) {
-    constexpr int kWarps = B / 32;
+    static_assert(B / 32 <= 32, "one lane per warp total");
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
 #pragma unroll
     for (int d = 1; d < 32; d <<= 1) {
@@ -153,17 +153,12 @@ __device__ __forceinline__ long long block_scan(long long x, BlockState<B>& st) 
     }
     if (lane == 31) st.warpSum[warp] = x;
     __syncthreads();
-    if (warp == 0) {
-        long long w = lane < kWarps ? st.warpSum[lane] : 0;
+    // every warp adds up the totals of the warps before it itself (at most
+    // 16 values), which saves the second barrier of a two-level scan
+    long long w = lane < warp ? st.warpSum[lane] : 0;
 #pragma unroll
-        for (int d = 1; d < 32; d <<= 1) {
-            const long long y = __shfl_up_sync(0xffffffffu, w, d);
-            if (lane >= d) w += y;
-        }
-        if (lane < kWarps) st.warpSum[lane] = w;
-    }
-    __syncthreads();
-    return warp ? x + st.warpSum[warp - 1] : x;
+    for (int d = 16; d; d >>= 1) w += __shfl_xor_sync(0xffffffffu, w, d);
+    return x + w;
 }
 
 template <int B>
