@@ -225,6 +225,18 @@ int gpu_graph_stats(void* ctx, long long* entities, long long* predicates, long 
  * rule miner enumerates head and body predicates with it). */
 int gpu_graph_predicate(void* ctx, long long index, char* name, int capacity, long long* triples);
 
+/* Writes the loaded graph (dictionaries, rule prefixes and the whole host
+ * index) to one binary file; 0, or -1 with gpu_last_error() set.  No
+ * counterpart in the reference, which parses and indexes the Turtle file on
+ * every load (gpu_index.cuh:33-79). */
+int gpu_save_index(void* ctx, const char* path);
+
+/* Loads a graph from a file written by gpu_save_index, skipping the Turtle
+ * parse and the index build; otherwise like gpu_load_graph (NULL with
+ * gpu_last_error() set on failure, including a file of another format
+ * version or one whose sizes or offsets do not agree). */
+void* gpu_load_index(const char* path);
+
 /* Last error message of the calling thread ("" if none). */
 const char* gpu_last_error(void);
 

@@ -44,6 +44,8 @@ API_SYMBOLS = (
     "gpu_serve_stop",
     "gpu_graph_stats",
     "gpu_graph_predicate",
+    "gpu_save_index",
+    "gpu_load_index",
     "gpu_batch_counts",
     "gpu_evaluate_rule_shard",
     "gpu_last_error",
@@ -149,6 +151,10 @@ def load_library(path: os.PathLike | str | None = None) -> ctypes.CDLL:
     lib.gpu_graph_predicate.restype = ctypes.c_int
     lib.gpu_graph_predicate.argtypes = [ctypes.c_void_p, ctypes.c_longlong, ctypes.c_char_p, ctypes.c_int,
                                         ctypes.POINTER(ctypes.c_longlong)]
+    lib.gpu_save_index.restype = ctypes.c_int
+    lib.gpu_save_index.argtypes = [ctypes.c_void_p, ctypes.c_char_p]
+    lib.gpu_load_index.restype = ctypes.c_void_p
+    lib.gpu_load_index.argtypes = [ctypes.c_char_p]
     lib.gpu_graph_stats.restype = ctypes.c_int
     lib.gpu_graph_stats.argtypes = [ctypes.c_void_p] + [ctypes.POINTER(ctypes.c_longlong)] * 3
     lib.gpu_last_error.restype = ctypes.c_char_p
@@ -170,13 +176,22 @@ def query_vram() -> tuple[int, int]:
 class GpuRulesLib:
     """Graph resident on the GPU between calls (GPU_03/GpuRulesLib.scala:61-116)."""
 
-    def __init__(self, ttl_path: os.PathLike | str):
+    def __init__(self, ttl_path: os.PathLike | str | None = None, index_path: os.PathLike | str | None = None):
+        """Loads a Turtle file, or (index_path) a graph file written by
+        save_index, which skips parsing and indexing."""
+        if (ttl_path is None) == (index_path is None):
+            raise ValueError("give exactly one of ttl_path and index_path")
         self._lib = load_library()
         query_vram()
-        ctx = self._lib.gpu_load_graph(str(ttl_path).encode())
+        if index_path is not None:
+            ctx = self._lib.gpu_load_index(str(index_path).encode())
+            what, src = "gpu_load_index", index_path
+        else:
+            ctx = self._lib.gpu_load_graph(str(ttl_path).encode())
+            what, src = "gpu_load_graph", ttl_path
         if not ctx:
             err = self._lib.gpu_last_error().decode(errors="replace")
-            raise RuntimeError(f"gpu_load_graph failed for: {ttl_path} ({err})")
+            raise RuntimeError(f"{what} failed for: {src} ({err})")
         self._ctx = ctypes.c_void_p(ctx)
 
     # -- reference entry points -------------------------------------------------
@@ -240,6 +255,12 @@ class GpuRulesLib:
     def set_option(self, name: str, value: int) -> None:
         if self._lib.gpu_set_option(self._handle(), name.encode(), int(value)) != 0:
             raise ValueError(f"bad option {name}={value}")
+
+    def save_index(self, path: os.PathLike | str) -> None:
+        """Writes the loaded graph to one binary file (load it with
+        GpuRulesLib(index_path=...))."""
+        if self._lib.gpu_save_index(self._handle(), str(path).encode()) != 0:
+            raise RuntimeError(f"gpu_save_index failed: {self._lib.gpu_last_error().decode(errors='replace')}")
 
     def stats(self) -> dict:
         e, p, t = ctypes.c_longlong(), ctypes.c_longlong(), ctypes.c_longlong()

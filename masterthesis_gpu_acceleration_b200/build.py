@@ -23,9 +23,10 @@ LIB = PKG / "lib"
 NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 
-ENGINE_SOURCES = ["turtle.cpp", "rules.cpp", "index.cpp", "planner.cpp", "tasks.cpp", "kernels.cu", "context.cu", "serve.cu"]
-HEADERS = ["common.hpp", "turtle.hpp", "rules.hpp", "index.hpp", "planner.hpp", "tasks.hpp", "engine.hpp",
-           "parallel.hpp"]
+ENGINE_SOURCES = ["turtle.cpp", "rules.cpp", "index.cpp", "index_io.cpp", "planner.cpp", "tasks.cpp", "kernels.cu",
+                  "context.cu", "serve.cu"]
+HEADERS = ["common.hpp", "turtle.hpp", "rules.hpp", "index.hpp", "index_io.hpp", "planner.hpp", "tasks.hpp",
+           "engine.hpp", "parallel.hpp"]
 
 
 def _newer(target: Path, deps) -> bool:

@@ -24,6 +24,7 @@
 #include <vector>
 
 #include "engine.hpp"
+#include "index_io.hpp"
 #include "parallel.hpp"
 
 namespace gr {
@@ -525,6 +526,26 @@ Context* as_ctx(void* p) { return static_cast<Context*>(p); }
 
 using namespace gr;
 
+namespace {
+
+// The rest of a load, whichever source the index came from: the state built
+// on the index, and its upload.
+void finish_load(Context* c) {
+    c->tasks.reset(new TaskBuilder(c->hix));
+    c->tasks->memoRows = [c](int p1, int d1, int p2, int d2, double* cost) -> const std::vector<uint8_t>* {
+        const uint64_t key = ((uint64_t)(uint32_t)(p1 * 2 + d1) << 32) | (uint32_t)(p2 * 2 + d2);
+        auto it = c->memos.find(key);
+        if (it == c->memos.end() || !it->second) return nullptr;
+        *cost = it->second->words / 4.0 + 8.0;   // a memo word costs about a quarter of a candidate
+        return &it->second->rowHasMemo;
+    };
+    c->parser.reset(new RuleParser(c->ents, c->preds, c->prefixes));
+    c->init_device();
+    c->upload_index();
+}
+
+}  // namespace
+
 extern "C" {
 
 const char* gpu_last_error(void) { return g_lastError.c_str(); }
@@ -563,17 +584,7 @@ void* gpu_load_graph(const char* ttlPath) {
         int32_t hubMin = kHubMinDegree;
         if (const char* h = std::getenv("GPU_RULES_HUB_MIN_DEGREE")) hubMin = std::max(0, std::atoi(h));
         c->hix = build_index(spo, (int32_t)c->ents.size(), (int32_t)c->preds.size(), hubMin);
-        c->tasks.reset(new TaskBuilder(c->hix));
-        c->tasks->memoRows = [c](int p1, int d1, int p2, int d2, double* cost) -> const std::vector<uint8_t>* {
-            const uint64_t key = ((uint64_t)(uint32_t)(p1 * 2 + d1) << 32) | (uint32_t)(p2 * 2 + d2);
-            auto it = c->memos.find(key);
-            if (it == c->memos.end() || !it->second) return nullptr;
-            *cost = it->second->words / 4.0 + 8.0;   // a memo word costs about a quarter of a candidate
-            return &it->second->rowHasMemo;
-        };
-        c->parser.reset(new RuleParser(c->ents, c->preds, c->prefixes));
-        c->init_device();
-        c->upload_index();
+        finish_load(c);
         return c;
     } catch (const std::exception& e) {
         set_error(std::string("gpu_load_graph error: ") + e.what());
@@ -581,6 +592,39 @@ void* gpu_load_graph(const char* ttlPath) {
         delete c;
         return nullptr;
     }
+}
+
+void* gpu_load_index(const char* path) {
+    if (!path) { set_error("gpu_load_index: null path"); return nullptr; }
+    Context* c = nullptr;
+    try {
+        c = new Context();
+        std::string err;
+        if (!load_graph_file(path, c->ents, c->preds, c->prefixes, c->hix, &err)) {
+            set_error(err);
+            delete c;
+            return nullptr;
+        }
+        if (const char* g = std::getenv("GPU_RULES_MEMO_GAIN")) c->memoGain = std::atof(g);
+        finish_load(c);
+        return c;
+    } catch (const std::exception& e) {
+        set_error(std::string("gpu_load_index error: ") + e.what());
+        cudaGetLastError();
+        delete c;
+        return nullptr;
+    }
+}
+
+int gpu_save_index(void* ctx, const char* path) {
+    if (!ctx || !path) return -1;
+    Context& c = *as_ctx(ctx);
+    std::string err;
+    if (!save_graph_file(path, c.ents, c.preds, c.prefixes, c.hix, &err)) {
+        set_error(err);
+        return -1;
+    }
+    return 0;
 }
 
 void gpu_free_graph(void* ctx) {

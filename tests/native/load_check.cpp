@@ -7,14 +7,18 @@
 //   3. row signatures have no false negatives: every edge's value signature
 //      holds the bit of every (pred, dir) under which the value keys a row,
 //      and every suffix signature is the union of the value signatures from
-//      its edge to the end of its row.
-// Usage: load_check FILE.ttl MIN_CHUNK_BYTES
+//      its edge to the end of its row;
+//   4. the graph written to a binary file reads back identical, and a
+//      truncated copy of the file is refused.
+// Usage: load_check FILE.ttl MIN_CHUNK_BYTES [SCRATCH_FILE]
 #include <cstdio>
 #include <cstdlib>
+#include <cstring>
 #include <string>
 #include <vector>
 
 #include "../../masterthesis_gpu_acceleration_b200/csrc/index.hpp"
+#include "../../masterthesis_gpu_acceleration_b200/csrc/index_io.hpp"
 #include "../../masterthesis_gpu_acceleration_b200/csrc/turtle.hpp"
 
 using namespace gr;
@@ -66,7 +70,45 @@ int main(int argc, char** argv) {
             }
     }
     bad += badSig;
-    std::printf("triples %zu rows %zu hubs %zu mismatches %ld (signatures %ld)\n", s2.size() / 3,
-                ix.rowKey[0].size() + ix.rowKey[1].size(), ix.hubOff.size(), bad, badSig);
+    long badFile = 0;
+    if (argc >= 4) {
+        const std::string file = argv[3];
+        const Prefixes pf = scan_rule_prefixes_text(text);
+        std::string e;
+        if (!save_graph_file(file, e2, p2, pf, ix, &e)) { std::printf("save: %s\n", e.c_str()); ++badFile; }
+        TermDict e3, p3;
+        Prefixes pf3;
+        HostIndex ix3;
+        if (!load_graph_file(file, e3, p3, pf3, ix3, &e)) { std::printf("load: %s\n", e.c_str()); ++badFile; }
+        if (e3.names != e2.names || p3.names != p2.names || pf3 != pf) ++badFile;
+        for (size_t i = 0; i < e3.names.size(); ++i)
+            if (e3.find(e3.names[i]) != (int32_t)i) { ++badFile; break; }
+        if (ix3.nPred != ix.nPred || ix3.nEnt != ix.nEnt || ix3.nTriples != ix.nTriples || ix3.hashMask != ix.hashMask) ++badFile;
+        for (int d = 0; d < 2; ++d)
+            if (ix3.val[d] != ix.val[d] || ix3.valRank[d] != ix.valRank[d] || ix3.src[d] != ix.src[d] ||
+                ix3.srcRank[d] != ix.srcRank[d] || ix3.rowKey[d] != ix.rowKey[d] || ix3.rowBeg[d] != ix.rowBeg[d] ||
+                ix3.predRow[d] != ix.predRow[d] || ix3.predEdge[d] != ix.predEdge[d] || ix3.hubOf[d] != ix.hubOf[d] ||
+                ix3.valSig[d] != ix.valSig[d] || ix3.sufSig[d] != ix.sufSig[d])
+                ++badFile;
+        if (ix3.hubOff != ix.hubOff || ix3.hubBits != ix.hubBits || ix3.hash.size() != ix.hash.size() ||
+            std::memcmp(ix3.hash.data(), ix.hash.data(), ix.hash.size() * sizeof(HashSlot)) != 0)
+            ++badFile;
+        // a truncated copy must be refused
+        std::string all;
+        read_file(file, all, &e);
+        const std::string cut = file + ".cut";
+        if (FILE* f = std::fopen(cut.c_str(), "wb")) {
+            std::fwrite(all.data(), 1, all.size() / 2, f);
+            std::fclose(f);
+        }
+        TermDict e4, p4;
+        Prefixes pf4;
+        HostIndex ix4;
+        if (load_graph_file(cut, e4, p4, pf4, ix4, &e)) ++badFile;
+        std::remove(cut.c_str());
+    }
+    bad += badFile;
+    std::printf("triples %zu rows %zu hubs %zu mismatches %ld (signatures %ld, graph file %ld)\n", s2.size() / 3,
+                ix.rowKey[0].size() + ix.rowKey[1].size(), ix.hubOff.size(), bad, badSig, badFile);
     return bad == 0 ? 0 : 1;
 }

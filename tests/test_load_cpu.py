@@ -16,12 +16,13 @@ def checker(tmp_path_factory):
     out = tmp_path_factory.mktemp("native") / "load_check"
     subprocess.run(["g++", "-O2", "-std=c++17", "-pthread", "-o", str(out),
                     str(ROOT / "tests" / "native" / "load_check.cpp"), str(CSRC / "turtle.cpp"),
-                    str(CSRC / "index.cpp")], check=True)
+                    str(CSRC / "index.cpp"), str(CSRC / "index_io.cpp")], check=True)
     return out
 
 
 def _run(checker, path, min_chunk):
-    r = subprocess.run([str(checker), str(path), str(min_chunk)], capture_output=True, text=True, timeout=300)
+    scratch = str(path) + ".graph"
+    r = subprocess.run([str(checker), str(path), str(min_chunk), scratch], capture_output=True, text=True, timeout=300)
     assert r.returncode == 0, r.stdout + r.stderr
 
 

@@ -209,3 +209,22 @@ def test_hub_rows_everywhere_or_nowhere(hub_min, memo_gain, tmp_path, monkeypatc
     with eng.GpuRulesLib(d / "graph.ttl") as lib:
         res, _, _ = lib.evaluate_rules_batch(fx["rules"])
         _check(res, fx["expected"], f"c2s hub_min={hub_min}")
+
+
+@pytest.mark.parametrize("name", ["fuzz_1.json", "fuzz_3.json"])
+def test_graph_file_loads_identically(name, tmp_path):
+    """A graph written by save_index and loaded back answers every rule as
+    the Turtle load does, per rule and batched."""
+    fx = load_fixture(name)
+    p = tmp_path / "graph.ttl"
+    p.write_text(fx["ttl"])
+    f = tmp_path / "graph.bin"
+    with eng.GpuRulesLib(p) as lib:
+        lib.save_index(f)
+    with eng.GpuRulesLib(index_path=f) as lib:
+        res, st, _ = lib.evaluate_rules_batch(fx["rules"])
+        _check(res, fx["expected"], f"{name} from graph file, batch")
+        _check([lib.evaluate_rule(t) for t in fx["rules"][:30]], fx["expected"][:30], f"{name} from graph file, per rule")
+    (tmp_path / "cut.bin").write_bytes(f.read_bytes()[:1000])
+    with pytest.raises(RuntimeError):
+        eng.GpuRulesLib(index_path=tmp_path / "cut.bin")
