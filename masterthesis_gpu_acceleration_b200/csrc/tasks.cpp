@@ -39,14 +39,6 @@ DevPlan plan_identity(const PhasePlan& ph) {
 }
 }  // namespace
 
-std::string phase_signature(const PhasePlan& ph) {
-    const DevPlan p = plan_identity(ph);
-    std::string s(reinterpret_cast<const char*>(&p), sizeof(p));
-    s.append(reinterpret_cast<const char*>(&ph.rootBeg), sizeof(ph.rootBeg));
-    s.append(reinterpret_cast<const char*>(&ph.rootEnd), sizeof(ph.rootEnd));
-    return s;
-}
-
 bool phase_equal(const PhasePlan& a, const PhasePlan& b) {
     if (a.rootBeg != b.rootBeg || a.rootEnd != b.rootEnd) return false;
     const DevPlan pa = plan_identity(a), pb = plan_identity(b);

@@ -35,13 +35,11 @@ struct PhaseTasks {
 // Host time of one step of a per-root walk (ns), for the cost-aware mode.
 constexpr double kWalkNsPerEdge = 8.0;
 
-// Identity of a phase's device computation: the plan without its
-// per-launch fields, and its root range.  Phases with equal signatures
-// produce equal counts.
-std::string phase_signature(const PhasePlan& ph);
-// Whether two phases have equal signatures (without building them).
+// The signature of a phase is the identity of its device computation: the
+// plan without its per-launch fields, and its root range.  Phases with equal
+// signatures produce equal counts.  phase_equal compares two signatures;
+// phase_hash is a 64-bit hash of one (the key of the task builder's caches).
 bool phase_equal(const PhasePlan& a, const PhasePlan& b);
-// 64-bit hash of phase_signature (keys of the task builder's caches).
 uint64_t phase_hash(const PhasePlan& ph);
 
 class TaskBuilder {
