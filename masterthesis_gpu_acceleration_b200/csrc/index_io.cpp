@@ -12,8 +12,37 @@ namespace gr {
 namespace {
 
 constexpr char kMagic[8] = {'G', 'R', 'G', 'R', 'A', 'P', 'H', '1'};
-constexpr char kEnd[8] = {'G', 'R', 'E', 'N', 'D', '0', '0', '1'};
-constexpr uint32_t kVersion = 1;
+constexpr char kEnd[8] = {'G', 'R', 'E', 'N', 'D', '0', '0', '2'};
+constexpr uint32_t kVersion = 2;
+
+// Running 64-bit checksum of everything written before it.  Each call's
+// bytes go into four independent multiply-xorshift lanes, 32 bytes a round
+// (so that the lanes' multiplies overlap), then its trailing words and
+// bytes into the first lane; the lanes fold into one word at every call.
+struct Checksum {
+    uint64_t h = 0x6A09E667F3BCC909ull;
+    static uint64_t mix(uint64_t x, uint64_t w) {
+        x = (x ^ w) * 0x9E3779B97F4A7C15ull;
+        return x ^ (x >> 31);
+    }
+    void add(const void* p, size_t n) {
+        const unsigned char* b = static_cast<const unsigned char*>(p);
+        uint64_t l[4] = {h, h ^ 0xBB67AE8584CAA73Bull, h ^ 0x3C6EF372FE94F82Bull, h ^ 0xA54FF53A5F1D36F1ull};
+        size_t i = 0;
+        for (; i + 32 <= n; i += 32) {
+            uint64_t w[4];
+            std::memcpy(w, b + i, 32);
+            for (int k = 0; k < 4; ++k) l[k] = mix(l[k], w[k]);
+        }
+        for (; i + 8 <= n; i += 8) {
+            uint64_t w;
+            std::memcpy(&w, b + i, 8);
+            l[0] = mix(l[0], w);
+        }
+        for (; i < n; ++i) l[0] = (l[0] ^ b[i]) * 0x100000001B3ull;
+        h = mix(mix(mix(l[0], l[1]), l[2]), l[3] ^ (uint64_t)n);
+    }
+};
 constexpr uint32_t kByteOrder = 0x01020304u;
 
 struct Header {
@@ -32,8 +61,10 @@ using File = std::unique_ptr<FILE, FileCloser>;
 struct Writer {
     FILE* f;
     bool ok = true;
+    Checksum sum;
     void bytes(const void* p, size_t n) {
         if (ok && n && std::fwrite(p, 1, n, f) != n) ok = false;
+        sum.add(p, n);
     }
     template <class T> void pod(const T& v) { bytes(&v, sizeof(T)); }
     template <class T> void vec(const std::vector<T>& v) {
@@ -50,9 +81,11 @@ struct Reader {
     FILE* f;
     uint64_t left;   // bytes not yet read: no count may claim more
     bool ok = true;
+    Checksum sum;
     void bytes(void* p, size_t n) {
         if (!ok || n > left || (n && std::fread(p, 1, n, f) != n)) { ok = false; return; }
         left -= n;
+        sum.add(p, n);
     }
     template <class T> void pod(T& v) { bytes(&v, sizeof(T)); }
     template <class T> void vec(std::vector<T>& v) {
@@ -191,6 +224,8 @@ bool save_graph_file(const std::string& path, const TermDict& ents, const TermDi
     w.pod<uint64_t>(pf.size());
     for (const auto& kv : pf) { w.str(kv.first); w.str(kv.second); }
     each_array(const_cast<HostIndex&>(ix), [&](auto& v) { w.vec(v); });
+    const uint64_t sum = w.sum.h;
+    w.pod(sum);
     w.bytes(kEnd, 8);
     const bool flushed = std::fflush(f.get()) == 0;
     if (!w.ok || !flushed) { if (err) *err = "write failed: " + path; return false; }
@@ -229,9 +264,13 @@ bool load_graph_file(const std::string& path, TermDict& ents, TermDict& preds, P
         prefixes.emplace(std::move(k), std::move(v));
     }
     each_array(ix, [&](auto& v) { r.vec(v); });
+    const uint64_t want = r.sum.h;
+    uint64_t sum = 0;
+    r.pod(sum);
     char end[8] = {};
     r.bytes(end, 8);
     if (!r.ok || std::memcmp(end, kEnd, 8) != 0 || r.left != 0) return fail("truncated or damaged graph file");
+    if (sum != want) return fail("graph file checksum mismatch");
     std::string why;
     if (!consistent(ix, ents.names.size(), preds.names.size(), &why)) return fail("inconsistent graph file (" + why + ")");
     return true;

@@ -2,7 +2,8 @@
 // saved to and read back from one binary file, so that a graph is parsed
 // and indexed once and later loads skip both.  The file holds exactly the
 // arrays the index keeps, in this machine's byte order, after a header with
-// a format version; a file of another version or of inconsistent sizes is
+// a format version, and ends with a checksum of everything before it; a file
+// of another version, with a wrong checksum or of inconsistent sizes is
 // refused.
 #pragma once
 #include <string>

@@ -9,7 +9,7 @@
 //      and every suffix signature is the union of the value signatures from
 //      its edge to the end of its row;
 //   4. the graph written to a binary file reads back identical, and a
-//      truncated copy of the file is refused.
+//      truncated copy, or a copy with any one byte changed, is refused.
 // Usage: load_check FILE.ttl MIN_CHUNK_BYTES [SCRATCH_FILE]
 #include <cstdio>
 #include <cstdlib>
@@ -105,6 +105,21 @@ int main(int argc, char** argv) {
         Prefixes pf4;
         HostIndex ix4;
         if (load_graph_file(cut, e4, p4, pf4, ix4, &e)) ++badFile;
+        // single changed bytes at seeded positions
+        uint64_t x = 0x9E3779B97F4A7C15ull;
+        for (int k = 0; k < 24 && !all.empty(); ++k) {
+            x = x * 6364136223846793005ull + 1442695040888963407ull;
+            std::string bent = all;
+            bent[(size_t)((x >> 17) % all.size())] ^= (char)(1 + (x >> 61));
+            if (FILE* f = std::fopen(cut.c_str(), "wb")) {
+                std::fwrite(bent.data(), 1, bent.size(), f);
+                std::fclose(f);
+            }
+            TermDict e5, p5;
+            Prefixes pf5;
+            HostIndex ix5;
+            if (load_graph_file(cut, e5, p5, pf5, ix5, &e)) ++badFile;
+        }
         std::remove(cut.c_str());
     }
     bad += badFile;
