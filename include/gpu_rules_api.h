@@ -234,7 +234,8 @@ int gpu_save_index(void* ctx, const char* path);
 /* Loads a graph from a file written by gpu_save_index, skipping the Turtle
  * parse and the index build; otherwise like gpu_load_graph (NULL with
  * gpu_last_error() set on failure, including a file of another format
- * version or one whose sizes or offsets do not agree). */
+ * version, one whose checksum does not match, or one whose sizes or offsets
+ * do not agree). */
 void* gpu_load_index(const char* path);
 
 /* Last error message of the calling thread ("" if none). */
