@@ -24,6 +24,7 @@ from dataclasses import dataclass, field
 from typing import Callable, Sequence
 
 Atom = tuple[str, str, str]   # (subject variable, predicate IRI, object variable)
+_RENAMED = tuple(f"?x{i}" for i in range(8))   # canonical names of body-only variables
 
 
 @dataclass(frozen=True)
@@ -54,10 +55,18 @@ class Rule:
     def key(self) -> tuple:
         """Canonical form: the smallest sorted atom list over renamings of
         the body-only variables (the head keeps ?a and ?b)."""
-        extra = [v for v in self.variables() if v not in self.head[0::2]]
+        hs, _, ho = self.head
+        extra: list[str] = []   # body-only variables in first-occurrence order
+        for s, _, o in self.body:
+            if s != hs and s != ho and s not in extra:
+                extra.append(s)
+            if o != hs and o != ho and o not in extra:
+                extra.append(o)
+        if not extra:
+            return (self.head, tuple(sorted(self.body)))
         best = None
-        for perm in itertools.permutations(range(len(extra))):
-            ren = {v: f"?x{perm[i]}" for i, v in enumerate(extra)}
+        for perm in itertools.permutations(_RENAMED[:len(extra)]):
+            ren = dict(zip(extra, perm))
             atoms = tuple(sorted((ren.get(s, s), p, ren.get(o, o)) for s, p, o in self.body))
             if best is None or atoms < best:
                 best = atoms
@@ -151,6 +160,8 @@ def mine(evaluate: Callable[[list[Rule]], list[dict]], predicates: Sequence[tupl
             keep.append(r)
         if level == max_body:
             break
+        # only the first max_candidates new refinements are scored, so
+        # generation stops there (keys of longer bodies never meet these)
         nxt = []
         for r in keep:
             for c in refinements(r, body_preds, max_vars):
@@ -158,5 +169,9 @@ def mine(evaluate: Callable[[list[Rule]], list[dict]], predicates: Sequence[tupl
                 if k not in seen:
                     seen.add(k)
                     nxt.append(c)
+                    if len(nxt) >= max_candidates:
+                        break
+            if len(nxt) >= max_candidates:
+                break
         frontier = nxt
     return result
