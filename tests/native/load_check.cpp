@@ -8,9 +8,12 @@
 //      holds the bit of every (pred, dir) under which the value keys a row,
 //      and every suffix signature is the union of the value signatures from
 //      its edge to the end of its row;
-//   4. the graph written to a binary file reads back identical, and a
+//   4. every hub row's bitmap has exactly the bits of its edges' value
+//      ranks, within its predicate's domain;
+//   5. the graph written to a binary file reads back identical, and a
 //      truncated copy, or a copy with any one byte changed, is refused.
 // Usage: load_check FILE.ttl MIN_CHUNK_BYTES [SCRATCH_FILE]
+#include <algorithm>
 #include <cstdio>
 #include <cstdlib>
 #include <cstring>
@@ -70,6 +73,22 @@ int main(int argc, char** argv) {
             }
     }
     bad += badSig;
+    long badHub = 0;
+    for (int d = 0; d < 2; ++d)
+        for (int32_t p = 0; p < ix.nPred; ++p) {
+            const int64_t words = (ix.pred_rows(p, 1 - d) + 31) / 32;
+            for (int32_t r = ix.predRow[d][p]; r < ix.predRow[d][p + 1]; ++r) {
+                const int32_t h = ix.hubOf[d][r];
+                if (h < 0) continue;
+                std::vector<uint32_t> want((size_t)words, 0u);
+                for (int32_t e = ix.rowBeg[d][r]; e < ix.rowBeg[d][r + 1]; ++e)
+                    want[(size_t)(ix.valRank[d][e] >> 5)] |= 1u << (ix.valRank[d][e] & 31);
+                if (ix.hubOff[h] + words > (int64_t)ix.hubBits.size() ||
+                    !std::equal(want.begin(), want.end(), ix.hubBits.begin() + ix.hubOff[h]))
+                    ++badHub;
+            }
+        }
+    bad += badHub;
     long badFile = 0;
     if (argc >= 4) {
         const std::string file = argv[3];
@@ -123,7 +142,8 @@ int main(int argc, char** argv) {
         std::remove(cut.c_str());
     }
     bad += badFile;
-    std::printf("triples %zu rows %zu hubs %zu mismatches %ld (signatures %ld, graph file %ld)\n", s2.size() / 3,
-                ix.rowKey[0].size() + ix.rowKey[1].size(), ix.hubOff.size(), bad, badSig, badFile);
+    std::printf("triples %zu rows %zu hubs %zu mismatches %ld (signatures %ld, hub bitmaps %ld, graph file %ld)\n",
+                s2.size() / 3, ix.rowKey[0].size() + ix.rowKey[1].size(), ix.hubOff.size(), bad, badSig, badHub,
+                badFile);
     return bad == 0 ? 0 : 1;
 }
