@@ -46,11 +46,17 @@ class Rule:
         return seen
 
     def closed(self) -> bool:
+        return self.singletons() == 0
+
+    def singletons(self) -> int:
+        """Variables that occur once (head included).  A dangling atom never
+        lowers the count and a closing atom lowers it by at most 2, so a rule
+        with more than 2 x (atoms still to add) of them never closes."""
         count: dict[str, int] = {}
         for s, _, o in (self.head,) + self.body:
             count[s] = count.get(s, 0) + 1
             count[o] = count.get(o, 0) + 1
-        return all(c >= 2 for c in count.values())
+        return sum(1 for c in count.values() if c == 1)
 
     def key(self) -> tuple:
         """Canonical form: the smallest sorted atom list over renamings of
@@ -119,12 +125,18 @@ def gpu_evaluator(lib, per_rule: bool = False) -> Callable[[list[Rule]], list[di
 def mine(evaluate: Callable[[list[Rule]], list[dict]], predicates: Sequence[tuple[str, int]],
          max_body: int = 2, min_support: int = 2, min_head_coverage: float = 0.01,
          min_confidence: float = 0.1, max_head_predicates: int | None = None, max_vars: int = 4,
-         max_candidates: int = 200_000) -> MiningResult:
+         max_candidates: int = 200_000, prune_unclosable: bool = True) -> MiningResult:
     """Level-wise mining of rules with up to `max_body` body atoms.
 
     predicates: (IRI, triples) of the graph (GpuRulesLib.predicates()); head
     predicates are those with at least `min_support` triples, the largest
-    first, at most `max_head_predicates` of them."""
+    first, at most `max_head_predicates` of them.  prune_unclosable: skip
+    candidates that can no longer become closed within `max_body` atoms
+    (they could be neither output nor refined into output rules)."""
+
+    def closable(r: Rule) -> bool:
+        return not prune_unclosable or r.singletons() <= 2 * (max_body - len(r.body))
+
     heads = [p for p, n in sorted(predicates, key=lambda x: -x[1]) if n >= min_support]
     if max_head_predicates is not None:
         heads = heads[:max_head_predicates]
@@ -140,7 +152,7 @@ def mine(evaluate: Callable[[list[Rule]], list[dict]], predicates: Sequence[tupl
                 if atom == head:
                     continue
                 r = Rule(head, (atom,))
-                if r.key() not in seen:
+                if closable(r) and r.key() not in seen:
                     seen.add(r.key())
                     frontier.append(r)
     for level in range(1, max_body + 1):
@@ -165,6 +177,8 @@ def mine(evaluate: Callable[[list[Rule]], list[dict]], predicates: Sequence[tupl
         nxt = []
         for r in keep:
             for c in refinements(r, body_preds, max_vars):
+                if not closable(c):
+                    continue
                 k = c.key()
                 if k not in seen:
                     seen.add(k)

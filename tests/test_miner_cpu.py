@@ -39,3 +39,15 @@ def test_mining_with_the_oracle():
     again = oracle_evaluator(g)([s.rule for s in res.rules])
     assert [m["support"] for m in again] == [s.support for s in res.rules]
     assert [m["bodySize"] for m in again] == [s.body_size for s in res.rules]
+
+
+def test_unclosable_candidates_are_skipped_without_changing_output():
+    t, _ = small_graph()
+    g = oracle.OracleGraph(t, 4)
+    preds = [(P + str(k), int((t[:, 1] == k).sum())) for k in range(4)]
+    kw = dict(max_body=2, min_support=5, min_head_coverage=0.01, min_confidence=0.0, max_head_predicates=2)
+    pruned = miner.mine(oracle_evaluator(g), preds, **kw)
+    full = miner.mine(oracle_evaluator(g), preds, prune_unclosable=False, **kw)
+    assert pruned.evaluated < full.evaluated
+    key = lambda res: sorted((s.rule.key(), s.support, s.body_size) for s in res.rules)
+    assert key(pruned) == key(full)
