@@ -165,6 +165,19 @@ def cpu_sample(cfg: str, n: int) -> tuple[list[int], str]:
     return list(range(n)), f"every {cfg} rule"
 
 
+def host_cpu() -> dict:
+    """The host's CPU model and logical core count (stated beside CPU timings)."""
+    model = ""
+    try:
+        for line in Path("/proc/cpuinfo").read_text().splitlines():
+            if line.startswith("model name"):
+                model = line.split(":", 1)[1].strip()
+                break
+    except OSError:
+        pass
+    return {"model": model, "logical_cores": os.cpu_count()}
+
+
 def cpu_baseline(d: Path, rules: list[str], cfg: str = "c3", timeout: float = 300.0) -> dict:
     """The reference's CPU_01 code, one thread, on a bounded sample."""
     import oracle
@@ -186,7 +199,7 @@ def cpu_baseline(d: Path, rules: list[str], cfg: str = "c3", timeout: float = 30
             secs = oracle.time_oracle(g, np.concatenate(ir), len(ir))
             kind = "port"
     return {"value": len(sample) / secs, "unit": "rules/s", "cores": 1, "kind": kind, "sample": desc,
-            "seconds": secs}
+            "seconds": secs, "host": host_cpu()}
 
 
 def _oracle_worker(triples_path, n_pred, irs, q):
@@ -327,7 +340,7 @@ def reference_arm(args):
     line = dict(base)
     line.update({"value": value, "ms_per_step": 1e3 * total_s / steps,
                  "cpu_baseline": {"value": value, "unit": "rules/s", "cores": threads if kind == "reference" else 1,
-                                  "kind": kind, "sample": desc},
+                                  "kind": kind, "sample": desc, "host": host_cpu()},
                  "e2e": {"value": value, "unit": "rules/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}})
     print(json.dumps(line), flush=True)
 

@@ -23,5 +23,19 @@ def test_reference_arm_prints_contract_line(tmp_path):
         assert k in line, k
     cb = line["cpu_baseline"]
     assert cb["kind"] == "reference" and cb["cores"] >= 1 and cb["value"] == line["value"] and cb["sample"]
+    assert cb["host"]["logical_cores"] >= cb["cores"]
     assert line["e2e"] == {"value": line["value"], "unit": "rules/s", "h2d_bytes_per_step": 0,
                            "d2h_bytes_per_step": 0}
+
+
+@pytest.mark.skipif(not oracle.ref_available(), reason="oracle/_ref not built")
+def test_engine_arm_cpu_baseline_helper(tmp_path):
+    """The engine arm's cpu_baseline (timed by the reference's CPU code on a
+    bounded sample) runs without a GPU and states the host."""
+    sys.path.insert(0, str(ROOT))
+    import bench
+    from masterthesis_gpu_acceleration_b200 import synth
+    d = synth.generate("c1", tmp_path / "c1", seed=0)
+    cb = bench.cpu_baseline(d, synth.read_rules(d), "c1")
+    assert cb["kind"] == "reference" and cb["value"] > 0 and cb["cores"] == 1
+    assert cb["host"]["logical_cores"] >= 1 and "model" in cb["host"]
