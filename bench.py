@@ -13,8 +13,16 @@ The graph and rules are seeded synthetic data with the reference's shapes
             flushed (256 MiB write) before every step, outside the timed span
     e2e     rules/s through gpu_evaluate_rules_batch with host rule strings:
             parse, plan, pinned host->device copy, kernel, device->host copy
-    per_rule  the plain form, one launch per phase per rule via
-            gpu_evaluate_rule (the reference library's calling pattern)
+            (warm: the same rules were prepared on this context before)
+    e2e_cold  the same call on unseen rules: a fresh context per step and a
+            rule set of its own
+    per_rule_rules_per_s  the plain form, one launch per phase per rule via
+            gpu_evaluate_rule (the reference library's calling pattern), and
+            batched_vs_per_rule = value / that
+    dense_confidence  c2 and c2s: the body-size (confidence) launch alone,
+            algorithmic GB/s as a fraction of the measured HBM peak
+    serving_c5  the c3 and c4 graphs resident together, one Poisson stream
+            across both at 1k-50k rules/s: sustained rate, p50, p99
 
 Multi-GPU (torchrun): each rank evaluates its own 10,000-rule set (rule seed =
 rank) over the same graph; no data-path collective; value = all ranks' rules
@@ -73,6 +81,8 @@ def parse_args():
     ap.add_argument("--no-serve", action="store_true")
     ap.add_argument("--no-gpu03", action="store_true",
                     help="skip the reference GPU library (GPU_03) per-rule comparator")
+    ap.add_argument("--no-cold", action="store_true", help="skip the cold end-to-end measurement")
+    ap.add_argument("--no-dense", action="store_true", help="skip the dense (c2, c2s) confidence measurement")
     ap.add_argument("--data", default=os.environ.get("KG_DATA_DIR", str(Path(tempfile.gettempdir()) / "kg_synth_data")))
     return ap.parse_args()
 
@@ -246,24 +256,45 @@ def check_sample(graph_dir: Path, stream_dir: Path, results: dict, n_pred: int, 
     return {"sampled": len(picks), "checked": len(got), "mismatches": bad, "exact": bad == 0 and len(got) > 0}
 
 
+SERVE_RATES = [1000, 2000, 5000, 10000, 20000, 50000]
+
+
 def serving_sweep(lib, d: Path, args) -> dict:
-    """C5-shaped requests (chain rules, geometric(0.4) lengths up to 8,
-    predicates by frequency) on the resident c3 graph at swept Poisson rates."""
+    """Config 5: the c3 and c4 graphs resident together (one server each) and
+    one open-loop Poisson stream of chain rules (lengths geometric(0.4) in
+    1..8, predicates by frequency) drawn across both graphs, at swept rates;
+    1 % of the results checked bit-exact against the C oracle."""
+    import masterthesis_gpu_acceleration_b200 as eng
     from masterthesis_gpu_acceleration_b200 import serving, synth
-    n_pred = int(synth.read_meta(d)["predicates"])
-    pc = synth.pred_counts(synth.read_triples(d), n_pred)
-    sd = synth.rule_stream(pc, 20000, Path(args.data) / "c5_stream", p=0.4, max_len=8, seed=1)
-    rules = synth.read_rules(sd)
-    rates = [1000, 2000, 5000, 10000, 20000, 50000]
-    rows, res = serving.sweep(lib, rules, rates, duration=args.serve_seconds, seed=11)
-    check = check_sample(d, sd, res, n_pred)
-    return {"workload": "c5-shaped stream on the c3 graph: 20,000 chain rules, lengths geometric(0.4) in 1..8, "
-                        "predicates by frequency, open-loop Poisson arrivals",
-            "seconds_per_rate": args.serve_seconds, "slots": "4 (3 light + 1 heavy lane)", "rates": rows,
-            "oracle_check_1pct": check}
+    graphs, dirs, streams = [(lib, None)], [d], []
+    d4 = data_for(argparse.Namespace(**{**vars(args), "config": "c4"}), 0)
+    lib4 = eng.GpuRulesLib(d4 / "graph.ttl")
+    try:
+        graphs.append((lib4, None))
+        dirs.append(d4)
+        for g, gd in enumerate(dirs):
+            n_pred = int(synth.read_meta(gd)["predicates"])
+            pc = synth.pred_counts(synth.read_triples(gd), n_pred)
+            sd = synth.rule_stream(pc, 20000, Path(args.data) / f"c5_stream_{g}", p=0.4, max_len=8, seed=1 + g)
+            streams.append(sd)
+            graphs[g] = (graphs[g][0], synth.read_rules(sd))
+        rows, res = serving.sweep_multi(graphs, SERVE_RATES, duration=args.serve_seconds, seed=11)
+        checks = [check_sample(gd, sd, r, int(synth.read_meta(gd)["predicates"]))
+                  for gd, sd, r in zip(dirs, streams, res)]
+    finally:
+        lib4.close()
+    return {"graphs": "c3 + c4 resident, one server each (4 slots), arrivals split 50/50",
+            "seconds_per_rate": args.serve_seconds,
+            "rates": [[r["offered_rules_per_s"], round(r["sustained_rules_per_s"]), round(r["p50_ms"], 2),
+                       round(r["p99_ms"], 2)] for r in rows],
+            "rates_fields": ["offered/s", "sustained/s", "p50 ms", "p99 ms"],
+            "p99_ms_by_graph": [[round(x["p99_ms"], 2) if x["p99_ms"] is not None else None for x in r["per_graph"]]
+                                for r in rows],
+            "oracle_check_1pct": [f"{c['checked']}/{c['sampled']} checked, {c['mismatches']} mismatches"
+                                  for c in checks]}
 
 
-def gpu03_comparator(d: Path, per_rule: dict | None, timeout: float = 600.0) -> dict:
+def gpu03_comparator(d: Path, timeout: float = 600.0) -> dict:
     """The reference's own GPU library (GPU_03, built from its sources for
     sm_100a by baseline/build_gpu03.sh) on every rule, one call per rule, in a
     separate process.  GPU_03 skips the body size when support is 0 and
@@ -282,17 +313,74 @@ def gpu03_comparator(d: Path, per_rule: dict | None, timeout: float = 600.0) -> 
     g = json.loads(lines[-1])
     if "unavailable" in g:
         return g
-    out = {k: g[k] for k in ("rules", "wall_s", "device_ms", "rules_per_s_wall", "rules_per_s_device")}
+    out = {"rules_per_s_wall": round(g["rules_per_s_wall"], 1), "rules_per_s_device": round(g["rules_per_s_device"], 1)}
     gold = ROOT / "tests" / "golden" / "c3_seed0.npz"
     if gold.exists():
         exp = np.load(gold)["expected"].tolist()
-        res = g["results"]
-        out["equal_to_reference_cpu"] = sum(1 for a, b in zip(res, exp) if a == b)
-        out["support_equal_to_reference_cpu"] = sum(1 for a, b in zip(res, exp) if a and a[0] == b[0])
-    if per_rule:
-        out["engine_per_rule_speedup_wall"] = per_rule["rules_per_s_wall"] / out["rules_per_s_wall"]
-    out["api"] = "GPU_03 gpu_evaluate_rule, one call per rule (the reference library's calling pattern)"
+        out["equal_to_reference_cpu"] = sum(1 for a, b in zip(g["results"], exp) if a == b)
     return out
+
+
+def dense_confidence(args, peak_gbs: float) -> dict:
+    """The dense configurations (c2, and c2s with Zipf(1.3) subjects): the
+    batched rules/s, and the confidence (body-size) launch alone, prepared
+    with only body-size phases, as algorithmic GB/s against the measured HBM
+    peak, batched (one launch for all rules, L2 flushed before each) and
+    plain (one launch per rule, device span)."""
+    import masterthesis_gpu_acceleration_b200 as eng
+    from masterthesis_gpu_acceleration_b200 import synth
+    out = {}
+    for cfg in ("c2", "c2s"):
+        d = synth.generate(cfg, Path(args.data) / cfg, seed=0)
+        rules = synth.read_rules(d)
+        with eng.GpuRulesLib(d / "graph.ttl") as lib:
+            full = lib.prepare_batch(rules)
+            full.autotune(1)
+            for _ in range(3):
+                full.run(FLUSH_BYTES)
+            ms = sum(full.run(FLUSH_BYTES)[2] for _ in range(args.steps)) / args.steps
+            full.close()
+            lib.set_option("batch_phases", 2)
+            body = lib.prepare_batch(rules)
+            body.autotune(1)
+            for _ in range(3):
+                body.run(FLUSH_BYTES)
+            bms = sum(body.run(FLUSH_BYTES)[2] for _ in range(args.steps)) / args.steps
+            nbytes = body.count_bytes()
+            body.close()
+            lib.set_option("batch_phases", 3)
+            per = [lib.evaluate_rule(r) for r in rules]   # warm
+            conf_ms = sum(lib.evaluate_rule(r).confidenceMs for r in rules)
+            pairs = sum(r.bodySize for r in per)
+        gbs_b = nbytes / (bms / 1e3) / 1e9
+        gbs_p = nbytes / (conf_ms / 1e3) / 1e9 if conf_ms > 0 else None
+        out[cfg] = {"rules_per_s": round(len(rules) / (ms / 1e3)), "body_pairs": pairs,
+                    "conf_batched_ms": round(bms, 4), "conf_batched_gbs": round(gbs_b, 1),
+                    "conf_batched_frac": round(gbs_b / peak_gbs, 4),
+                    "conf_per_rule_ms": round(conf_ms, 4),
+                    "conf_per_rule_frac": round(gbs_p / peak_gbs, 4) if gbs_p else None,
+                    "conf_alg_bytes": nbytes}
+    return out
+
+
+def e2e_cold(args, steps: int) -> dict:
+    """End to end on rules the engine has never seen: per step a fresh
+    context on the c3 graph (load untimed) and a 10,000-rule set of its own
+    (rule seeds 1..steps, disjoint from the timed batch's set), one call of
+    gpu_evaluate_rules_batch with host strings, host wall clock."""
+    import masterthesis_gpu_acceleration_b200 as eng
+    from masterthesis_gpu_acceleration_b200 import synth
+    total_rules, total_s, h2d = 0, 0.0, 0
+    for k in range(1, steps + 1):
+        d = synth.generate("c3", Path(args.data) / f"c3_cold{k}", seed=0, rule_seed=1000 + k)
+        rules = synth.read_rules(d)
+        with eng.GpuRulesLib(d / "graph.ttl") as lib:
+            t0 = time.perf_counter()
+            lib.evaluate_rules_batch(rules)
+            total_s += time.perf_counter() - t0
+        total_rules += len(rules)
+    return {"value": round(total_rules / total_s, 1), "unit": "rules/s", "steps": steps,
+            "what": "fresh context per step, unseen c3 rule set (rule seeds 1001..), gpu_evaluate_rules_batch, wall"}
 
 
 def reference_arm(args):
@@ -390,9 +478,8 @@ def engine_arm(args):
     phys = int(vis[dev]) if dev < len(vis) and vis[dev].strip().isdigit() else dev
     clocks = ClockSampler(phys).start()
     total_ms = 0.0
-    results = None
     for _ in range(args.steps):
-        results, st, ms = batch.run(FLUSH_BYTES)
+        _, _, ms = batch.run(FLUSH_BYTES)
         total_ms += ms
     barrier()
     clk = clocks.stop()
@@ -410,6 +497,7 @@ def engine_arm(args):
                             for e in fx["expected"]], dtype=np.int64)
         if exp is not None:
             exact = bool((batch.counts() == exp).all())
+    modes, _ = batch.dedup()
 
     # ---- roofline: algorithmic bytes per launch over the average launch ----
     alg_bytes = batch.count_bytes()
@@ -418,7 +506,8 @@ def engine_arm(args):
     achieved = alg_bytes / avg_s / 1e9
     traffic = profile_traffic() if args.config == "c3" and not args.max_rules else None
 
-    # ---- end to end through the C ABI with host strings ----
+    # ---- end to end through the C ABI with host strings (warm: the rules
+    # were prepared and autotuned on this context above) ----
     for _ in range(max(1, args.warmup // 2)):
         lib.evaluate_rules_batch(rules)
     barrier()
@@ -429,62 +518,57 @@ def engine_arm(args):
     e2e_s = allmax(time.perf_counter() - t0)
     e2e = {"value": world * len(rules) * args.steps / e2e_s, "unit": "rules/s",
            "h2d_bytes_per_step": info["h2d_bytes"], "d2h_bytes_per_step": info["d2h_bytes"],
-           "api": "gpu_evaluate_rules_batch (parse + plan + H2D + kernel + D2H), host wall clock"}
+           "api": "gpu_evaluate_rules_batch, host strings in, results out, wall clock; warm (rules seen before)"}
 
     # ---- the plain per-rule form (one launch per phase per rule) ----
     per_rule = None
     if not args.no_per_rule:
         barrier()
         t0 = time.perf_counter()
-        dev_ms = 0.0
         for r in rules:
-            res = lib.evaluate_rule(r)
-            dev_ms += res.supportMs + res.confidenceMs
-        wall = allmax(time.perf_counter() - t0)
-        dev_ms = allmax(dev_ms)
-        per_rule = {"rules_per_s_wall": world * len(rules) / wall,
-                    "rules_per_s_device": world * len(rules) / (dev_ms / 1e3),
-                    "batched_speedup_vs_per_rule_wall": value / (world * len(rules) / wall)}
+            lib.evaluate_rule(r)
+        per_rule = world * len(rules) / allmax(time.perf_counter() - t0)
 
-    cpu = None
-    if rank == 0 and world == 1 and not args.no_cpu_baseline:
-        cpu = cpu_baseline(d, rules, args.config)
-
-    gpu03 = None
-    if rank == 0 and world == 1 and not args.no_gpu03 and args.config == "c3" and not args.max_rules:
-        gpu03 = gpu03_comparator(d, per_rule)
-        if "rules_per_s_wall" in gpu03:
-            gpu03["engine_batched_speedup_wall"] = value / gpu03["rules_per_s_wall"]
-
-    serving = None
-    if rank == 0 and world == 1 and not args.no_serve and args.config == "c3":
-        serving = serving_sweep(lib, d, args)
+    solo = rank == 0 and world == 1
+    cold = e2e_cold(args, min(args.steps, 5)) if solo and args.config == "c3" and not args.max_rules \
+        and not args.no_cold else None
+    cpu = cpu_baseline(d, rules, args.config) if solo and not args.no_cpu_baseline else None
+    gpu03 = gpu03_comparator(d) if solo and not args.no_gpu03 and args.config == "c3" and not args.max_rules else None
+    dense = dense_confidence(args, peaks["hbm_gbs"]) if solo and not args.no_dense and args.config == "c3" \
+        and not args.max_rules else None
+    serving = serving_sweep(lib, d, args) if solo and not args.no_serve and args.config == "c3" \
+        and not args.max_rules else None
 
     batch.close()
     lib.close()
     if rank == 0:
+        if cpu:
+            cpu = {k: (round(v, 3) if isinstance(v, float) else v) for k, v in cpu.items() if k != "seconds"}
         line = {
             "metric": METRIC, "value": value, "unit": "rules/s", "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": max_ms / args.steps, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "int32", "data": "synthetic",
             "config": {"workload": WORKLOADS[args.config], "global_batch": world * len(rules),
-                       "rules_per_rank": len(rules),
                        "parallelism": f"rule sets sharded over {world} GPU(s), no collective",
                        "l2": "flushed before every step (256 MiB write, outside the timed span)",
                        "exact_vs_reference_golden": exact, "plans": info["plans"], "tasks": info["tasks"],
+                       "dedup_modes": {str(m): int((modes == m).sum()) for m in sorted(set(modes.tolist())) if m >= 0},
                        "graph_load_s": round(load_s, 3)},
+            "per_rule_rules_per_s": round(per_rule, 1) if per_rule else None,
+            "batched_vs_per_rule": round(value / per_rule, 2) if per_rule else None,
             "e2e": e2e,
-            "per_rule": per_rule,
-            "reference_gpu_per_rule": gpu03,
-            "serving": serving,
+            "e2e_cold": cold,
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": peaks["hbm_gbs"], "unit": "GB/s",
                          "frac": achieved / peaks["hbm_gbs"], "traffic": traffic,
                          "algorithmic_bytes_per_launch": alg_bytes, "peak_source": peaks["source"] + " (burst copy)"},
             "cpu_baseline": cpu,
             "clocks": clk,
             "gpu_launches": args.steps,
+            "reference_gpu03_per_rule": gpu03,
+            "dense_confidence": dense,
+            "serving_c5": serving,
         }
-        print(json.dumps(line), flush=True)
+        print(json.dumps(line, separators=(",", ":")), flush=True)
     if world > 1:
         import torch.distributed as dist
         dist.barrier()

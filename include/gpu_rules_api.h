@@ -70,7 +70,7 @@ int gpu_query_vram(size_t* freeBytesOut, size_t* totalBytesOut);
  * rule i does not parse (its result is then zero).  deviceMs (optional)
  * receives the device time of the whole batch.  Per-rule supportMs and
  * confidenceMs are 0 in this mode.  Returns 0, or -1 on null arguments or a
- * CUDA error. */
+ * CUDA error (then every out[i] is zero and every status[i] is -1). */
 int gpu_evaluate_rules_batch(void* ctx, const char* const* rules, int n, int isJson,
                              GpuRuleResult* out, int* status, double* deviceMs);
 
@@ -136,6 +136,17 @@ int gpu_batch_autotune(void* batch, int rounds);
 /* Frees a prepared batch (NULL is ignored). */
 void gpu_batch_free(void* batch);
 
+/* How each rule's body size deduplicates its (hS, hO) pairs in the batch's
+ * current staging (no counterpart in the reference, which picks a bitmap or
+ * a pair buffer with sort + unique from one N^2 size test,
+ * GPU_03/gpu_rules_lib.cu:296-316): modes[i] (n entries) = 0 bitmap rows in
+ * shared memory, 1 one global bitmap row per head subject, 2 global rows per
+ * resident block (memory bounded by the launch, not the rows), 3 pair keys
+ * radix-sorted and counted once each; -1 when rule i's body size needs no
+ * pair deduplication on the device.  sortKeys (optional): pair keys the last
+ * run appended.  Returns 0, or -1 on null arguments. */
+int gpu_batch_dedup(void* batch, int* modes, long long* sortKeys);
+
 /* No counterpart in the reference.  Same as gpu_evaluate_rule, for callers
  * that cannot allocate device memory while they evaluate: a host framework
  * that owns a fixed device-memory budget and forbids allocation per request,
@@ -159,12 +170,19 @@ int gpu_evaluate_rule_noalloc(void* ctx, const char* ruleText, GpuRuleResult* ou
  * their plans keep the layout of "block", so they reuse what batches learnt.
  * "rule_walk_budget": per-root measurement allowed per per-rule call.
  * "batch_chunks": pipelined chunks of gpu_evaluate_rules_batch (0 =
- * automatic).  Servers started afterwards: "serve_lanes"
+ * automatic).  "batch_phases": which phases batches prepared afterwards run
+ * on the device, 1 support, 2 body size, 3 both (default); a phase left out
+ * reads 0 (for timing one phase's launches alone).  Servers started afterwards: "serve_lanes"
  * (1: keep a heavy lane, default; 0: all slots alike), "serve_heavy_share"
  * (the heavy lane launches on 1/share of the blocks, default 2) and
  * "serve_heavy_us" (expected device time in microseconds above which a
- * request is heavy, default 5000).  Returns 0, or -1 for an unknown name or
- * value. */
+ * request is heavy, default 5000).  "dedup_budget": device bytes that one
+ * launch's global pair bitmaps may take (default 8 GiB); beyond it each
+ * body-size phase whose pairs do not fit shared memory uses either bitmap
+ * rows per resident block or pair keys sorted on the device, whichever
+ * moves fewer bytes (see gpu_batch_dedup).  "dedup_mode": 0 automatic, or
+ * force 1, 2 or 3 of gpu_batch_dedup's modes on every pair-counting phase
+ * (for tests).  Returns 0, or -1 for an unknown name or value. */
 int gpu_set_option(void* ctx, const char* name, long long value);
 
 /* ---- serving: continuous batching on a resident graph ---- */

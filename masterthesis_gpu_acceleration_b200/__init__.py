@@ -48,6 +48,7 @@ API_SYMBOLS = (
     "gpu_load_index",
     "gpu_batch_counts",
     "gpu_evaluate_rule_shard",
+    "gpu_batch_dedup",
     "gpu_last_error",
 )
 
@@ -130,6 +131,8 @@ def load_library(path: os.PathLike | str | None = None) -> ctypes.CDLL:
                                       ctypes.c_void_p, ctypes.c_longlong]
     lib.gpu_batch_counts.restype = ctypes.c_int
     lib.gpu_batch_counts.argtypes = [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p]
+    lib.gpu_batch_dedup.restype = ctypes.c_int
+    lib.gpu_batch_dedup.argtypes = [ctypes.c_void_p, ctypes.c_void_p, ctypes.POINTER(ctypes.c_longlong)]
     lib.gpu_evaluate_rule_shard.restype = ctypes.c_int
     lib.gpu_evaluate_rule_shard.argtypes = [ctypes.c_void_p, ctypes.c_char_p, ctypes.c_int, ctypes.c_int,
                                             ctypes.c_void_p]
@@ -344,6 +347,18 @@ class PreparedBatch:
         v = [ctypes.c_longlong() for _ in range(4)]
         self._lib.gpu_batch_info(self._h, *[ctypes.byref(x) for x in v])
         return dict(zip(("plans", "tasks", "h2d_bytes", "d2h_bytes"), (x.value for x in v)))
+
+    def dedup(self):
+        """(modes, sort keys): per rule, how its body size deduplicates pairs
+        in the current staging (gpu_batch_dedup: -1 none on the device, 0
+        shared bitmap, 1 global rows, 2 block rows, 3 sorted keys), and the
+        pair keys the last run appended."""
+        import numpy as np
+        m = np.zeros(max(self.n, 1), dtype=np.int32)
+        k = ctypes.c_longlong()
+        if self._lib.gpu_batch_dedup(self._h, m.ctypes.data, ctypes.byref(k)) != 0:
+            raise RuntimeError("gpu_batch_dedup failed")
+        return m[:self.n], k.value
 
     def autotune(self, rounds: int = 1) -> None:
         """Measure task times and rebalance the batch's tasks (see gpu_batch_autotune)."""

@@ -151,6 +151,23 @@ struct DevPlan {
     int32_t memoWords;            // words per memo bitmap (the rows of (memoP2, 1 - memoD2))
     const int32_t* memoTab;       // per hub row: memo slot or -1 (null: no memo)
     const uint32_t* memoBits;     // per slot: S1 then S2, memoWords words each
+    // kPairs deduplication outside the shared pool (per launch; see DedupMode):
+    int64_t gBlockWords;          // > 0: block rows, each block owns gBitmap + blockIdx.x * gBlockWords
+                                  // words for its current task's rows (cleared at task start)
+    unsigned long long* pairKeys;   // non-null: sort mode, keys keyBase | row << rankBits | rank appended
+    unsigned long long* keyCursor;  // sort mode: append cursor (keeps counting past keyCap)
+    unsigned long long keyCap;      // sort mode: capacity of pairKeys
+    unsigned long long keyBase;     // sort mode: the plan's key prefix (its sort index, shifted)
+    int32_t rankBits;               // sort mode: bits of the hO rank field
+    int32_t pad3;
+};
+
+// How a kPairs phase deduplicates its (hS row, hO rank) pairs.
+enum DedupMode : int32_t {
+    kDedupShared = 0,     // bitmap rows in the block's shared pool (the task's roots)
+    kDedupRows = 1,       // one global bitmap row per root of the phase, cleared before the launch
+    kDedupBlockRows = 2,  // global rows per resident block for its current task, cleared by the block
+    kDedupSort = 3,       // 64-bit pair keys appended, radix-sorted and counted once each
 };
 
 // A unit of device work: the roots [beg, end) of one plan.  A heavy root is

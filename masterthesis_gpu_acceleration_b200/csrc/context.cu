@@ -38,22 +38,136 @@ void set_error(const std::string& s) {
     std::fprintf(stderr, "[gpu_rules] %s\n", s.c_str());
 }
 
+namespace {
+// Bits that hold the values 0 .. n - 1 (at least one).
+int bits_for(uint64_t n) {
+    int b = 1;
+    while (b < 64 && n > 1 && ((n - 1) >> b) != 0) ++b;
+    return b;
+}
+constexpr unsigned long long kMaxSortKeys = 0xffffffffull;   // the sort's 32-bit positions
+}  // namespace
+
 void Staged::stage(Context& c, std::vector<DevPlan>& plans, const std::vector<const PhasePlan*>& phases,
-                   bool sortTasks, cudaStream_t s, double walkBudget, bool costAware) {
+                   bool sortTasks, cudaStream_t s, double walkBudget, bool costAware, bool allowSort) {
     nPlans = (int)plans.size();
     nTasks = 0;
     bitmapWords = 0;
+    blockWords = blockRegions = 0;
+    nSort = sortBits = sortSlotShift = 0;
+    keyCap = 0;
     h2dBytes = d2hBytes = 0;
+    dedup.assign(nPlans, kDedupShared);
+    const unsigned long long hint = keyHint;   // consumed by this staging
+    keyHint = 0;
+    if (hint > kMaxSortKeys) allowSort = false;
     if (!nPlans) return;
+
+    // ---- how each kPairs plan deduplicates ----
+    // Per-phase global rows (one bitmap row per root, cleared before the
+    // launch) while all of them fit the budget.  Beyond it, per plan: sort
+    // mode when the estimated keys (sorted in ~7 passes of 8 bits) cost fewer
+    // bytes than clearing and setting the rows, else block rows, whose
+    // memory grows with the launch's blocks instead of the phase's roots.
+    const size_t budgetWords = std::max<size_t>(c.dedupBudget / 4, 1);
+    std::vector<size_t> fullWords(nPlans, 0);
+    std::vector<double> est(nPlans, -1.0);
+    auto estimate = [&](int i) {
+        if (est[i] < 0) est[i] = std::max(1.0, c.tasks->work_estimate(*phases[i]));
+        return est[i];
+    };
+    size_t fullTotal = 0;
+    for (int i = 0; i < nPlans; ++i) {
+        if (plans[i].mode != kPairs || (!phases[i]->needsGlobalBitmap && c.dedupForce == 0)) continue;
+        fullWords[i] = (size_t)(phases[i]->rootEnd - phases[i]->rootBeg) * (size_t)std::max(plans[i].rowWords, 1);
+        fullTotal += fullWords[i];
+        dedup[i] = kDedupRows;
+    }
+    for (int i = 0; i < nPlans; ++i) {
+        if (dedup[i] == kDedupShared) continue;
+        if (c.dedupForce) {
+            dedup[i] = c.dedupForce;
+        } else if (fullTotal > budgetWords) {
+            const double e = estimate(i);
+            const double rowBytes = 4.0 * (double)fullWords[i] + 8.0 * e;
+            const double sortBytes = 8.0 * e * 22.0;
+            dedup[i] = (sortBytes < rowBytes && 16.0 * e <= (double)c.dedupBudget) ? kDedupSort : kDedupBlockRows;
+        }
+        if (dedup[i] == kDedupSort && !allowSort) dedup[i] = kDedupBlockRows;
+    }
+    // sort keys: [sort index | row | rank], at most 64 bits
+    std::vector<int32_t> sortPlans;
+    int rankBits = 1, rowBits = 1;
+    for (int i = 0; i < nPlans; ++i)
+        if (dedup[i] == kDedupSort) {
+            sortPlans.push_back(i);
+            rankBits = std::max(rankBits, bits_for((uint64_t)std::max(plans[i].wo, 1)));
+            rowBits = std::max(rowBits, bits_for((uint64_t)std::max(phases[i]->rootEnd - phases[i]->rootBeg, 1)));
+        }
+    if (!sortPlans.empty()) {
+        const int slotBits = sortPlans.size() > 1 ? bits_for(sortPlans.size()) : 0;
+        if (rankBits + rowBits + slotBits > 64) {
+            for (int i : sortPlans) dedup[i] = kDedupBlockRows;
+            sortPlans.clear();
+        } else {
+            nSort = (int)sortPlans.size();
+            sortSlotShift = rankBits + rowBits;
+            sortBits = sortSlotShift + slotBits;
+        }
+    }
+    if (nSort) {
+        // kept so that a run whose keys overflow can be staged again
+        inPlans = plans;
+        inPhases = phases;
+        inSortTasks = sortTasks;
+        inWalk = walkBudget;
+        inCostAware = costAware;
+        inAllowSort = allowSort;
+    } else {
+        inPlans.clear();
+        inPhases.clear();
+    }
+    // block rows: every resident block owns a region that holds its current
+    // task's rows; tasks are cut to the rows a region holds
+    std::vector<PhaseLimits> lim(nPlans);
+    {
+        size_t maxRow = 0;
+        for (int i = 0; i < nPlans; ++i)
+            if (dedup[i] == kDedupBlockRows) maxRow = std::max(maxRow, (size_t)std::max(plans[i].rowWords, 1));
+        if (maxRow) {
+            blockRegions = (size_t)std::max(c.grid, 1);
+            const size_t regionCap = std::max(maxRow, budgetWords / blockRegions);
+            size_t need = 0;
+            for (int i = 0; i < nPlans; ++i) {
+                if (dedup[i] != kDedupBlockRows) continue;
+                const size_t rw = (size_t)std::max(plans[i].rowWords, 1);
+                const int32_t g = (int32_t)std::max<size_t>(
+                    1, std::min<size_t>(regionCap / rw, (size_t)std::max(1, std::min(plans[i].cap, 512))));
+                lim[i].group = g;
+                lim[i].maxHeavy = (int32_t)std::min<size_t>(INT_MAX, budgetWords / 4 / rw);
+                need = std::max(need, (size_t)g * rw);
+            }
+            blockWords = (need + 3) & ~size_t(3);
+        }
+    }
     std::vector<size_t> gOff(nPlans, 0);
     for (int i = 0; i < nPlans; ++i) {
-        if (!phases[i]->needsGlobalBitmap) continue;
-        size_t rows = (size_t)(phases[i]->rootEnd - phases[i]->rootBeg);
+        if (dedup[i] != kDedupRows) continue;
         gOff[i] = bitmapWords;
-        bitmapWords += rows * (size_t)std::max(plans[i].rowWords, 1);   // word-aligned rows
+        bitmapWords += fullWords[i];   // word-aligned rows
     }
+    const size_t regionOff = (bitmapWords + 3) & ~size_t(3);   // 16-byte aligned regions
     cudaStream_t as = streamOrdered ? s : nullptr;
-    if (bitmapWords) dBitmap.ensure(bitmapWords * 4, as);
+    if (bitmapWords || blockWords) dBitmap.ensure((regionOff + blockRegions * blockWords) * 4, as);
+    if (nSort) {
+        double want = 0;
+        for (int i : sortPlans) want += estimate(i);
+        const double lo = 65536.0, hi = std::max(lo, (double)c.dedupBudget / 16.0);
+        keyCap = (unsigned long long)std::min(hi, std::max(lo, want));
+        keyCap = std::min(std::max(keyCap, hint), kMaxSortKeys);
+        dSort.ensure(256 + (size_t)keyCap * 16 + pairs_sort_hist_words(keyCap) * 4, as);
+        hSort.ensure(8);
+    }
     // suffix memos first: the task builder weighs memoised roots by them
     std::vector<std::array<int, 4>> memoKeys;
     for (int i = 0; i < nPlans; ++i)
@@ -63,13 +177,13 @@ void Staged::stage(Context& c, std::vector<DevPlan>& plans, const std::vector<co
         }
     if (!memoKeys.empty()) c.ensure_memos(memoKeys, s);
     std::vector<PhaseTasks> pts;
-    c.tasks->build(phases, c.grid, true, pts, walkBudget, costAware);
+    c.tasks->build(phases, c.grid, true, pts, walkBudget, costAware, &lim);
     std::vector<size_t> hOff(nPlans, 0);
     heavyWords = 0;
     for (int i = 0; i < nPlans; ++i) {
         plans[i].rowWords = plans[i].mode == kPairs ? (plans[i].wo + 31) / 32 : 1;
         hOff[i] = heavyWords;
-        heavyWords += (size_t)pts[i].heavyRows * plans[i].rowWords;
+        if (dedup[i] != kDedupSort) heavyWords += (size_t)pts[i].heavyRows * plans[i].rowWords;   // keys need no rows
     }
     if (heavyWords) dHeavy.ensure(heavyWords * 4, as);
     std::vector<DevTask> tasks;
@@ -87,9 +201,28 @@ void Staged::stage(Context& c, std::vector<DevPlan>& plans, const std::vector<co
             }
         }
         plans[i].resultSlot = i;
-        plans[i].gBitmap = phases[i]->needsGlobalBitmap ? static_cast<uint32_t*>(dBitmap.p) + gOff[i] : nullptr;
-        plans[i].gRowBase = phases[i]->needsGlobalBitmap ? phases[i]->rootBeg : 0;
-        plans[i].gHeavy = pts[i].heavyRows ? static_cast<uint32_t*>(dHeavy.p) + hOff[i] : nullptr;
+        const int dm = dedup[i];
+        uint32_t* gb = static_cast<uint32_t*>(dBitmap.p);
+        plans[i].gBitmap = dm == kDedupRows ? gb + gOff[i] : (dm == kDedupBlockRows ? gb + regionOff : nullptr);
+        plans[i].gRowBase = (dm == kDedupRows || dm == kDedupSort) ? phases[i]->rootBeg : 0;
+        plans[i].gBlockWords = dm == kDedupBlockRows ? (int64_t)blockWords : 0;
+        plans[i].gHeavy = (pts[i].heavyRows && dm != kDedupSort) ? static_cast<uint32_t*>(dHeavy.p) + hOff[i] : nullptr;
+        plans[i].pairKeys = nullptr;
+        plans[i].keyCursor = nullptr;
+        plans[i].keyCap = 0;
+        plans[i].keyBase = 0;
+        plans[i].rankBits = 0;
+        if (dm == kDedupSort) {
+            const int k = (int)(std::find(sortPlans.begin(), sortPlans.end(), i) - sortPlans.begin());
+            char* sb = static_cast<char*>(dSort.p);
+            plans[i].keyCursor = reinterpret_cast<unsigned long long*>(sb);
+            plans[i].pairKeys = reinterpret_cast<unsigned long long*>(sb + 256);
+            plans[i].keyCap = keyCap;
+            plans[i].keyBase = (unsigned long long)k << sortSlotShift;
+            plans[i].rankBits = rankBits;
+            plans[i].memoTab = nullptr;   // memos set bitmap words; keys carry every pair
+            plans[i].memoBits = nullptr;
+        }
         tasks.insert(tasks.end(), pts[i].tasks.begin(), pts[i].tasks.end());
         cost.insert(cost.end(), pts[i].cost.begin(), pts[i].cost.end());
     }
@@ -144,10 +277,11 @@ void Staged::stage(Context& c, std::vector<DevPlan>& plans, const std::vector<co
     }
     size_t planBytes = (size_t)nPlans * sizeof(DevPlan);
     size_t taskBytes = (size_t)nTasks * sizeof(DevTask);
-    size_t blob = planBytes + taskBytes;
+    size_t blob = planBytes + taskBytes + (size_t)nSort * sizeof(int32_t);
     hBlob.ensure(blob);
     std::memcpy(hBlob.p, plans.data(), planBytes);
     std::memcpy(static_cast<char*>(hBlob.p) + planBytes, tasks.data(), taskBytes);
+    if (nSort) std::memcpy(static_cast<char*>(hBlob.p) + planBytes + taskBytes, sortPlans.data(), nSort * sizeof(int32_t));
     hTasks = std::move(tasks);   // kept for profiles and task-time learning
     hCost = std::move(cost);
     dBlob.ensure(blob, as);
@@ -158,6 +292,8 @@ void Staged::stage(Context& c, std::vector<DevPlan>& plans, const std::vector<co
     ck(cudaMemcpyAsync(dBlob.p, hBlob.p, blob, cudaMemcpyHostToDevice, s), "H2D plans");
     dPlans = static_cast<const DevPlan*>(dBlob.p);
     dTasks = reinterpret_cast<const DevTask*>(static_cast<const char*>(dBlob.p) + planBytes);
+    dSortSlots = nSort ? reinterpret_cast<const int32_t*>(static_cast<const char*>(dBlob.p) + planBytes + taskBytes)
+                       : nullptr;
     h2dBytes = blob;
     d2hBytes = (size_t)nPlans * sizeof(unsigned long long) + 8;
 }
@@ -253,12 +389,33 @@ void Context::ensure_memos(const std::vector<std::array<int, 4>>& keys, cudaStre
     ck(cudaStreamSynchronize(s), "memo build");   // memos are shared by every stream afterwards
 }
 
+void Staged::enqueue_sort(Context& c, cudaStream_t s, unsigned long long* results, int* status) {
+    if (!nSort) return;
+    char* base = static_cast<char*>(dSort.p);
+    auto* cursor = reinterpret_cast<unsigned long long*>(base);
+    auto* keys = reinterpret_cast<unsigned long long*>(base + 256);
+    auto* tmp = keys + keyCap;
+    auto* hist = reinterpret_cast<uint32_t*>(tmp + keyCap);
+    ck(pairs_sort_count(keys, tmp, cursor, keyCap, sortBits, sortSlotShift, dSortSlots, nSort, results, status,
+                        hist, std::max(c.sms, 1) * 8, s),
+       "pair sort");
+}
+
+void Staged::restage(Context& c, cudaStream_t s) {
+    if (!nSort) return;
+    keyHint = *static_cast<const unsigned long long*>(hSort.p);
+    std::vector<DevPlan> p = inPlans;
+    std::vector<const PhasePlan*> ph = inPhases;
+    stage(c, p, ph, inSortTasks, s, inWalk, inCostAware, inAllowSort);
+}
+
 void Staged::enqueue(Context& c, cudaStream_t s, int instr, int gridCap) {
     if (!nPlans) return;
     ck(cudaMemsetAsync(dResults.p, 0, (size_t)nPlans * sizeof(unsigned long long), s), "memset results");
     ck(cudaMemsetAsync(dCtl.p, 0, 8, s), "memset ctl");
     if (bitmapWords) ck(cudaMemsetAsync(dBitmap.p, 0, bitmapWords * 4, s), "memset bitmap");
     if (heavyWords) ck(cudaMemsetAsync(dHeavy.p, 0, heavyWords * 4, s), "memset heavy rows");
+    if (nSort) ck(cudaMemsetAsync(dSort.p, 0, 8, s), "memset key cursor");
     EngineProfile prof;
     if (instr >= 1) {
         dTaskNs.ensure((size_t)std::max(nTasks, 1) * 16, streamOrdered ? s : nullptr);
@@ -270,10 +427,12 @@ void Staged::enqueue(Context& c, cudaStream_t s, int instr, int gridCap) {
         prof.bytes = static_cast<unsigned long long*>(dBytes.p);
     }
     int grid = std::max(1, std::min(nTasks, gridCap > 0 ? std::min(gridCap, c.grid) : c.grid));
+    if (blockWords && (size_t)grid > blockRegions) throw CudaError("launch grid exceeds the block-row regions");
     ck(engine_launch(c.dix, dPlans, dTasks, nTasks, static_cast<int*>(dCtl.p),
                      static_cast<unsigned long long*>(dResults.p), static_cast<int*>(dCtl.p) + 1, grid,
                      c.geom.block, s, instr ? &prof : nullptr),
        "engine launch");
+    enqueue_sort(c, s, static_cast<unsigned long long*>(dResults.p), static_cast<int*>(dCtl.p) + 1);
 }
 
 void Staged::enqueue_per_plan(Context& c, cudaStream_t s) {
@@ -285,22 +444,26 @@ void Staged::enqueue_per_plan(Context& c, cudaStream_t s) {
     ck(cudaMemsetAsync(dCtl.p, 0, 64, s), "memset ctl");
     if (bitmapWords) ck(cudaMemsetAsync(dBitmap.p, 0, bitmapWords * 4, s), "memset bitmap");
     if (heavyWords) ck(cudaMemsetAsync(dHeavy.p, 0, heavyWords * 4, s), "memset heavy rows");
+    if (nSort) ck(cudaMemsetAsync(dSort.p, 0, 8, s), "memset key cursor");
     int* ctl = static_cast<int*>(dCtl.p);
     for (int i = 0; i < nPlans; ++i) {
         const int32_t b = i ? planTaskEnd[i - 1] : 0, e = planTaskEnd[i];
         EngineProfile prof;
         prof.span = reinterpret_cast<unsigned long long*>(static_cast<char*>(dCtl.p) + 16 + 16 * i);
         const int grid = std::max(1, std::min(e - b, c.grid));
+        if (blockWords && (size_t)grid > blockRegions) throw CudaError("launch grid exceeds the block-row regions");
         ck(engine_launch(c.dix, dPlans, dTasks + b, e - b, ctl + i,
                          reinterpret_cast<unsigned long long*>(static_cast<char*>(dCtl.p) + kPerPlanResults), ctl + 2,
                          grid, c.geom.block, s, &prof),
            "engine launch");
     }
+    enqueue_sort(c, s, reinterpret_cast<unsigned long long*>(static_cast<char*>(dCtl.p) + kPerPlanResults), ctl + 2);
 }
 
 void Staged::download_spans(cudaStream_t s) {
     if (!nPlans) return;
     ck(cudaMemcpyAsync(hCtl.p, dCtl.p, 64, cudaMemcpyDeviceToHost, s), "D2H control words");
+    download_cursor(s);
 }
 
 void compose(const RulePlan& rp, int64_t sup, int64_t body, double supMs, double confMs, GpuRuleResult* out) {
@@ -324,12 +487,16 @@ namespace {
 int64_t run_one_phase(Context& c, const PhasePlan& ph, float* ms) {
     std::vector<DevPlan> plans{ph.plan};
     c.one.stage(c, plans, {&ph}, false, c.stream, c.ruleWalkBudget, true);
-    ck(cudaEventRecord(c.ev[0], c.stream), "event");
-    c.one.enqueue(c, c.stream, 0);
-    ck(cudaEventRecord(c.ev[1], c.stream), "event");
-    c.one.download(c.stream);
-    ck(cudaStreamSynchronize(c.stream), "engine");
-    c.one.check_status();
+    for (int attempt = 0;; ++attempt) {
+        ck(cudaEventRecord(c.ev[0], c.stream), "event");
+        c.one.enqueue(c, c.stream, 0);
+        ck(cudaEventRecord(c.ev[1], c.stream), "event");
+        c.one.download(c.stream);
+        ck(cudaStreamSynchronize(c.stream), "engine");
+        c.one.check_status();
+        if (attempt > 0 || !c.one.sort_overflow()) break;
+        c.one.restage(c, c.stream);   // the exact key count is known now
+    }
     ck(cudaEventElapsedTime(ms, c.ev[0], c.ev[1]), "elapsed");
     return (int64_t)c.one.counts()[0];
 }
@@ -365,9 +532,13 @@ int evaluate_parsed(Context& c, const Rule& rule, GpuRuleResult* out) {
     if (!plans.empty()) {
         // one upload, one launch per phase (each timed on the device), one download
         c.one.stage(c, plans, phases, false, c.stream, c.ruleWalkBudget, true);
-        with_rule_block(c, [&] { c.one.enqueue_per_plan(c, c.stream); });
-        c.one.download_spans(c.stream);
-        ck(cudaStreamSynchronize(c.stream), "engine");
+        for (int attempt = 0;; ++attempt) {
+            with_rule_block(c, [&] { c.one.enqueue_per_plan(c, c.stream); });
+            c.one.download_spans(c.stream);
+            ck(cudaStreamSynchronize(c.stream), "engine");
+            if (attempt > 0 || !c.one.sort_overflow()) break;
+            c.one.restage(c, c.stream);   // the exact key count is known now
+        }
         if (static_cast<const int*>(c.one.hCtl.p)[2] != 0)
             throw CudaError("engine reported internal status " + std::to_string(static_cast<const int*>(c.one.hCtl.p)[2]));
         int k = 0;
@@ -443,7 +614,7 @@ void prepare(Batch& b, Context& c, const char* const* rules, int n, int isJson, 
         if (rp.status != kRuleOk) continue;
         for (int k = 0; k < 2; ++k) {
             const PhasePlan& ph = k == 0 ? rp.support : rp.body;
-            if (ph.how != kDevice) continue;
+            if (ph.how != kDevice || !(c.batchPhases & (1 << k))) continue;
             // identical computations (same plan and roots, e.g. one body under
             // several heads) run once; the others share the count
             // keyed by hash, confirmed by the full signature (plans are
@@ -495,7 +666,12 @@ void collect(const Batch& b, GpuRuleResult* out, int* status) {
 
 // Runs a prepared batch: optional L2 flush (untimed), then the device work
 // between two events, then the result download.
-void run_batch(Batch& b, bool useGraph, size_t flushBytes) {
+void drop_graph(Batch& b) {
+    if (b.exec) { cudaGraphExecDestroy(b.exec); b.exec = nullptr; }
+    if (b.graph) { cudaGraphDestroy(b.graph); b.graph = nullptr; }
+}
+
+void run_batch(Batch& b, bool useGraph, size_t flushBytes, bool retried = false) {
     Context& c = *b.c;
     if (flushBytes) {
         b.flush.ensure(flushBytes);
@@ -514,6 +690,14 @@ void run_batch(Batch& b, bool useGraph, size_t flushBytes) {
     b.st.download(b.stream);
     ck(cudaStreamSynchronize(b.stream), "engine");
     b.st.check_status();
+    if (!retried && b.st.sort_overflow()) {
+        // sort-mode keys outgrew the estimate: stage again with the exact
+        // count (the next runs fit) and run once more
+        b.st.restage(c, b.stream);
+        drop_graph(b);
+        run_batch(b, useGraph, flushBytes, true);
+        return;
+    }
     float ms = 0.f;
     ck(cudaEventElapsedTime(&ms, b.ev0, b.ev1), "elapsed");
     b.lastMs = ms;
@@ -690,6 +874,15 @@ int gpu_evaluate_rules_batch(void* ctx, const char* const* rules, int n, int isJ
             Batch& b = *c.pipe[k];
             ck(cudaStreamSynchronize(b.stream), "engine");
             b.st.check_status();
+            if (b.st.sort_overflow()) {   // run this chunk again with the exact key count
+                b.st.restage(c, b.stream);
+                ck(cudaEventRecord(b.ev0, b.stream), "event");
+                b.st.enqueue(c, b.stream, 0);
+                ck(cudaEventRecord(b.ev1, b.stream), "event");
+                b.st.download(b.stream);
+                ck(cudaStreamSynchronize(b.stream), "engine");
+                b.st.check_status();
+            }
             float ms = 0.f;
             ck(cudaEventElapsedTime(&ms, c.pipe[0]->ev0, b.ev1), "elapsed");
             span = std::max(span, ms);
@@ -700,6 +893,15 @@ int gpu_evaluate_rules_batch(void* ctx, const char* const* rules, int n, int isJ
         return 0;
     } catch (const std::exception& e) {
         set_error(std::string("gpu_evaluate_rules_batch error: ") + e.what());
+        // no chunk may still be writing into the reused buffers, and the
+        // caller sees no partial results
+        for (Batch* b : c.pipe)
+            if (b && b->stream) cudaStreamSynchronize(b->stream);
+        cudaGetLastError();
+        for (int i = 0; i < n; ++i) {
+            out[i] = GpuRuleResult{};
+            if (status) status[i] = -1;
+        }
         return -1;
     }
 }
@@ -789,6 +991,22 @@ int gpu_batch_info(void* batch, long long* plans, long long* tasks, long long* h
     return 0;
 }
 
+int gpu_batch_dedup(void* batch, int* modes, long long* sortKeys) {
+    if (!batch || !modes) return -1;
+    const Batch& b = *static_cast<const Batch*>(batch);
+    for (int i = 0; i < b.n; ++i) modes[i] = -1;
+    // the body-size phase (owner rule * 2 + 1) of each rule whose body size
+    // counts pairs on the device
+    auto put = [&](int owner, int plan) {
+        if (owner % 2 != 1 || plan < 0 || plan >= (int)b.st.dedup.size() || plan >= (int)b.phases.size()) return;
+        if (b.phases[plan]->plan.mode == kPairs) modes[owner / 2] = b.st.dedup[plan];
+    };
+    for (size_t k = 0; k < b.owner.size(); ++k) put(b.owner[k], (int)k);
+    for (const auto& sh : b.shared) put(sh.first, sh.second);
+    if (sortKeys) *sortKeys = b.st.nSort ? (long long)*static_cast<const unsigned long long*>(b.st.hSort.p) : 0;
+    return 0;
+}
+
 int gpu_batch_count_bytes(void* batch, unsigned long long* bytes) {
     return gpu_batch_profile(batch, bytes, nullptr, nullptr, 0);
 }
@@ -835,8 +1053,7 @@ int gpu_batch_autotune(void* batch, int rounds) {
             ck(cudaMemcpyAsync(ns.data(), b.st.dTaskNs.p, ns.size() * 8, cudaMemcpyDeviceToHost, b.stream), "D2H task times");
             ck(cudaStreamSynchronize(b.stream), "autotune");
             c.tasks->learn(b.phases, b.st.hTasks, b.st.hCost, ns.data(), c.grid);
-            if (b.exec) { cudaGraphExecDestroy(b.exec); b.exec = nullptr; }
-            if (b.graph) { cudaGraphDestroy(b.graph); b.graph = nullptr; }
+            drop_graph(b);
             std::vector<DevPlan> pl = b.plans0;
             b.st.stage(c, pl, b.phases, true, b.stream, b.walkBudget);
             ck(cudaStreamSynchronize(b.stream), "restage");
@@ -864,6 +1081,12 @@ int gpu_set_option(void* ctx, const char* name, long long value) {
     }
     if (n == "serve_heavy_share" && value >= 1 && value <= 16) { c.serveHeavyShare = (int)value; return 0; }
     if (n == "serve_heavy_us" && value >= 0) { c.serveHeavyNs = 1e3 * (double)value; return 0; }
+    if (n == "batch_phases" && value >= 1 && value <= 3) { c.batchPhases = (int)value; return 0; }
+    if (n == "dedup_budget" && value >= 4096) { c.dedupBudget = (size_t)value; return 0; }
+    if (n == "dedup_mode" && (value == 0 || value == kDedupRows || value == kDedupBlockRows || value == kDedupSort)) {
+        c.dedupForce = (int)value;
+        return 0;
+    }
     return -1;
 }
 

@@ -30,6 +30,13 @@ cudaError_t memo_build(const DevIndex& ix, const MemoJob* jobs, int nJobs, cudaS
 cudaError_t engine_launch(const DevIndex& ix, const DevPlan* plans, const DevTask* tasks, int nTasks,
                           int* taskCounter, unsigned long long* results, int* status, int grid, int block,
                           cudaStream_t stream, const EngineProfile* prof);
+// Sort mode (sort.cu): radix sort of the appended pair keys and the count of
+// each plan's distinct keys into its result slot.
+size_t pairs_sort_hist_words(unsigned long long cap);
+cudaError_t pairs_sort_count(unsigned long long* keys, unsigned long long* tmp, const unsigned long long* count,
+                             unsigned long long cap, int bits, int slotShift, const int32_t* slotOf, int nSlots,
+                             unsigned long long* results, int* status, uint32_t* hist, int grid,
+                             cudaStream_t stream);
 
 // Records the calling thread's last error (gpu_last_error) and logs it.
 void set_error(const std::string& s);
@@ -100,7 +107,7 @@ struct Context;
 // A set of plans and their tasks resident on the device, with the buffers
 // one launch over them needs.
 struct Staged {
-    DevBuf dBlob, dResults, dCtl, dBitmap, dHeavy, dBytes, dTaskNs;
+    DevBuf dBlob, dResults, dCtl, dBitmap, dHeavy, dBytes, dTaskNs, dSort;
     std::vector<DevTask> hTasks;  // task list as uploaded (for profiles)
     std::vector<double> hCost;    // estimated work per uploaded task
     HostBuf hBlob, hResults, hCtl;
@@ -112,10 +119,40 @@ struct Staged {
     bool streamOrdered = false;   // grow device buffers on the launch stream (serving slots)
     std::vector<int32_t> planTaskEnd;   // tasks in plan order (unsorted staging): end of each plan's tasks
 
+    // Deduplication of kPairs plans (DedupMode per plan).  Per-phase global
+    // rows while all of them fit the context's budget; beyond it, per plan,
+    // block rows (each resident block owns `blockWords` words after the
+    // per-phase rows in dBitmap, `blockRegions` regions) or sort mode (keys
+    // in dSort: [cursor | keys | tmp | histogram]), whichever the byte
+    // estimate favours.
+    std::vector<int32_t> dedup;
+    size_t blockWords = 0, blockRegions = 0;
+    int nSort = 0, sortBits = 0, sortSlotShift = 0;
+    unsigned long long keyCap = 0;
+    unsigned long long keyHint = 0;     // exact keys of a run that overflowed keyCap
+    const int32_t* dSortSlots = nullptr;   // result slot of each sort index (in dBlob)
+    HostBuf hSort;                      // the downloaded append cursor
+    // inputs of the last staging, kept while it has sort-mode plans so that
+    // an overflowing run can be staged again with the exact key count
+    std::vector<DevPlan> inPlans;
+    std::vector<const PhasePlan*> inPhases;
+    bool inSortTasks = true, inCostAware = false, inAllowSort = true;
+    double inWalk = 4.0e6;
+
     // walkBudget: how much per-root measurement the task builder may do
     // (prepared batches afford more than one-shot or served launches).
+    // allowSort: sort mode may be chosen (launches that can be run again
+    // when the key buffer overflows; the serving loop cannot).
     void stage(Context& c, std::vector<DevPlan>& plans, const std::vector<const PhasePlan*>& phases,
-               bool sortTasks, cudaStream_t s, double walkBudget = 4.0e6, bool costAware = false);
+               bool sortTasks, cudaStream_t s, double walkBudget = 4.0e6, bool costAware = false,
+               bool allowSort = true);
+    // After download + synchronisation: whether sort-mode keys exceeded the
+    // buffer (the counts are then incomplete).  restage() stages the same
+    // plans again with a buffer of the exact size (one upload, no launch).
+    bool sort_overflow() const {
+        return nSort > 0 && *static_cast<const unsigned long long*>(hSort.p) > keyCap;
+    }
+    void restage(Context& c, cudaStream_t s);
     // instr: 0 plain, 1 task times into dTaskNs, 2 also algorithmic bytes
     // into dBytes.  gridCap > 0 limits the launch to that many blocks (a
     // share of the SMs).
@@ -160,7 +197,14 @@ struct Staged {
         if (!nPlans) return;
         ck(cudaMemcpyAsync(hResults.p, dResults.p, nPlans * sizeof(unsigned long long), cudaMemcpyDeviceToHost, s), "D2H results");
         ck(cudaMemcpyAsync(hCtl.p, dCtl.p, 8, cudaMemcpyDeviceToHost, s), "D2H status");
+        download_cursor(s);
     }
+    void download_cursor(cudaStream_t s) {
+        if (nSort) ck(cudaMemcpyAsync(hSort.p, dSort.p, 8, cudaMemcpyDeviceToHost, s), "D2H key cursor");
+    }
+    // Sort and count the keys of the launch(es) just enqueued on s into
+    // `results` (per result slot); bad keys are flagged in `status`.
+    void enqueue_sort(Context& c, cudaStream_t s, unsigned long long* results, int* status);
     const unsigned long long* counts() const { return static_cast<const unsigned long long*>(hResults.p); }
     void check_status() const {
         if (nPlans && static_cast<const int*>(hCtl.p)[1] != 0)
@@ -196,6 +240,7 @@ struct Context {
     Geom geom;
     double ruleWalkBudget = 4.0e6;   // per-root measurement allowed per plain per-rule launch
     int batchChunks = 0;             // pipelined chunks of one-shot batches (0: automatic)
+    int batchPhases = 3;             // phases batches run on the device: 1 support, 2 body size, 3 both
     // suffix memos: a hub row gets one when its suffix candidates are at
     // least memoGain x the memo's words (negative: no memos)
     double memoGain = 0.25;
@@ -213,6 +258,12 @@ struct Context {
     int serveLanes = 1;        // servers started on this context keep a heavy lane
     int serveHeavyShare = 2;   // the heavy lane launches on grid / serveHeavyShare blocks
     double serveHeavyNs = 5.0e6;
+    // kPairs deduplication beyond the shared pool: device bytes that the
+    // global dedup buffers of one launch may take before block rows or sort
+    // mode replace per-phase rows, and a forced mode for every kPairs plan
+    // (0: automatic; else a DedupMode other than kDedupShared).
+    size_t dedupBudget = size_t(8) << 30;
+    int dedupForce = 0;
     int grid = 0;
     int sms = 0;
     std::unique_ptr<RuleParser> parser;

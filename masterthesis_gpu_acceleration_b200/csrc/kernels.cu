@@ -33,6 +33,7 @@
 // The reference's kernels (GPU_03/gpu_kernels.cuh:34-443) run one thread
 // per head triple or per first-atom triple with template-unrolled
 // recursion; this engine replaces them as a whole.
+#include <cooperative_groups.h>
 #include <cuda_runtime.h>
 
 #include <cstdint>
@@ -40,6 +41,8 @@
 #include "common.hpp"
 
 namespace gr {
+
+namespace cg = cooperative_groups;
 
 // Counts the global-memory bytes the algorithm requests (the roofline's
 // algorithmic bytes).  Compiled out of the timed kernel.
@@ -55,8 +58,7 @@ template <int B>
 struct BlockState {
     static constexpr int kWarps = B / 32;
     int task;
-    int k;
-    int curItem[kMaxBody + 1];
+    int curItem[kMaxBody + 1];      // a level's position, saved when the search descends below it
     long long curOff[kMaxBody + 1];
     int count[kMaxBody + 1];
     int levelOff[kMaxBody + 1];
@@ -71,7 +73,7 @@ struct Smem {
     BlockState<B> st;
     int wBeg[B];
     long long wLen[B];
-    long long wPre[B];
+    long long wLoc[B];   // inclusive prefix of wLen within the item's warp
     int pool[Geom::pool_for(B)];   // frontier levels, then the dedup bitmap at plan.bitmapOff
 };
 
@@ -141,25 +143,53 @@ __device__ __forceinline__ int2 step_segment(const DevPlan& P, const DevIndex& i
     return make_int2(__ldg(ix.predEdge[0] + st.pred), __ldg(ix.predEdge[0] + st.pred + 1));
 }
 
-// Inclusive block scan of one 64-bit value per thread.
 template <int B>
-__device__ __forceinline__ long long block_scan(long long x, BlockState<B>& st) {
-    static_assert(B / 32 <= 32, "one lane per warp total");
+struct Smem;
+
+// Publishes a window's prefix sums with one barrier: every thread stores
+// the inclusive sum of x over its warp's threads up to itself (wLoc) and
+// every warp its total (warpSum), so item i's block-wide prefix is the
+// totals of the warps before i's warp plus wLoc[i] (WinCursor reads it
+// that way).  The barrier also ORs `flag` over the block.
+template <int B>
+__device__ __forceinline__ bool publish_window(long long x, bool flag, Smem<B>& sm) {
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
 #pragma unroll
     for (int d = 1; d < 32; d <<= 1) {
         const long long y = __shfl_up_sync(0xffffffffu, x, d);
         if (lane >= d) x += y;
     }
-    if (lane == 31) st.warpSum[warp] = x;
-    __syncthreads();
-    // every warp adds up the totals of the warps before it itself (at most
-    // 16 values), which saves the second barrier of a two-level scan
-    long long w = lane < warp ? st.warpSum[lane] : 0;
-#pragma unroll
-    for (int d = 16; d; d >>= 1) w += __shfl_xor_sync(0xffffffffu, w, d);
-    return x + w;
+    sm.wLoc[threadIdx.x] = x;
+    if (lane == 31) sm.st.warpSum[warp] = x;
+    return __syncthreads_or(flag) != 0;
 }
+
+// The window item that holds candidate j, for j that never decreases:
+// whole warps are stepped over by their totals, then the item is searched
+// among its warp's 32 prefixes, starting after the previous item (a hub's
+// long segment costs one probe per candidate).
+template <int B>
+struct WinCursor {
+    int item = 0, warp = 0;
+    long long base = 0;   // candidates of the warps before `warp`
+    __device__ __forceinline__ void seek(const Smem<B>& sm, int nw, long long j) {
+        if (base + sm.wLoc[item] > j) return;
+        long long end = base + sm.st.warpSum[warp];
+        while (end <= j) {
+            base = end;
+            ++warp;
+            end = base + sm.st.warpSum[warp];
+        }
+        int lo = max(item + 1, warp * 32), hi = min(nw, warp * 32 + 32) - 1;
+        while (lo < hi) {
+            const int mid = (lo + hi) >> 1;
+            if (base + sm.wLoc[mid] > j) hi = mid; else lo = mid + 1;
+        }
+        item = lo;
+    }
+    // index of the item's first candidate
+    __device__ __forceinline__ long long first(const Smem<B>& sm) const { return base + sm.wLoc[item] - sm.wLen[item]; }
+};
 
 template <int B>
 __device__ __forceinline__ unsigned long long block_sum(unsigned long long x, BlockState<B>& st) {
@@ -321,6 +351,20 @@ __device__ __noinline__ int classify_item(const DevPlan& P, const DevIndex& ix, 
     return -3;
 }
 
+// Sort mode: appends the pair key of (row, rank) to the plan's key buffer.
+// The threads that emit together take consecutive slots with one atomic; the
+// cursor keeps counting past the capacity, so the host learns the exact
+// number of keys when they did not fit (and runs again with that size).
+__device__ __forceinline__ void emit_pair(const DevPlan& P, long long row, int rank) {
+    const unsigned long long key = P.keyBase | ((unsigned long long)row << P.rankBits) | (unsigned)rank;
+    cg::coalesced_group g = cg::coalesced_threads();
+    unsigned long long base = 0;
+    if (g.thread_rank() == 0) base = atomicAdd(P.keyCursor, (unsigned long long)g.size());
+    base = g.shfl(base, 0);
+    const unsigned long long slot = base + g.thread_rank();
+    if (slot < P.keyCap) P.pairKeys[slot] = key;
+}
+
 template <int B, bool kC>
 __device__ __forceinline__ void run_task(Smem<B>& sm, const DevIndex& ix, const DevTask& task,
                                          unsigned long long* results, int* status, Meter<kC>& mt) {
@@ -337,12 +381,19 @@ __device__ __forceinline__ void run_task(Smem<B>& sm, const DevIndex& ix, const 
     // row for both the pair bits and the found bit; counting happens on
     // insertion so that the slices of one root count each result once.
     const bool heavy = task.gRow >= 0;
-    const bool shared = !heavy && !(pairs && P.gBitmap);
+    // Sort mode appends pair keys instead of setting bits (no bitmap at
+    // all); block rows keep the task's rows in the block's own region of a
+    // global buffer instead of one row per root of the phase.
+    const bool sortMode = pairs && P.pairKeys != nullptr;
+    const bool blockRows = pairs && !heavy && !sortMode && P.gBlockWords > 0;
+    const bool shared = !heavy && !(pairs && (P.gBitmap || sortMode));
     uint32_t* sbits = reinterpret_cast<uint32_t*>(sm.pool + P.bitmapOff);
     int* const items = sm.pool;
-    uint32_t* bm = heavy ? P.gHeavy + (long long)task.gRow * P.rowWords : (shared ? sbits : P.gBitmap);
+    uint32_t* bm = heavy ? (P.gHeavy ? P.gHeavy + (long long)task.gRow * P.rowWords : nullptr)
+                         : (shared ? sbits : (blockRows ? P.gBitmap + (long long)blockIdx.x * P.gBlockWords : P.gBitmap));
     uint32_t* fb = heavy ? bm : sbits;   // kExist found bits
-    const long long rowBase = (heavy || shared) ? 0 : (long long)task.beg - P.gRowBase;
+    const long long rowBase = (heavy || shared || blockRows) ? 0 : (long long)task.beg - P.gRowBase;
+    const long long keyRow0 = (long long)task.beg - P.gRowBase;   // sort mode: key row of the task's root 0
 
     // clear the task's shared dedup bits
     // pair rows are word-aligned: row r occupies words [r * rowWords, (r + 1) * rowWords)
@@ -350,8 +401,18 @@ __device__ __forceinline__ void run_task(Smem<B>& sm, const DevIndex& ix, const 
     const int nWords = heavy ? 0 : (shared ? (int)(pairs ? (long long)G * P.rowWords : ((G + 31) >> 5))
                                            : (pairs ? 0 : ((G + 31) >> 5)));
     for (int i = tid; i < nWords; i += B) sbits[i] = 0u;
+    if (blockRows && (long long)G * P.rowWords > P.gBlockWords) {   // the task builder keeps tasks this small
+        if (tid == 0) atomicOr(status, 32);
+        return;
+    }
+    if (blockRows) {
+        // the region is 16-byte aligned and a whole number of uint4 long
+        uint4* b4 = reinterpret_cast<uint4*>(bm);
+        const long long n4 = ((long long)G * P.rowWords + 3) >> 2;
+        for (long long i = tid; i < n4; i += B) b4[i] = make_uint4(0u, 0u, 0u, 0u);
+        if (tid == 0) mt.add(16 * (unsigned long long)n4);
+    }
     if (tid == 0) {
-        S.k = 0;
         int off = 0;
         for (int l = 0; l <= kMaxBody; ++l) {
             S.curItem[l] = 0;
@@ -434,15 +495,22 @@ __device__ __forceinline__ void run_task(Smem<B>& sm, const DevIndex& ix, const 
             if (heavy && !(old & (1u << (root & 31)))) myNew++;
         }
     } else {
+        // The search position (level k, first window item w0, candidates of
+        // that item consumed already) is kept alike in every thread's
+        // registers; a level's position goes to shared memory only when the
+        // search descends below it.  A round takes two barriers: one
+        // publishes the window's prefix sums, one closes the round.  Reads
+        // of the shared counters that a later step may reset can only see
+        // the reset when the decision they feed is the same either way.
+        int k = 0, w0 = 0;
+        long long off = 0;
         for (;;) {
-            __syncthreads();
-            const int k = S.k;
-            const int w0 = S.curItem[k];
             const int cnt = min(S.count[k], P.cap);
             if (w0 >= cnt) {
                 if (k == 0) break;
-                __syncthreads();
-                if (tid == 0) S.k = k - 1;
+                --k;
+                w0 = S.curItem[k];
+                off = S.curOff[k];
                 continue;
             }
             const int nw = min(B, cnt - w0);
@@ -457,13 +525,13 @@ __device__ __forceinline__ void run_task(Smem<B>& sm, const DevIndex& ix, const 
             // injectivity, an item whose segment is a whole hub row is
             // counted by OR-ing the row's rank bitmap into its pair row (32
             // candidates per word) instead of candidate by candidate.
-            const bool hubPath = leaf && pairs && stp.hoWhich != 0 && stp.kind == kExpand && stp.nNew == 1 &&
-                                 !hasFilters && ix.nHub > 0 && !(heavy && k == 0);
+            const bool hubPath = leaf && pairs && !sortMode && stp.hoWhich != 0 && stp.kind == kExpand &&
+                                 stp.nNew == 1 && !hasFilters && ix.nHub > 0 && !(heavy && k == 0);
             // Memo path: the plan ends in two expand steps x -> y -> hO with
             // nothing but injectivity to test; an item whose first segment
             // is a hub row with a suffix memo is counted from the memo's
             // "one witness y" / "two witnesses y" bitmaps (see below).
-            const bool memoPath = !leaf && pairs && P.memoTab != nullptr && k + 1 == P.memoLevel;
+            const bool memoPath = !leaf && pairs && !sortMode && P.memoTab != nullptr && k + 1 == P.memoLevel;
             const bool existMemo = leaf && !pairs && P.memoTab != nullptr && k + 1 == P.memoLevel &&
                                    !(heavy && k == 0);
             bool isHub = false;   // item marked for the hub or memo pass
@@ -477,7 +545,7 @@ __device__ __forceinline__ void run_task(Smem<B>& sm, const DevIndex& ix, const 
                 if (!pairs) {
                     pruned = (fb[it[0] >> 5] >> (it[0] & 31)) & 1u;
                     if (heavy) mt.add(4);
-                } else if (itemHasRank) {
+                } else if (itemHasRank && !sortMode) {
                     const long long bit = (rowBase + it[0]) * rowBits + it[1];
                     pruned = (bm[bit >> 5] >> (bit & 31)) & 1u;
                     if (!shared) mt.add(4);
@@ -486,7 +554,7 @@ __device__ __forceinline__ void run_task(Smem<B>& sm, const DevIndex& ix, const 
                     myBeg = it[lenK];
                     myLen = it[lenK + 1];
                     const int pathKind = hubPath ? 1 : (memoPath ? 2 : (existMemo ? 3 : 0));
-                    if (pathKind && myLen > 0 && !(tid == 0 && S.curOff[k] != 0)) {
+                    if (pathKind && myLen > 0 && !(tid == 0 && off != 0)) {
                         int code = classify_item(P, ix, stp, it, lenK, pathKind, myBeg, (int)myLen, fb, heavy, mt);
                         if (code == -4) {
                             myNew += 1;          // a new found bit of a split root
@@ -501,21 +569,30 @@ __device__ __forceinline__ void run_task(Smem<B>& sm, const DevIndex& ix, const 
                         }
                     }
                     if (tid == 0 && !isHub) {
-                        const long long off = S.curOff[k];
                         myBeg += (int)off;
                         myLen = myLen > off ? myLen - off : 0;
                     }
                 }
             }
-            const bool anyHub = (hubPath || memoPath) && __syncthreads_or(isHub);
             sm.wBeg[tid] = myBeg;
             sm.wLen[tid] = myLen;
             if (tid == 0 && !leaf) S.count[k + 1] = 0;
-            const long long pre = block_scan<B>(myLen, S);
-            sm.wPre[tid] = pre;
-            __syncthreads();
-            const long long total = sm.wPre[nw - 1];
+            const bool anyHub = publish_window<B>(myLen, isHub, sm) && (hubPath || memoPath);
+            long long total = 0;
+#pragma unroll
+            for (int w = 0; w < B / 32; ++w) total += S.warpSum[w];
             const long long take = min(total, (long long)(leaf ? kLeafChunk : P.cap));
+            // where the next round at this level starts: the item holding
+            // candidate `take` (items before it are consumed), and how much
+            // of it is
+            int cut = nw;
+            long long cutOff = 0;
+            if (take < total) {
+                WinCursor<B> c;
+                c.seek(sm, nw, take);
+                cut = c.item;
+                cutOff = take - c.first(sm) + (c.item == 0 ? off : 0);
+            }
             const int lenN = leaf ? 0 : P.tupleLen[k + 1];
             const int strideN = lenN + 2;
             int* baseN = leaf ? nullptr : items + S.levelOff[k + 1];
@@ -548,7 +625,7 @@ __device__ __forceinline__ void run_task(Smem<B>& sm, const DevIndex& ix, const 
                 int rank = par[1];
                 if (pairs && stp.hoWhich) {
                     rank = rankLoaded;
-                    if (!leaf) {
+                    if (!leaf && !sortMode) {
                         const long long bit = (rowBase + root) * rowBits + rank;
                         if (!shared) mt.add(4);
                         if ((bm[bit >> 5] >> (bit & 31)) & 1u) return;
@@ -559,6 +636,9 @@ __device__ __forceinline__ void run_task(Smem<B>& sm, const DevIndex& ix, const 
                         const uint32_t mask = 1u << (root & 31);
                         const uint32_t old = atomicOr(&fb[root >> 5], mask);
                         if (heavy) { mt.add(8); myNew += (old & mask) ? 0ull : 1ull; }
+                    } else if (sortMode) {
+                        emit_pair(P, keyRow0 + root, rank);
+                        mt.add(8);
                     } else {
                         const long long bit = (rowBase + root) * rowBits + rank;
                         const uint32_t mask = 1u << (bit & 31);
@@ -600,7 +680,7 @@ __device__ __forceinline__ void run_task(Smem<B>& sm, const DevIndex& ix, const 
                                  P.steps[k + 1].keyRef == lenK;
             const int sigBit = sig_bit(P.steps[k + 1 < P.m ? k + 1 : k].pred, P.steps[k + 1 < P.m ? k + 1 : k].dir);
             const uint32_t* sigWords = reinterpret_cast<const uint32_t*>(ix.valSig[stp.dir]) + (sigBit >> 5);
-            int hint = 0;
+            WinCursor<B> cur;
             for (long long jb = tid; jb < take; jb += (long long)B * kU) {
                 int lo_[kU], e_[kU], n0_[kU], n1_[kU], rk_[kU];
                 uint32_t sw_[kU];
@@ -610,21 +690,9 @@ __device__ __forceinline__ void run_task(Smem<B>& sm, const DevIndex& ix, const 
                     lo_[u] = -1;
                     e_[u] = 0;
                     if (j < take) {
-                        // the item holding candidate j: j only grows for this
-                        // thread, so try the previous item first (a hub's long
-                        // segment then costs one probe per candidate)
-                        int lo = hint;
-                        if (sm.wPre[lo] <= j) {
-                            int hi = nw - 1;
-                            ++lo;
-                            while (lo < hi) {
-                                const int mid = (lo + hi) >> 1;
-                                if (sm.wPre[mid] > j) hi = mid; else lo = mid + 1;
-                            }
-                        }
-                        hint = lo;
-                        lo_[u] = lo;
-                        e_[u] = sm.wBeg[lo] + (int)(j - (sm.wPre[lo] - sm.wLen[lo]));
+                        cur.seek(sm, nw, j);
+                        lo_[u] = cur.item;
+                        e_[u] = sm.wBeg[cur.item] + (int)(j - cur.first(sm));
                     }
                 }
 #pragma unroll
@@ -643,15 +711,6 @@ __device__ __forceinline__ void run_task(Smem<B>& sm, const DevIndex& ix, const 
             }
             if (anyHub) {
                 // hub items of the consumed part of the window: [0, cut)
-                int cut = nw;
-                if (take < total) {
-                    int lo = 0, hi = nw - 1;
-                    while (lo < hi) {
-                        const int mid = (lo + hi) >> 1;
-                        if (sm.wPre[mid] > take) hi = mid; else lo = mid + 1;
-                    }
-                    cut = lo;
-                }
                 const int lane = tid & 31, warp = tid >> 5;
                 constexpr int kWarps = B / 32;
                 const int words = P.rowWords;
@@ -702,26 +761,18 @@ __device__ __forceinline__ void run_task(Smem<B>& sm, const DevIndex& ix, const 
                 }
             }
             __syncthreads();
-            if (tid == 0) {
-                if (take >= total) {
-                    S.curItem[k] = w0 + nw;
-                    S.curOff[k] = 0;
-                } else {
-                    int lo = 0, hi = nw - 1;
-                    while (lo < hi) {
-                        const int mid = (lo + hi) >> 1;
-                        if (sm.wPre[mid] > take) hi = mid; else lo = mid + 1;
-                    }
-                    long long off = take - (sm.wPre[lo] - sm.wLen[lo]);
-                    if (lo == 0) off += S.curOff[k];
-                    S.curItem[k] = w0 + lo;
-                    S.curOff[k] = off;
+            const int nextItem = w0 + cut;
+            if (!leaf && S.count[k + 1] > 0) {
+                if (tid == 0) {
+                    S.curItem[k] = nextItem;
+                    S.curOff[k] = cutOff;
                 }
-                if (!leaf && S.count[k + 1] > 0) {
-                    S.k = k + 1;
-                    S.curItem[k + 1] = 0;
-                    S.curOff[k + 1] = 0;
-                }
+                ++k;
+                w0 = 0;
+                off = 0;
+            } else {
+                w0 = nextItem;
+                off = cutOff;
             }
         }
     }

@@ -99,7 +99,7 @@ struct Server {
             size_t roots = (size_t)std::max(1, ph->rootEnd - ph->rootBeg);
             size_t tasks = roots / (size_t)std::max(1, std::min(P.groupMax, P.cap)) + 1;
             b += sizeof(DevPlan) + 8 + tasks * sizeof(DevTask) * 2;
-            if (ph->needsGlobalBitmap) b += roots * (size_t)std::max(P.rowWords, 1) * 4;
+            if (ph->needsGlobalBitmap) b += std::min(roots * (size_t)std::max(P.rowWords, 1) * 4, c->dedupBudget);
         }
         return b;
     }
@@ -236,7 +236,8 @@ struct Server {
         }
         s.busy = true;
         const bool heavyWork = s.heavyLane || overflow;
-        s.st.stage(*c, plans, phases, true, s.stream, heavyWork ? 4.0e6 : 2.0e5);
+        // no sort mode: a served launch is never run a second time
+        s.st.stage(*c, plans, phases, true, s.stream, heavyWork ? 4.0e6 : 2.0e5, false, false);
         // Launches record task times, from which the task builder learns
         // each plan shape's cost (the launches that follow split slow plans
         // finer and classify requests by it).

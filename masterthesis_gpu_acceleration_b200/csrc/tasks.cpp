@@ -32,9 +32,16 @@ DevPlan plan_identity(const PhasePlan& ph) {
     p.memoTab = nullptr;
     p.memoBits = nullptr;
     p.memoWords = 0;
+    p.gBlockWords = 0;
+    p.pairKeys = nullptr;
+    p.keyCursor = nullptr;
+    p.keyCap = 0;
+    p.keyBase = 0;
+    p.rankBits = 0;
     p.pad0 = 0;
     p.pad1 = 0;
     p.pad2 = 0;
+    p.pad3 = 0;
     return p;
 }
 }  // namespace
@@ -267,7 +274,8 @@ TaskBuilder::Walk TaskBuilder::compute_walk(const PhasePlan& ph) {
 }
 
 void TaskBuilder::build(const std::vector<const PhasePlan*>& phases, int blocks, bool split,
-                        std::vector<PhaseTasks>& out, double walkBudget, bool costAware) {
+                        std::vector<PhaseTasks>& out, double walkBudget, bool costAware,
+                        const std::vector<PhaseLimits>* limits) {
     size_t n = phases.size();
     out.assign(n, PhaseTasks{});
     if (cacheBytes_ > kCacheLimit) {  // only here: walks hand out references into the cache
@@ -361,6 +369,8 @@ void TaskBuilder::build(const std::vector<const PhasePlan*>& phases, int blocks,
         pt.scale = scale[i];
         int32_t g = std::max(P.groupMax, 1);
         if (ph.needsGlobalBitmap) g = std::min(P.cap, 512);
+        const PhaseLimits lim = limits ? (*limits)[i] : PhaseLimits{};
+        if (lim.group > 0) g = std::min(g, lim.group);
         const int32_t R = ph.rootEnd - ph.rootBeg;
         const double uniform = R > 0 ? std::max(1.0, pt.work / R) : 1.0;
         const Walk* wk = walked[i];
@@ -415,7 +425,7 @@ void TaskBuilder::build(const std::vector<const PhasePlan*>& phases, int blocks,
             }
             const double wu = (double)w[o];
             const double wr = wu * sc;
-            if (canSplit && wr > splitAt) {
+            if (canSplit && wr > splitAt && (lim.maxHeavy < 0 || pt.heavyRows < lim.maxHeavy)) {
                 // a heavy root: slices of its first segment, one task each
                 flush(r);
                 int32_t vals[2];

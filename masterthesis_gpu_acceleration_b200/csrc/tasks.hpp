@@ -14,6 +14,14 @@
 
 namespace gr {
 
+// Per-phase limits of one build: at most `group` roots per task (0: the
+// plan's own limit) and at most `maxHeavy` heavy roots split over tasks that
+// share a global dedup row (-1: no limit; further heavy roots stay whole).
+struct PhaseLimits {
+    int32_t group = 0;
+    int32_t maxHeavy = -1;
+};
+
 struct PhaseTasks {
     std::vector<DevTask> tasks;
     std::vector<double> cost;   // estimated work per task
@@ -53,8 +61,14 @@ public:
     // costAware: walk a phase only when its expected device time exceeds
     // the walk's own host time, and cut only roots above a block's fair
     // share of their phase (per-rule launches, where nothing overlaps).
+    // limits (optional): one entry per phase.
     void build(const std::vector<const PhasePlan*>& phases, int blocks, bool split,
-               std::vector<PhaseTasks>& out, double walkBudget = 4.0e6, bool costAware = false);
+               std::vector<PhaseTasks>& out, double walkBudget = 4.0e6, bool costAware = false,
+               const std::vector<PhaseLimits>* limits = nullptr);
+
+    // Estimated candidate bindings of a phase (average fan-outs; exact first
+    // two levels for chain-shaped plans rooted at the first step's rows).
+    double work_estimate(const PhasePlan& ph) { return estimate2(ph); }
 
     size_t cache_bytes() const { return cacheBytes_; }
 

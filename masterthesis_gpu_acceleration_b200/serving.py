@@ -21,24 +21,46 @@ def run_rate(lib, rules, rate: float, duration: float, seed: int = 0, slots: int
     """Offers `rate` requests/s for `duration` seconds (rules cycled in order).
 
     Returns (summary dict, {request_id: (rule_index, status, GpuRuleResult)})."""
+    summ, res = run_rate_multi([(lib, rules)], rate, duration, seed=seed, slots=slots, max_batch=max_batch,
+                               mem_budget=mem_budget, id_base=id_base)
+    return summ, res[0]
+
+
+def run_rate_multi(graphs, rate: float, duration: float, seed: int = 0, weights=None, slots: int = 4,
+                   max_batch: int = 4096, mem_budget: int = 1 << 30, id_base: int = 0):
+    """One Poisson stream of `rate` requests/s for `duration` seconds over
+    several resident graphs: `graphs` is a list of (GpuRulesLib, rules), each
+    graph gets its own server, and every arrival goes to graph g with
+    probability weights[g] (uniform by default), taking that graph's next
+    rule in order.
+
+    Returns (summary dict with latencies over all graphs and per graph,
+    [{request_id: (rule_index, status, GpuRuleResult)} per graph])."""
     rng = np.random.default_rng(seed)
     n = max(1, int(rate * duration))
-    gaps = rng.exponential(1.0 / rate, size=n)
-    at = np.cumsum(gaps)
-    results = {}
-    lat = []
+    at = np.cumsum(rng.exponential(1.0 / rate, size=n))
+    k = len(graphs)
+    w = np.full(k, 1.0 / k) if weights is None else np.asarray(weights, dtype=float) / np.sum(weights)
+    dest = rng.choice(k, size=n, p=w)
+    results = [dict() for _ in range(k)]
+    lat = [[] for _ in range(k)]
     done = threading.Event()
-    with lib.serve(slots=slots, max_batch=max_batch, mem_budget=mem_budget) as sv:
+    servers = [lib.serve(slots=slots, max_batch=max_batch, mem_budget=mem_budget) for lib, _ in graphs]
+    try:
+        idx_of = {}   # request id -> rule index within its graph's list
+
         def drain():
-            while not done.is_set() or len(results) < n:
-                for rid, st, res, ms in sv.poll(wait_ms=20):
-                    results[rid] = ((rid - id_base) % len(rules), st, res)
-                    lat.append(ms)
-                if done.is_set() and len(results) >= n:
+            while True:
+                for g, sv in enumerate(servers):
+                    for rid, st, res, ms in sv.poll(wait_ms=5 if k > 1 else 20):
+                        results[g][rid] = (idx_of[rid], st, res)
+                        lat[g].append(ms)
+                if done.is_set() and sum(len(r) for r in results) >= n:
                     break
         th = threading.Thread(target=drain, daemon=True)
-        th.start()
+        next_rule = [0] * k
         t0 = time.perf_counter()
+        th.start()
         for i in range(n):
             target = t0 + at[i]
             while True:
@@ -47,27 +69,41 @@ def run_rate(lib, rules, rate: float, duration: float, seed: int = 0, slots: int
                     break
                 if target - now > 0.002:
                     time.sleep(target - now - 0.001)
-            sv.submit(id_base + i, rules[i % len(rules)])
+            g = int(dest[i])
+            rules = graphs[g][1]
+            ri = next_rule[g] % len(rules)
+            next_rule[g] += 1
+            idx_of[id_base + i] = ri
+            servers[g].submit(id_base + i, rules[ri])
         t_sub = time.perf_counter() - t0
         done.set()
         th.join(timeout=600)
         t_end = time.perf_counter() - t0
-        stats = sv.stats()
-    lat = np.array(lat) if lat else np.zeros(1)
-    ok = sum(1 for v in results.values() if v[1] == 0)
-    return {
+        stats = [sv.stats() for sv in servers]
+    finally:
+        for sv in servers:
+            sv.stop()
+    every = np.concatenate([np.array(x) for x in lat if x]) if any(lat) else np.zeros(1)
+    completed = sum(len(r) for r in results)
+    ok = sum(1 for r in results for v in r.values() if v[1] == 0)
+    summ = {
         "offered_rules_per_s": rate,
         "submitted": n,
         "completed_ok": ok,
-        "sustained_rules_per_s": len(results) / t_end if t_end > 0 else 0.0,
+        "sustained_rules_per_s": completed / t_end if t_end > 0 else 0.0,
         "achieved_arrival_rate": n / t_sub if t_sub > 0 else 0.0,
-        "p50_ms": float(np.percentile(lat, 50)),
-        "p99_ms": float(np.percentile(lat, 99)),
-        "max_ms": float(lat.max()),
-        "launches": stats["launches"],
-        "device_ms": stats["device_ms"],
-        "host_prepare_ms": stats["host_ms"],
-    }, results
+        "p50_ms": float(np.percentile(every, 50)),
+        "p99_ms": float(np.percentile(every, 99)),
+        "max_ms": float(every.max()),
+        "launches": sum(s["launches"] for s in stats),
+        "device_ms": sum(s["device_ms"] for s in stats),
+        "host_prepare_ms": sum(s["host_ms"] for s in stats),
+    }
+    if k > 1:
+        summ["per_graph"] = [{"requests": len(lat[g]),
+                              "p50_ms": float(np.percentile(lat[g], 50)) if lat[g] else None,
+                              "p99_ms": float(np.percentile(lat[g], 99)) if lat[g] else None} for g in range(k)]
+    return summ, results
 
 
 def sweep(lib, rules, rates, duration: float, seed: int = 0, **kw):
@@ -77,5 +113,18 @@ def sweep(lib, rules, rates, duration: float, seed: int = 0, **kw):
         summ, res = run_rate(lib, rules, r, duration, seed + k, id_base=base, **kw)
         out.append(summ)
         allres.update(res)
+        base += summ["submitted"]
+    return out, allres
+
+
+def sweep_multi(graphs, rates, duration: float, seed: int = 0, **kw):
+    """sweep over several resident graphs (run_rate_multi per rate)."""
+    out, allres = [], [dict() for _ in graphs]
+    base = 0
+    for k, r in enumerate(rates):
+        summ, res = run_rate_multi(graphs, r, duration, seed + k, id_base=base, **kw)
+        out.append(summ)
+        for g, x in enumerate(res):
+            allres[g].update(x)
         base += summ["submitted"]
     return out, allres

@@ -13,6 +13,9 @@ Fixtures:
                          size, hub rules included; generated with --threads)
   c3_seed0.npz           all 10,000 c3 rules: support, headSize, headSupport,
                          bodySize per rule (generated with --threads)
+  c4_seed0_hub.json      the 10 hub rules of the full c4 graph (body sizes up
+                         to ~10^10, wrapped by the reference's int; run
+                         separately with --c4-hub, tens of CPU minutes)
   fuzz_<k>.json          small dense graphs with prefixes, literals,
                          self-loops and constants, and random rules that use
                          constants, unknown terms, repeated atoms, empty bodies,
@@ -269,11 +272,40 @@ def edge_cases(tmp: Path):
     (OUT / "edge_cases.json").write_text(json.dumps(fx, indent=1))
 
 
+def c4_hub(tmp: Path, threads: int = 6):
+    """The 10 hub rules of the full c4 graph (seed 0), run by the reference.
+
+    CPU_01 adds the per-hS pair counts into an `int` (SupportCounting.cpp,
+    countBodySize: `int bodySizeResult`), so body sizes above 2^31 come out
+    wrapped modulo 2^32; the fixture keeps the reference's value as printed
+    (`bodySize_ref`, two's-complement int32) and the engine's 64-bit count is
+    compared modulo 2^32.  Support and head sizes fit an int exactly."""
+    d = synth.generate("c4", tmp / "c4", seed=0)
+    rules = synth.read_rules(d)[:10]
+    rf = tmp / "c4_hub_rules.txt"
+    rf.write_text("\n".join(rules) + "\n")
+    rows, summary = oracle.run_reference(d / "graph.ttl", rf, threads=threads)
+    fx = {
+        "config": "c4", "seed": 0, "rules_index": list(range(10)),
+        "triples_sha256": sha(d / "triples.bin"),
+        "rules": rules,
+        "expected": [{"support": r["support"], "headSize": r["headSize"], "headSupport": r["headSupport"],
+                      "bodySize_ref": r["bodySize"], "supportMs": r["supportMs"], "confidenceMs": r["confidenceMs"]}
+                     for r in rows],
+        "reference_eval_wall_ms": summary.get("eval_wall_ms"), "threads": threads,
+    }
+    (OUT / "c4_seed0_hub.json").write_text(json.dumps(fx, indent=1))
+
+
 def main():
     if not oracle.ref_available():
         oracle.build()
     with tempfile.TemporaryDirectory() as t:
         tmp = Path(t)
+        if "--c4-hub" in sys.argv:
+            c4_hub(tmp)
+            print("fixture written to", OUT / "c4_seed0_hub.json")
+            return
         only = [a.split("=", 1)[1] for a in sys.argv if a.startswith("--only=")]
         if only:
             for cfg in only[0].split(","):

@@ -126,3 +126,34 @@ def test_c4_split_hub_rules_sum_to_whole(c4):
     for i in HUB_RULES:
         parts = np.array([lib.evaluate_rule_shard(rules[i], k, 4) for k in range(4)])
         assert parts[:, 0].sum() == cnt[i, 0] and parts[:, 3].sum() == cnt[i, 3], (i, parts.tolist())
+
+
+def _as_int32(x: int) -> int:
+    """x reduced the way the reference's `int` accumulator wraps it."""
+    x &= 0xFFFFFFFF
+    return x - (1 << 32) if x >= (1 << 31) else x
+
+
+def test_int32_wrap_helper():
+    assert _as_int32(5) == 5 and _as_int32(2**31) == -2**31 and _as_int32(2**32 + 7) == 7
+    assert _as_int32(8_800_000_000) == 8_800_000_000 - 2 * 2**32
+
+
+@pytest.mark.gpu
+def test_c4_hub_rules_match_reference(c4):
+    """The 10 hub rules of the full c4 graph against the reference's own
+    CPU_01 results (tests/golden/c4_seed0_hub.json, run by
+    tests/golden/make_golden.py --c4-hub): support and head sizes exactly,
+    body sizes exactly modulo 2^32, because CPU_01 sums them in an int
+    (SupportCounting.cpp, countBodySize) and the largest exceed 2^31 here."""
+    _, d, rules, _, cnt = c4
+    from conftest import GOLDEN
+    if not (GOLDEN / "c4_seed0_hub.json").exists():
+        pytest.skip("tests/golden/c4_seed0_hub.json not generated (make_golden.py --c4-hub)")
+    fx = load_fixture("c4_seed0_hub.json")
+    assert hashlib.sha256((d / "triples.bin").read_bytes()).hexdigest() == fx["triples_sha256"]
+    for k, i in enumerate(fx["rules_index"]):
+        assert rules[i] == fx["rules"][k]
+        e = fx["expected"][k]
+        assert [int(cnt[i, 0]), int(cnt[i, 1]), int(cnt[i, 2])] == [e["support"], e["headSize"], e["headSupport"]], i
+        assert _as_int32(int(cnt[i, 3])) == e["bodySize_ref"], (i, int(cnt[i, 3]), e["bodySize_ref"])

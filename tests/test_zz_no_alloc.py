@@ -45,3 +45,26 @@ def test_noalloc_matches_allocating_entry_point_c3(tmp_path):
             want = lib.evaluate_rule(rule)
             got = [lib.evaluate_rule_noalloc(rule) for _ in range(2)]
             assert all(_same(g, want) for g in got), rule
+
+
+def test_noalloc_global_bitmap_in_scratch_and_size_limit(tmp_path):
+    """Rules whose pair bitmap cannot sit in shared memory (an hO domain of
+    400,000 values) keep it in the scratch array: 100 head subjects need
+    5 MB of rows, which fits the 8 MiB array; 200 need 10 MB, which the
+    entry point refuses with -1 and the size in gpu_last_error().  Warm
+    calls take no device memory."""
+    from conftest import wide_domain_graph
+    ttl, rules, exp = wide_domain_graph(tmp_path / "wide")
+    with eng.GpuRulesLib(ttl) as lib:
+        want = lib.evaluate_rule(rules[0])
+        assert [want.support, want.headSize, want.headSupport, want.bodySize] == exp[0].tolist()
+        got = [lib.evaluate_rule_noalloc(rules[0]) for _ in range(2)]
+        assert all(_same(g, want) for g in got)
+        before = eng.query_vram()[0]
+        for _ in range(3):
+            assert _same(lib.evaluate_rule_noalloc(rules[0]), want)
+        assert eng.query_vram()[0] == before, "no-allocation calls changed free device memory"
+        with pytest.raises(RuntimeError, match="scratch"):
+            lib.evaluate_rule_noalloc(rules[1])
+        # the array is still usable after a refusal
+        assert _same(lib.evaluate_rule_noalloc(rules[0]), want)
