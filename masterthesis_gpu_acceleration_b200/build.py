@@ -24,7 +24,7 @@ NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 
 ENGINE_SOURCES = ["turtle.cpp", "rules.cpp", "index.cpp", "index_io.cpp", "planner.cpp", "tasks.cpp", "kernels.cu",
-                  "sort.cu", "context.cu", "serve.cu"]
+                  "sort.cu", "index_gpu.cu", "context.cu", "serve.cu"]
 HEADERS = ["common.hpp", "turtle.hpp", "rules.hpp", "index.hpp", "index_io.hpp", "planner.hpp", "tasks.hpp",
            "engine.hpp", "parallel.hpp"]
 

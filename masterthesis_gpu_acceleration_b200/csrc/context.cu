@@ -767,7 +767,12 @@ void* gpu_load_graph(const char* ttlPath) {
         // GPU_RULES_HUB_MIN_DEGREE overrides the hub-row threshold (0: no hub rows)
         int32_t hubMin = kHubMinDegree;
         if (const char* h = std::getenv("GPU_RULES_HUB_MIN_DEGREE")) hubMin = std::max(0, std::atoi(h));
-        c->hix = build_index(spo, (int32_t)c->ents.size(), (int32_t)c->preds.size(), hubMin);
+        // the index is built on the device (GPU_RULES_INDEX_BUILD=host: on host threads)
+        const char* where = std::getenv("GPU_RULES_INDEX_BUILD");
+        if (where && std::strcmp(where, "host") == 0)
+            c->hix = build_index(spo, (int32_t)c->ents.size(), (int32_t)c->preds.size(), hubMin);
+        else
+            c->hix = build_index_device(spo, (int32_t)c->ents.size(), (int32_t)c->preds.size(), hubMin);
         finish_load(c);
         return c;
     } catch (const std::exception& e) {

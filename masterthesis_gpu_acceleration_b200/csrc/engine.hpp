@@ -33,6 +33,11 @@ cudaError_t engine_launch(const DevIndex& ix, const DevPlan* plans, const DevTas
 // Sort mode (sort.cu): radix sort of the appended pair keys and the count of
 // each plan's distinct keys into its result slot.
 size_t pairs_sort_hist_words(unsigned long long cap);
+// Sorts min(*count, cap) keys by their low `bits` bits (8 bits a pass,
+// stable), ping-ponging with tmp; returns the buffer that holds the result.
+unsigned long long* radix_sort_keys(unsigned long long* keys, unsigned long long* tmp, const unsigned long long* count,
+                                    unsigned long long cap, int bits, uint32_t* hist, int grid, cudaStream_t stream,
+                                    cudaError_t* err);
 cudaError_t pairs_sort_count(unsigned long long* keys, unsigned long long* tmp, const unsigned long long* count,
                              unsigned long long cap, int bits, int slotShift, const int32_t* slotOf, int nSlots,
                              unsigned long long* results, int* status, uint32_t* hist, int grid,

@@ -115,6 +115,8 @@ void build_hubs(HostIndex& ix, int32_t minDegree) {
 
 }  // namespace
 
+void build_hub_rows(HostIndex& ix, int32_t minDegree) { build_hubs(ix, minDegree); }
+
 std::pair<int32_t, int32_t> HostIndex::row_range(int32_t p, int d, int32_t key) const {
     if (p < 0 || p >= nPred || key < 0 || hash.empty()) return {0, 0};
     uint32_t tag = (uint32_t)p * 2u + (uint32_t)d;

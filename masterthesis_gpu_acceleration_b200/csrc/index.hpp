@@ -55,4 +55,15 @@ constexpr int32_t kHubMinDegree = 128;
 HostIndex build_index(const std::vector<int32_t>& spo, int32_t nEnt, int32_t nPred,
                       int32_t hubMinDegree = kHubMinDegree);
 
+// The same index with the sorts, rows, ranks, lookup table and signatures
+// built on the current CUDA device and copied back (index_gpu.cu); only the
+// hub bitmaps are built on the host.  Throws on a CUDA error.  A graph whose
+// packed (predicate, key, value) keys need more than 64 bits is built on the
+// host.
+HostIndex build_index_device(const std::vector<int32_t>& spo, int32_t nEnt, int32_t nPred,
+                             int32_t hubMinDegree = kHubMinDegree);
+
+// Hub rows and their bitmaps of an index whose other arrays are complete.
+void build_hub_rows(HostIndex& ix, int32_t minDegree);
+
 }  // namespace gr

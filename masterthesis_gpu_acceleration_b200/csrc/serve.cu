@@ -29,6 +29,7 @@
 #include <thread>
 
 #include "engine.hpp"
+#include "parallel.hpp"
 
 namespace gr {
 namespace {
@@ -167,9 +168,13 @@ struct Server {
         }
         if (got.empty()) return false;
         const auto h0 = Clock::now();
-        for (auto& r : got) {
-            Planned q;
-            q.req = std::move(r);
+        // parse, plan and cost the new requests on host threads (they only
+        // read the graph, the dictionaries and the learnt costs, which only
+        // this thread changes, between batches)
+        std::vector<Planned> qs(got.size());
+        parallel_for(got.size(), [&](size_t i) {
+            Planned& q = qs[i];
+            q.req = std::move(got[i]);
             try {
                 q.rp = plan_rule(c->parser->parse_text(q.req.text), c->hix, c->geom);
             } catch (const std::exception&) {
@@ -183,6 +188,9 @@ struct Server {
                     ns = c->tasks->expected_ns(q.rp.support) + c->tasks->expected_ns(q.rp.body);
             }
             q.ns = ns;
+        }, 64);
+        for (Planned& q : qs) {
+            const double ns = q.ns;
             if (lanes && ns > c->serveHeavyNs) {
                 heavyBacklogNs += ns;
                 heavy.push_back(std::move(q));

@@ -248,6 +248,10 @@ size_t pairs_sort_hist_words(unsigned long long cap) {
     return (size_t)kRadix * (size_t)(tiles > 0 ? tiles : 1) + kRadix;
 }
 
+unsigned long long* radix_sort_keys(unsigned long long* keys, unsigned long long* tmp, const unsigned long long* count,
+                                    unsigned long long cap, int bits, uint32_t* hist, int grid, cudaStream_t stream,
+                                    cudaError_t* err);
+
 // Sorts the first min(*count, cap) keys by their low `bits` bits, ping-
 // ponging between keys and tmp, then adds each plan's distinct keys to
 // results[slotOf[key >> slotShift]] (nSlots sort indices; status as the
@@ -261,11 +265,29 @@ cudaError_t pairs_sort_count(unsigned long long* keys, unsigned long long* tmp, 
     if (bits < 1 || bits > 64 || slotShift < 0 || slotShift > 63 || cap > 0xffffffffull) return cudaErrorInvalidValue;
     const long long tilesCap = (long long)((cap + kSortTile - 1) / kSortTile);
     const int g = (int)(tilesCap < grid ? tilesCap : grid);
+    cudaError_t e = cudaSuccess;
+    unsigned long long* a = radix_sort_keys(keys, tmp, count, cap, bits, hist, grid, stream, &e);
+    if (e != cudaSuccess) return e;
+    pairs_unique_kernel<<<g, kSortThreads, 0, stream>>>(a, count, cap, slotShift, slotOf, nSlots, results, status);
+    return cudaGetLastError();
+}
+
+unsigned long long* radix_sort_keys(unsigned long long* keys, unsigned long long* tmp, const unsigned long long* count,
+                                    unsigned long long cap, int bits, uint32_t* hist, int grid, cudaStream_t stream,
+                                    cudaError_t* err) {
+    *err = cudaSuccess;
+    if (cap == 0) return keys;
+    if (bits < 1 || bits > 64 || cap > 0xffffffffull) {
+        *err = cudaErrorInvalidValue;
+        return keys;
+    }
+    const long long tilesCap = (long long)((cap + kSortTile - 1) / kSortTile);
+    const int g = (int)(tilesCap < grid ? tilesCap : grid);
     unsigned long long* a = keys;
     unsigned long long* b = tmp;
     for (int shift = 0; shift < bits; shift += 8) {
         cudaError_t e = cudaMemsetAsync(hist + (size_t)kRadix * tilesCap, 0, kRadix * sizeof(uint32_t), stream);
-        if (e != cudaSuccess) return e;
+        if (e != cudaSuccess) { *err = e; return a; }
         radix_hist_kernel<<<g, kSortThreads, 0, stream>>>(a, count, cap, shift, hist, tilesCap);
         radix_scan_kernel<<<kRadix, 1024, 0, stream>>>(hist, count, cap, tilesCap);
         radix_scatter_kernel<<<g, kSortThreads, 0, stream>>>(a, b, count, cap, shift, hist, tilesCap);
@@ -273,8 +295,8 @@ cudaError_t pairs_sort_count(unsigned long long* keys, unsigned long long* tmp, 
         a = b;
         b = x;
     }
-    pairs_unique_kernel<<<g, kSortThreads, 0, stream>>>(a, count, cap, slotShift, slotOf, nSlots, results, status);
-    return cudaGetLastError();
+    *err = cudaGetLastError();
+    return a;
 }
 
 }  // namespace gr

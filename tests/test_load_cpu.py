@@ -61,3 +61,25 @@ def test_prefix_after_first_chunk_falls_back(checker, tmp_path):
 def test_parallel_read_and_index_synthetic(checker, data_dir):
     d = synth.generate("c2s", data_dir / "c2s_load", seed=3)
     _run(checker, d / "graph.ttl", 1 << 16)
+
+
+def test_graph_file_reader_of_the_index_comparison(checker, tmp_path):
+    """tests/test_index_gpu.py compares host- and device-built indexes by
+    reading graph files; its reader is checked here on a file the native
+    checker wrote from the host build."""
+    from test_index_gpu import ARRAYS, read_graph_file
+    p = tmp_path / "fuzz.ttl"
+    p.write_text(load_fixture("fuzz_2.json")["ttl"])
+    _run(checker, p, 64)
+    g = read_graph_file(str(p) + ".graph")
+    n = g["n_triples"]
+    assert n > 0 and g["hash"].shape == (g["hash_mask"] + 1, 4)
+    for d in (0, 1):
+        for name in ("val", "valRank", "src", "srcRank", "valSig", "sufSig"):
+            assert len(g[f"{name}{d}"]) == n, (name, d)
+        assert g[f"rowBeg{d}"][-1] == n and g[f"predEdge{d}"][-1] == n
+        assert len(g[f"predRow{d}"]) == len(g[f"predEdge{d}"]) == g["n_pred"] + 1
+        assert len(g[f"rowKey{d}"]) + 1 == len(g[f"rowBeg{d}"]) == g[f"predRow{d}"][-1] + 1
+    used = (g["hash"][:, 0] != 0xFFFFFFFF).sum()
+    assert used == len(g["rowKey0"]) + len(g["rowKey1"])
+    assert len(ARRAYS) == 25
