@@ -4,10 +4,11 @@
 # sm_100a into baseline/_ref/gpu03/libgpu_rules.so, as the per-rule GPU
 # comparator of bench.py --gpu03.  Nothing of the reference is copied into
 # this repository; the output directory is git-ignored.  Runs only where the
-# reference tree is present (REF_DIR, default /root/reference).
+# reference tree is present (REF_DIR, default: a `reference` checkout
+# beside this repository).
 set -euo pipefail
 HERE="$(cd "$(dirname "${BASH_SOURCE[0]}")" && pwd)"
-REF_DIR="${REF_DIR:-/root/reference}"
+REF_DIR="${REF_DIR:-$(cd "$HERE/../.." && pwd)/reference}"
 SRC="$REF_DIR/GPU_03"
 if [ ! -f "$SRC/gpu_rules_lib.cu" ]; then
   echo "reference GPU_03 sources not found under $REF_DIR; keeping any prebuilt library" >&2

@@ -4,11 +4,11 @@
 #   oracle/_ref/cpu01_harness   the reference's CPU_01_nonparallel sources,
 #                               compiled where they lie, with ref_harness.cpp
 # The second step runs only when the reference tree is present (REF_DIR,
-# default /root/reference); on a machine without it the prebuilt binary, if
-# any, is kept.
+# default: a `reference` checkout beside this repository); on a machine
+# without it the prebuilt binary, if any, is kept.
 set -euo pipefail
 HERE="$(cd "$(dirname "${BASH_SOURCE[0]}")" && pwd)"
-REF_DIR="${REF_DIR:-/root/reference}"
+REF_DIR="${REF_DIR:-$(cd "$HERE/../.." && pwd)/reference}"
 mkdir -p "$HERE/lib"
 gcc -O2 -std=c11 -Wall -Wextra -shared -fPIC "$HERE/rules_oracle.c" -o "$HERE/lib/liborules.so"
 SRC="$REF_DIR/CPU_01_nonparallel"

@@ -13,9 +13,10 @@ Fixtures:
                          size, hub rules included; generated with --threads)
   c3_seed0.npz           all 10,000 c3 rules: support, headSize, headSupport,
                          bodySize per rule (generated with --threads)
-  c4_seed0_hub.json      the 10 hub rules of the full c4 graph (body sizes up
-                         to ~10^10, wrapped by the reference's int; run
-                         separately with --c4-hub, tens of CPU minutes)
+  c4_seed0_hub.json      the 10 hub rules of the full c4 graph (body sizes
+                         above 2^31 come out wrapped by the reference's int;
+                         run separately with --c4-hub: 23 minutes on 6
+                         threads)
   fuzz_<k>.json          small dense graphs with prefixes, literals,
                          self-loops and constants, and random rules that use
                          constants, unknown terms, repeated atoms, empty bodies,

@@ -91,3 +91,13 @@ def test_oracle_c3_sample():
         ir = np.concatenate([rules[i] for i in idx])
         counts, _ = g.evaluate_ir(ir, len(idx))
         assert (counts == exp[idx]).all()
+
+
+def test_c4_hub_fixture_is_well_formed():
+    """The full-size c4 hub-rule fixture (reference output) holds the 10 hub
+    rules and at least one body size that wrapped past 2^31 in the
+    reference's int."""
+    fx = load_fixture("c4_seed0_hub.json")
+    assert fx["rules_index"] == list(range(10)) and len(fx["rules"]) == len(fx["expected"]) == 10
+    assert any(e["bodySize_ref"] < 0 for e in fx["expected"])
+    assert all(e["support"] <= e["headSupport"] <= e["headSize"] for e in fx["expected"])
