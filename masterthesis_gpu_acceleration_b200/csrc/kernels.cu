@@ -36,6 +36,7 @@
 #include <cooperative_groups.h>
 #include <cuda_runtime.h>
 
+#include <climits>
 #include <cstdint>
 
 #include "common.hpp"
@@ -61,6 +62,8 @@ struct BlockState {
     int curItem[kMaxBody + 1];      // a level's position, saved when the search descends below it
     long long curOff[kMaxBody + 1];
     int count[kMaxBody + 1];
+    int firstFail;                  // first candidate of a wide round that found the next level full
+    unsigned safeLevels;            // bit l: level l takes capacity-sized rounds until exhausted
     int levelOff[kMaxBody + 1];
     long long warpSum[kWarps];
     unsigned long long red[kWarps];
@@ -162,6 +165,25 @@ __device__ __forceinline__ bool publish_window(long long x, bool flag, Smem<B>& 
     sm.wLoc[threadIdx.x] = x;
     if (lane == 31) sm.st.warpSum[warp] = x;
     return __syncthreads_or(flag) != 0;
+}
+
+// The window's candidate total: the warps' totals summed by shuffles.
+// (Up to 256 threads the eight totals are added directly; the two forms
+// differ only in the registers the kernel needs around them.)
+template <int B>
+__device__ __forceinline__ long long window_total(const Smem<B>& sm) {
+    if constexpr (B <= 256) {
+        long long v = 0;
+#pragma unroll
+        for (int w = 0; w < B / 32; ++w) v += sm.st.warpSum[w];
+        return v;
+    } else {
+        const int lane = threadIdx.x & 31;
+        long long v = lane < B / 32 ? sm.st.warpSum[lane] : 0;
+#pragma unroll
+        for (int d = 16; d; d >>= 1) v += __shfl_xor_sync(0xffffffffu, v, d);
+        return v;
+    }
 }
 
 // The window item that holds candidate j, for j that never decreases:
@@ -369,6 +391,10 @@ template <int B, bool kC>
 __device__ __forceinline__ void run_task(Smem<B>& sm, const DevIndex& ix, const DevTask& task,
                                          unsigned long long* results, int* status, Meter<kC>& mt) {
     constexpr int kLeafChunk = 16 * B;
+    // candidates of a non-leaf round whose next step has a signature test
+    // (most candidates die on it): more than the next level's capacity, so
+    // a round may find that level full (see `wide` below)
+    constexpr int kWideChunk = 8 * B;
     // candidates per thread per group (1, 2 and 4 measured on c3: 44.96,
     // 45.22 and 46.92 ms per launch; 8 makes compilation impractical)
     constexpr int kU = 1;
@@ -413,6 +439,8 @@ __device__ __forceinline__ void run_task(Smem<B>& sm, const DevIndex& ix, const 
         if (tid == 0) mt.add(16 * (unsigned long long)n4);
     }
     if (tid == 0) {
+        S.firstFail = INT_MAX;
+        S.safeLevels = 0;
         int off = 0;
         for (int l = 0; l <= kMaxBody; ++l) {
             S.curItem[l] = 0;
@@ -508,6 +536,8 @@ __device__ __forceinline__ void run_task(Smem<B>& sm, const DevIndex& ix, const 
             const int cnt = min(S.count[k], P.cap);
             if (w0 >= cnt) {
                 if (k == 0) break;
+                // nobody reads level k's bit again before it is re-entered
+                if (tid == 0) S.safeLevels &= ~(1u << k);
                 --k;
                 w0 = S.curItem[k];
                 off = S.curOff[k];
@@ -578,21 +608,22 @@ __device__ __forceinline__ void run_task(Smem<B>& sm, const DevIndex& ix, const 
             sm.wLen[tid] = myLen;
             if (tid == 0 && !leaf) S.count[k + 1] = 0;
             const bool anyHub = publish_window<B>(myLen, isHub, sm) && (hubPath || memoPath);
-            long long total = 0;
-#pragma unroll
-            for (int w = 0; w < B / 32; ++w) total += S.warpSum[w];
-            const long long take = min(total, (long long)(leaf ? kLeafChunk : P.cap));
-            // where the next round at this level starts: the item holding
-            // candidate `take` (items before it are consumed), and how much
-            // of it is
-            int cut = nw;
-            long long cutOff = 0;
-            if (take < total) {
-                WinCursor<B> c;
-                c.seek(sm, nw, take);
-                cut = c.item;
-                cutOff = take - c.first(sm) + (c.item == 0 ? off : 0);
-            }
+            const long long total = window_total<B>(sm);
+            // When the next step expands from the value this step binds,
+            // that value's row signature (stored beside it) drops most
+            // candidates whose next row is absent before any lookup.
+            const bool sigTest = !leaf && stp.kind == kExpand && P.steps[k + 1].kind == kExpand &&
+                                 P.steps[k + 1].keyRef == lenK;
+            // Wide round: up to kWideChunk candidates although each survivor
+            // takes a slot of the next level.  A survivor that finds it full
+            // records its candidate index, and the level resumes from the
+            // first such candidate; items made from later candidates are made
+            // again then, which changes no count (every dedup structure is a
+            // set counted on insertion).  A level that overflowed takes
+            // capacity-sized rounds, which cannot overflow, until it is
+            // exhausted, so the search always advances.
+            const bool wide = sigTest && !((S.safeLevels >> k) & 1u);
+            const long long take = min(total, (long long)(leaf ? kLeafChunk : (wide ? kWideChunk : P.cap)));
             const int lenN = leaf ? 0 : P.tupleLen[k + 1];
             const int strideN = lenN + 2;
             int* baseN = leaf ? nullptr : items + S.levelOff[k + 1];
@@ -607,7 +638,7 @@ __device__ __forceinline__ void run_task(Smem<B>& sm, const DevIndex& ix, const 
 
             // One candidate: its parent item `lo`, edge `e`, new value(s)
             // n0/n1 and (when this step binds hO) the loaded rank.
-            auto eval = [&](int lo, int e, int n0, int n1, int rankLoaded) {
+            auto eval = [&](int lo, int e, int n0, int n1, int rankLoaded, int j) {
                 const int* par = baseK + (w0 + lo) * strideK;
                 const int root = par[0];
                 if (!pairs && ((fb[root >> 5] >> (root & 31)) & 1u)) return;
@@ -654,7 +685,11 @@ __device__ __forceinline__ void run_task(Smem<B>& sm, const DevIndex& ix, const 
                         if (!((__ldg(lookWords + 2 * (long long)seg.x) >> (lookBit & 31)) & 1u)) return;
                     }
                     const int slot = atomicAdd(&S.count[k + 1], 1);
-                    if (slot >= P.cap) { atomicOr(status, 8); return; }
+                    if (slot >= P.cap) {
+                        if (wide) atomicMin(&S.firstFail, j);
+                        else atomicOr(status, 8);   // a capacity-sized round cannot fill the level
+                        return;
+                    }
                     int* dst = baseN + slot * strideN;
                     dst[0] = root;
                     dst[1] = rank;
@@ -673,11 +708,6 @@ __device__ __forceinline__ void run_task(Smem<B>& sm, const DevIndex& ix, const 
             const int* rbase = stp.kind == kExpand ? ix.valRank[stp.dir]
                                                    : (stp.hoWhich == 1 ? ix.srcRank[0] : ix.valRank[0]);
             const bool wantRank = pairs && stp.hoWhich;
-            // When the next step expands from the value this step binds,
-            // that value's row signature (stored beside it) drops most
-            // candidates whose next row is absent before any lookup.
-            const bool sigTest = !leaf && stp.kind == kExpand && P.steps[k + 1].kind == kExpand &&
-                                 P.steps[k + 1].keyRef == lenK;
             const int sigBit = sig_bit(P.steps[k + 1 < P.m ? k + 1 : k].pred, P.steps[k + 1 < P.m ? k + 1 : k].dir);
             const uint32_t* sigWords = reinterpret_cast<const uint32_t*>(ix.valSig[stp.dir]) + (sigBit >> 5);
             WinCursor<B> cur;
@@ -707,7 +737,22 @@ __device__ __forceinline__ void run_task(Smem<B>& sm, const DevIndex& ix, const 
                 }
 #pragma unroll
                 for (int u = 0; u < kU; ++u)
-                    if (lo_[u] >= 0 && ((sw_[u] >> (sigBit & 31)) & 1u)) eval(lo_[u], e_[u], n0_[u], n1_[u], rk_[u]);
+                    if (lo_[u] >= 0 && ((sw_[u] >> (sigBit & 31)) & 1u))
+                        eval(lo_[u], e_[u], n0_[u], n1_[u], rk_[u], (int)(jb + (long long)u * B));
+            }
+            // where the next round at this level starts: the item holding
+            // candidate `take` (items before it are consumed), and how much
+            // of it is (computed here, not before the candidates, so that it
+            // holds no registers across them)
+            int cut = nw;
+            long long cutOff = 0;
+            {
+                if (take < window_total<B>(sm)) {
+                    WinCursor<B> c;
+                    c.seek(sm, nw, take);
+                    cut = c.item;
+                    cutOff = take - c.first(sm) + (c.item == 0 ? off : 0);
+                }
             }
             if (anyHub) {
                 // hub items of the consumed part of the window: [0, cut)
@@ -761,6 +806,20 @@ __device__ __forceinline__ void run_task(Smem<B>& sm, const DevIndex& ix, const 
                 }
             }
             __syncthreads();
+            if (wide) {
+                const int ff = S.firstFail;   // final after the barrier
+                if (ff < take) {
+                    WinCursor<B> c;
+                    c.seek(sm, nw, ff);
+                    cut = c.item;
+                    cutOff = ff - c.first(sm) + (c.item == 0 ? off : 0);
+                    if (tid == 0) S.safeLevels |= 1u << k;
+                    // every thread has read the window and firstFail: the
+                    // next round may rewrite them
+                    __syncthreads();
+                    if (tid == 0) S.firstFail = INT_MAX;
+                }
+            }
             const int nextItem = w0 + cut;
             if (!leaf && S.count[k + 1] > 0) {
                 if (tid == 0) {
