@@ -176,7 +176,12 @@ int gpu_evaluate_rule_noalloc(void* ctx, const char* ruleText, GpuRuleResult* ou
  * (1: keep a heavy lane, default; 0: all slots alike), "serve_heavy_share"
  * (the heavy lane launches on 1/share of the blocks, default 2) and
  * "serve_heavy_us" (expected device time in microseconds above which a
- * request is heavy, default 5000).  "dedup_budget": device bytes that one
+ * request is heavy, default 5000), "serve_deadline_us" (device time a
+ * served launch may take, from each block's start; past it the blocks
+ * abandon their work at the end of a frontier round and the requests that
+ * lost work complete with status -4; 0, the default: none) and
+ * "serve_max_us" (requests whose expected device time exceeds it are
+ * refused at admission with status -4; 0, the default: none).  "dedup_budget": device bytes that one
  * launch's global pair bitmaps may take (default 8 GiB); beyond it each
  * body-size phase whose pairs do not fit shared memory uses either bitmap
  * rows per resident block or pair keys sorted on the device, whichever
@@ -189,7 +194,10 @@ int gpu_set_option(void* ctx, const char* name, long long value);
 
 /* One completed request.  status: 0 ok, -1 the rule does not parse, -2 the
  * rule's device-memory estimate exceeds the server's whole budget, -3 a CUDA
- * or engine error.  latencyMs: from gpu_serve_submit to completion. */
+ * or engine error, -4 over the server's time limits (its expected device
+ * time exceeds "serve_max_us", or its launch reached "serve_deadline_us"
+ * before the rule was counted; see gpu_set_option); the result is then
+ * zero.  latencyMs: from gpu_serve_submit to completion. */
 typedef struct {
     long long     requestId;
     int           status;

@@ -209,6 +209,11 @@ struct EngineProfile {
     // zeroed word works as the initial value), span[1] = max block end,
     // both in device global-timer ns.
     unsigned long long* span = nullptr;
+    // Served launches: a device-time budget in ns from each block's start
+    // (0: none), after which blocks abandon the task they run and skip the
+    // rest; incomplete[plan] is set for every plan that lost a task.
+    unsigned long long budgetNs = 0;
+    int* incomplete = nullptr;
 };
 
 }  // namespace gr

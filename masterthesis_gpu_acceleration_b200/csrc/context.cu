@@ -409,7 +409,8 @@ void Staged::restage(Context& c, cudaStream_t s) {
     stage(c, p, ph, inSortTasks, s, inWalk, inCostAware, inAllowSort);
 }
 
-void Staged::enqueue(Context& c, cudaStream_t s, int instr, int gridCap) {
+void Staged::enqueue(Context& c, cudaStream_t s, int instr, int gridCap, unsigned long long budgetNs) {
+    budgeted = false;
     if (!nPlans) return;
     ck(cudaMemsetAsync(dResults.p, 0, (size_t)nPlans * sizeof(unsigned long long), s), "memset results");
     ck(cudaMemsetAsync(dCtl.p, 0, 8, s), "memset ctl");
@@ -425,6 +426,14 @@ void Staged::enqueue(Context& c, cudaStream_t s, int instr, int gridCap) {
         dBytes.ensure(8, streamOrdered ? s : nullptr);
         ck(cudaMemsetAsync(dBytes.p, 0, 8, s), "memset bytes");
         prof.bytes = static_cast<unsigned long long*>(dBytes.p);
+    }
+    if (budgetNs && instr == 1) {
+        dIncomplete.ensure((size_t)nPlans * sizeof(int), streamOrdered ? s : nullptr);
+        hIncomplete.ensure((size_t)nPlans * sizeof(int));
+        ck(cudaMemsetAsync(dIncomplete.p, 0, (size_t)nPlans * sizeof(int), s), "memset incomplete plans");
+        prof.budgetNs = budgetNs;
+        prof.incomplete = static_cast<int*>(dIncomplete.p);
+        budgeted = true;
     }
     int grid = std::max(1, std::min(nTasks, gridCap > 0 ? std::min(gridCap, c.grid) : c.grid));
     if (blockWords && (size_t)grid > blockRegions) throw CudaError("launch grid exceeds the block-row regions");
@@ -1086,6 +1095,8 @@ int gpu_set_option(void* ctx, const char* name, long long value) {
     }
     if (n == "serve_heavy_share" && value >= 1 && value <= 16) { c.serveHeavyShare = (int)value; return 0; }
     if (n == "serve_heavy_us" && value >= 0) { c.serveHeavyNs = 1e3 * (double)value; return 0; }
+    if (n == "serve_deadline_us" && value >= 0) { c.serveDeadlineNs = 1e3 * (double)value; return 0; }
+    if (n == "serve_max_us" && value >= 0) { c.serveMaxNs = 1e3 * (double)value; return 0; }
     if (n == "batch_phases" && value >= 1 && value <= 3) { c.batchPhases = (int)value; return 0; }
     if (n == "dedup_budget" && value >= 4096) { c.dedupBudget = (size_t)value; return 0; }
     if (n == "dedup_mode" && (value == 0 || value == kDedupRows || value == kDedupBlockRows || value == kDedupSort)) {

@@ -112,7 +112,7 @@ struct Context;
 // A set of plans and their tasks resident on the device, with the buffers
 // one launch over them needs.
 struct Staged {
-    DevBuf dBlob, dResults, dCtl, dBitmap, dHeavy, dBytes, dTaskNs, dSort;
+    DevBuf dBlob, dResults, dCtl, dBitmap, dHeavy, dBytes, dTaskNs, dSort, dIncomplete;
     std::vector<DevTask> hTasks;  // task list as uploaded (for profiles)
     std::vector<double> hCost;    // estimated work per uploaded task
     HostBuf hBlob, hResults, hCtl;
@@ -137,6 +137,8 @@ struct Staged {
     unsigned long long keyHint = 0;     // exact keys of a run that overflowed keyCap
     const int32_t* dSortSlots = nullptr;   // result slot of each sort index (in dBlob)
     HostBuf hSort;                      // the downloaded append cursor
+    HostBuf hIncomplete;                // per plan: a task was abandoned at the deadline
+    bool budgeted = false;              // the last enqueue ran under a deadline
     // inputs of the last staging, kept while it has sort-mode plans so that
     // an overflowing run can be staged again with the exact key count
     std::vector<DevPlan> inPlans;
@@ -160,8 +162,12 @@ struct Staged {
     void restage(Context& c, cudaStream_t s);
     // instr: 0 plain, 1 task times into dTaskNs, 2 also algorithmic bytes
     // into dBytes.  gridCap > 0 limits the launch to that many blocks (a
-    // share of the SMs).
-    void enqueue(Context& c, cudaStream_t s, int instr, int gridCap = 0);
+    // share of the SMs).  budgetNs > 0 (with instr 1): blocks stop that long
+    // after they start, and plan_incomplete() tells which plans lost work.
+    void enqueue(Context& c, cudaStream_t s, int instr, int gridCap = 0, unsigned long long budgetNs = 0);
+    bool plan_incomplete(int i) const {
+        return budgeted && static_cast<const int*>(hIncomplete.p)[i] != 0;
+    }
     // One launch per plan of an unsorted staging (at most kMaxPerPlan plans),
     // each with its own task counter, launch span and result in the 64
     // control bytes (counters and status at 0, spans at 16, results at
@@ -203,6 +209,9 @@ struct Staged {
         ck(cudaMemcpyAsync(hResults.p, dResults.p, nPlans * sizeof(unsigned long long), cudaMemcpyDeviceToHost, s), "D2H results");
         ck(cudaMemcpyAsync(hCtl.p, dCtl.p, 8, cudaMemcpyDeviceToHost, s), "D2H status");
         download_cursor(s);
+        if (budgeted)
+            ck(cudaMemcpyAsync(hIncomplete.p, dIncomplete.p, (size_t)nPlans * sizeof(int), cudaMemcpyDeviceToHost, s),
+               "D2H incomplete plans");
     }
     void download_cursor(cudaStream_t s) {
         if (nSort) ck(cudaMemcpyAsync(hSort.p, dSort.p, 8, cudaMemcpyDeviceToHost, s), "D2H key cursor");
@@ -263,6 +272,11 @@ struct Context {
     int serveLanes = 1;        // servers started on this context keep a heavy lane
     int serveHeavyShare = 2;   // the heavy lane launches on grid / serveHeavyShare blocks
     double serveHeavyNs = 5.0e6;
+    // servers started afterwards: a device-time budget per served launch
+    // (0: none) and a limit on a request's expected device time (0: none);
+    // requests beyond either complete with status -4
+    double serveDeadlineNs = 0.0;
+    double serveMaxNs = 0.0;
     // kPairs deduplication beyond the shared pool: device bytes that the
     // global dedup buffers of one launch may take before block rows or sort
     // mode replace per-phase rows, and a forced mode for every kPairs plan

@@ -59,6 +59,8 @@ template <int B>
 struct BlockState {
     static constexpr int kWarps = B / 32;
     int task;
+    int stop;                       // the block's deadline passed: abandon the task
+    unsigned long long deadline;    // global-timer ns (0: none)
     int curItem[kMaxBody + 1];      // a level's position, saved when the search descends below it
     long long curOff[kMaxBody + 1];
     int count[kMaxBody + 1];
@@ -373,6 +375,12 @@ __device__ __noinline__ int classify_item(const DevPlan& P, const DevIndex& ix, 
     return -3;
 }
 
+__device__ __forceinline__ unsigned long long global_ns() {
+    unsigned long long t;
+    asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+    return t;
+}
+
 // Sort mode: appends the pair key of (row, rank) to the plan's key buffer.
 // The threads that emit together take consecutive slots with one atomic; the
 // cursor keeps counting past the capacity, so the host learns the exact
@@ -387,7 +395,7 @@ __device__ __forceinline__ void emit_pair(const DevPlan& P, long long row, int r
     if (slot < P.keyCap) P.pairKeys[slot] = key;
 }
 
-template <int B, bool kC>
+template <int B, bool kC, bool kD>
 __device__ __forceinline__ void run_task(Smem<B>& sm, const DevIndex& ix, const DevTask& task,
                                          unsigned long long* results, int* status, Meter<kC>& mt) {
     constexpr int kLeafChunk = 16 * B;
@@ -805,7 +813,13 @@ __device__ __forceinline__ void run_task(Smem<B>& sm, const DevIndex& ix, const 
                     }
                 }
             }
+            if constexpr (kD) {
+                if (tid == 0 && global_ns() > S.deadline) S.stop = 1;
+            }
             __syncthreads();
+            if constexpr (kD) {
+                if (S.stop) break;   // set before the barrier, read by every thread after it: all leave together
+            }
             if (wide) {
                 const int ff = S.firstFail;   // final after the barrier
                 if (ff < take) {
@@ -849,29 +863,40 @@ __device__ __forceinline__ void run_task(Smem<B>& sm, const DevIndex& ix, const 
     if (tid == 0) mt.add(8);
 }
 
-__device__ __forceinline__ unsigned long long global_ns() {
-    unsigned long long t;
-    asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
-    return t;
-}
-
 // kI: 0 plain; 1 records each task's start and end time; 2 also counts
-// the algorithmic bytes.
+// the algorithmic bytes; 3 records task times under a deadline (served
+// launches: past prof.budgetNs from the block's start the block abandons
+// its task at the end of a frontier round, skips the rest, and marks the
+// plans that lost a task in prof.incomplete).
 template <int B, int kI>
 __global__ void __launch_bounds__(B, 1024 / B)
 engine_kernel(const __grid_constant__ DevIndex ix, const DevPlan* __restrict__ plans, const DevTask* __restrict__ tasks,
               int nTasks, int* taskCounter, unsigned long long* results, int* status, EngineProfile prof) {
     constexpr bool kC = kI == 2;
+    constexpr bool kD = kI == 3;
     extern __shared__ __align__(16) unsigned char smem_raw[];
     Smem<B>& sm = *reinterpret_cast<Smem<B>*>(smem_raw);
     Meter<kC> mt;
     if (prof.span && threadIdx.x == 0) atomicMax(prof.span, ~global_ns());
+    if constexpr (kD) {
+        if (threadIdx.x == 0) sm.st.deadline = global_ns() + prof.budgetNs;
+    }
     for (;;) {
-        if (threadIdx.x == 0) sm.st.task = atomicAdd(taskCounter, 1);
+        if (threadIdx.x == 0) {
+            sm.st.task = atomicAdd(taskCounter, 1);
+            if constexpr (kD) sm.st.stop = global_ns() > sm.st.deadline ? 1 : 0;
+        }
         __syncthreads();
         const int t = sm.st.task;
         if (t >= nTasks) break;
         const DevTask task = tasks[t];
+        if constexpr (kD) {
+            if (sm.st.stop) {   // past the deadline: the task is skipped and its plan marked
+                if (threadIdx.x == 0) atomicOr(prof.incomplete + task.plan, 1);
+                __syncthreads();
+                continue;
+            }
+        }
         unsigned long long t0 = 0;
         if constexpr (kI >= 1) {
             if (threadIdx.x == 0) {
@@ -883,8 +908,11 @@ engine_kernel(const __grid_constant__ DevIndex ix, const DevPlan* __restrict__ p
         int* dst = reinterpret_cast<int*>(&sm.plan);
         for (int i = threadIdx.x; i < (int)(sizeof(DevPlan) / 4); i += B) dst[i] = src[i];
         __syncthreads();
-        run_task<B, kC>(sm, ix, task, results, status, mt);
+        run_task<B, kC, kD>(sm, ix, task, results, status, mt);
         __syncthreads();
+        if constexpr (kD) {
+            if (threadIdx.x == 0 && sm.st.stop) atomicOr(prof.incomplete + task.plan, 1);
+        }
         if constexpr (kI >= 1) {
             if (threadIdx.x == 0 && prof.taskNs) {
                 prof.taskNs[2 * t] = t0;
@@ -908,6 +936,8 @@ static cudaError_t configure_b() {
         e = cudaFuncSetAttribute(engine_kernel<B, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
     if (e == cudaSuccess)
         e = cudaFuncSetAttribute(engine_kernel<B, 2>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+    if (e == cudaSuccess)
+        e = cudaFuncSetAttribute(engine_kernel<B, 3>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
     return e;
 }
 
@@ -934,6 +964,8 @@ static void launch_b(const DevIndex& ix, const DevPlan* plans, const DevTask* ta
     const EngineProfile p = prof ? *prof : EngineProfile{};
     if (p.bytes)
         engine_kernel<B, 2><<<grid, B, smem, stream>>>(ix, plans, tasks, nTasks, taskCounter, results, status, p);
+    else if (p.budgetNs && p.incomplete && p.taskNs)
+        engine_kernel<B, 3><<<grid, B, smem, stream>>>(ix, plans, tasks, nTasks, taskCounter, results, status, p);
     else if (p.taskNs)
         engine_kernel<B, 1><<<grid, B, smem, stream>>>(ix, plans, tasks, nTasks, taskCounter, results, status, p);
     else

@@ -134,7 +134,16 @@ struct Server {
             sup[i] = s.reqs[i].rp.support.value;
             body[i] = s.reqs[i].rp.body.value;
         }
-        if (status == 0 && s.timed) {
+        // requests that lost device work at the launch's deadline
+        std::vector<char> late(s.reqs.size(), 0);
+        bool anyLate = false;
+        if (status == 0)
+            for (size_t k = 0; k < s.owner.size(); ++k)
+                if (s.st.plan_incomplete((int)k)) {
+                    late[(size_t)s.owner[k] / 2] = 1;
+                    anyLate = true;
+                }
+        if (status == 0 && s.timed && !anyLate) {   // abandoned tasks have no times to learn from
             const auto h0 = Clock::now();
             c->tasks->learn(s.phases, s.st.hTasks, s.st.hCost,
                             static_cast<const unsigned long long*>(s.hTaskNs.p), s.grid, 0.5, kWalkAfterNs);
@@ -150,7 +159,7 @@ struct Server {
         }
         {
             std::lock_guard<std::mutex> lk(mu);
-            for (size_t i = 0; i < s.reqs.size(); ++i) publish(s.reqs[i], status, sup[i], body[i], now);
+            for (size_t i = 0; i < s.reqs.size(); ++i) publish(s.reqs[i], late[i] ? -4 : status, sup[i], body[i], now);
             completed += (long long)s.reqs.size();
             memInUse -= s.mem;
         }
@@ -186,6 +195,8 @@ struct Server {
                 if (q.mem > memBudget) { q.status = -2; q.mem = 0; }
                 if (q.rp.status == kRuleOk)
                     ns = c->tasks->expected_ns(q.rp.support) + c->tasks->expected_ns(q.rp.body);
+                // refused without a launch: expected to take longer than the limit
+                if (q.status == 0 && c->serveMaxNs > 0 && ns > c->serveMaxNs) { q.status = -4; q.mem = 0; ns = 0; }
             }
             q.ns = ns;
         }, 64);
@@ -253,7 +264,8 @@ struct Server {
         s.grid = s.heavyLane ? std::max(1, c->grid / c->serveHeavyShare) : c->grid;
         s.phases = phases;
         ck(cudaEventRecord(s.start, s.stream), "event");
-        s.st.enqueue(*c, s.stream, s.timed ? 1 : 0, s.heavyLane ? s.grid : 0);
+        s.st.enqueue(*c, s.stream, s.timed ? 1 : 0, s.heavyLane ? s.grid : 0,
+                     s.timed ? (unsigned long long)c->serveDeadlineNs : 0ull);
         ck(cudaEventRecord(s.kend, s.stream), "event");
         s.st.download(s.stream);
         if (s.timed) {

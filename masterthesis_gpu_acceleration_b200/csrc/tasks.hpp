@@ -69,6 +69,10 @@ public:
     // Estimated candidate bindings of a phase (average fan-outs; exact first
     // two levels for chain-shaped plans rooted at the first step's rows).
     double work_estimate(const PhasePlan& ph) { return estimate2(ph); }
+    // The hub-aware estimate: every expansion at the size-biased fan-out of
+    // its (predicate, direction), i.e. as if each step landed where a random
+    // edge lands (an upper-side estimate for rules through hub entities).
+    double hub_estimate(const PhasePlan& ph) { return estimate(ph, true); }
 
     size_t cache_bytes() const { return cacheBytes_; }
 

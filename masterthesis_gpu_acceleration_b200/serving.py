@@ -86,10 +86,12 @@ def run_rate_multi(graphs, rate: float, duration: float, seed: int = 0, weights=
     every = np.concatenate([np.array(x) for x in lat if x]) if any(lat) else np.zeros(1)
     completed = sum(len(r) for r in results)
     ok = sum(1 for r in results for v in r.values() if v[1] == 0)
+    shed = sum(1 for r in results for v in r.values() if v[1] == -4)
     summ = {
         "offered_rules_per_s": rate,
         "submitted": n,
         "completed_ok": ok,
+        "shed_over_time_limits": shed,
         "sustained_rules_per_s": completed / t_end if t_end > 0 else 0.0,
         "achieved_arrival_rate": n / t_sub if t_sub > 0 else 0.0,
         "p50_ms": float(np.percentile(every, 50)),

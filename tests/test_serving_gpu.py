@@ -102,3 +102,42 @@ def test_serving_reports_bad_rules(tmp_path):
             got = _collect(sv, 2)
     assert got[1][0] == -1
     assert got[2][0] == 0 and got[2][1]["bodySize"] == fx["cases"][0]["expected"]["bodySize"]
+
+
+def test_serving_time_limits(data_dir):
+    """A served launch past its deadline abandons its work: the requests that
+    lost work complete with status -4 and a zero result, every other result
+    stays exact.  A limit on expected device time refuses requests at
+    admission with the same status; without limits everything is exact."""
+    fx = load_fixture("synthetic_c4s.json")
+    d = synth.generate("c4s", data_dir / "c4s", seed=fx["seed"])
+    exp = {i: [e["support"], e["headSize"], e["headSupport"], e["bodySize"]] for i, e in enumerate(fx["expected"])}
+    rules = fx["rules"]
+
+    def serve_all():
+        with lib.serve(slots=2, max_batch=8) as sv:
+            for i, r in enumerate(rules):
+                sv.submit(i, r)
+            return _collect(sv, len(rules))
+
+    with eng.GpuRulesLib(d / "graph.ttl") as lib:
+        lib.set_option("serve_deadline_us", 20)
+        got = serve_all()
+        late = [i for i, (st, _, _) in got.items() if st == -4]
+        assert late, "a 20 us deadline must stop the hub rules"
+        for i, (st, res, _) in got.items():
+            assert st in (0, -4)
+            counts = [res["support"], res["headSize"], res["headSupport"], res["bodySize"]]
+            assert counts == (exp[i] if st == 0 else [0, 0, 0, 0]), i
+        lib.set_option("serve_deadline_us", 0)
+        lib.set_option("serve_max_us", 1)
+        got = serve_all()
+        refused = [i for i, (st, _, _) in got.items() if st == -4]
+        assert len(refused) >= len(rules) // 2, "a 1 us limit refuses (nearly) every rule"
+        for i, (st, res, _) in got.items():
+            counts = [res["support"], res["headSize"], res["headSupport"], res["bodySize"]]
+            assert counts == (exp[i] if st == 0 else [0, 0, 0, 0]), i
+        lib.set_option("serve_max_us", 0)
+        got = serve_all()
+        for i, (st, res, _) in got.items():
+            assert st == 0 and [res["support"], res["headSize"], res["headSupport"], res["bodySize"]] == exp[i], i
