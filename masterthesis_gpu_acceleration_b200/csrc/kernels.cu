@@ -629,8 +629,10 @@ __device__ __forceinline__ void run_task(Smem<B>& sm, const DevIndex& ix, const 
             // again then, which changes no count (every dedup structure is a
             // set counted on insertion).  A level that overflowed takes
             // capacity-sized rounds, which cannot overflow, until it is
-            // exhausted, so the search always advances.
-            const bool wide = sigTest && !((S.safeLevels >> k) & 1u);
+            // exhausted, so the search always advances.  Sort mode keeps
+            // capacity-sized rounds: its key count must not depend on how
+            // the threads raced (a launch is staged again with that count).
+            const bool wide = sigTest && !sortMode && !((S.safeLevels >> k) & 1u);
             const long long take = min(total, (long long)(leaf ? kLeafChunk : (wide ? kWideChunk : P.cap)));
             const int lenN = leaf ? 0 : P.tupleLen[k + 1];
             const int strideN = lenN + 2;
