@@ -649,7 +649,10 @@ void prepare(Batch& b, Context& c, const char* const* rules, int n, int isJson, 
     if (keepPlans) b.plans0 = plans;
     else b.plans0.clear();
     b.phases = phases;
-    b.st.stage(c, plans, phases, true, b.stream, b.walkBudget);
+    // a one-shot batch walks a phase only when the walk costs less host time
+    // than the phase is expected to take on the device; a prepared batch,
+    // replayed many times, walks every phase the budget allows
+    b.st.stage(c, plans, phases, true, b.stream, b.walkBudget, !keepPlans);
 }
 
 void collect(const Batch& b, GpuRuleResult* out, int* status) {

@@ -236,6 +236,9 @@ TaskBuilder::Walk TaskBuilder::compute_walk(const PhasePlan& ph) {
     const DevStep& s1 = P.steps[1];
     if (chain && P.mode == kPairs && P.m == 3 && P.memoLevel == 2 && memoRows)
         memo = memoRows(s1.pred, s1.dir, P.steps[2].pred, P.steps[2].dir, &memoCost);
+    // a second step that scans, or expands from a root value or a constant,
+    // costs the same after every edge of the first step
+    const bool uniformChild = P.m >= 2 && (s1.kind == kScan || s1.keyRef < P.tupleLen[0]);
     std::vector<float> w((size_t)(ph.rootEnd - ph.rootBeg));
     int32_t vals[2];
     for (int32_t r = ph.rootBeg; r < ph.rootEnd; ++r) {
@@ -255,6 +258,11 @@ TaskBuilder::Walk TaskBuilder::compute_walk(const PhasePlan& ph) {
         } else if (chain) {
             acc += seg.second - seg.first;
             if (seg.second > seg.first) acc += h->perRow[ix_.srcRank[P.steps[0].dir][seg.first]] * tail;
+        } else if (uniformChild) {
+            // the second step does not depend on the first step's value:
+            // every edge of the segment costs the same
+            if (seg.second > seg.first)
+                acc += (double)(seg.second - seg.first) * child_work(P, vals, seg.first, deg2, tail);
         } else
             for (int32_t e = seg.first; e < seg.second; ++e) acc += child_work(P, vals, e, deg2, tail);
         w[r - ph.rootBeg] = (float)acc;
