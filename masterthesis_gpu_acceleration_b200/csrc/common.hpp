@@ -147,7 +147,9 @@ struct DevPlan {
                                   // kExist plans ending in x -> y and the check (h, y) (memo_exists)
     int32_t memoP2, memoD2;       // the memo's second relation: y -> h through (memoP2, memoD2) rows
     TermRef memoH;                // kExist: tuple ref of h
-    int16_t pad2;
+    int8_t memoSteps;             // kPairs: 3 for a three-step suffix memo x -> v2 -> v3 -> hO (memo3_item),
+                                  // otherwise the two-step one
+    int8_t pad2;
     int32_t memoWords;            // words per memo bitmap (the rows of (memoP2, 1 - memoD2))
     const int32_t* memoTab;       // per hub row: memo slot or -1 (null: no memo)
     const uint32_t* memoBits;     // per slot: S1 then S2, memoWords words each
@@ -195,10 +197,13 @@ struct Geom {
 // Profiling outputs of the instrumented kernel variant (null members are
 // skipped): requested global-memory bytes, and per task its start and end
 // time (globaltimer ns).
-// One suffix-memo bitmap pair to build: hub row `row` of (p1, d1) through
-// (p2, d2), `words` words per bitmap at `bits` (S1, then S2).
+// One suffix memo to build for hub row `row` of (p1, d1).  Two steps
+// (p3 < 0): through (p2, d2), bitmaps S1 then S2 of `words` words at `bits`.
+// Three steps: through (p2, d2) then (p3, d3), the bitmap S1 (`words`
+// words) then one 32-bit path count per rank of the domain (`wo` ranks).
 struct MemoJob {
     int32_t p1, d1, p2, d2, row, words;
+    int32_t p3, d3, wo, pad;
     uint32_t* bits;
 };
 

@@ -169,12 +169,22 @@ void Staged::stage(Context& c, std::vector<DevPlan>& plans, const std::vector<co
         hSort.ensure(8);
     }
     // suffix memos first: the task builder weighs memoised roots by them
-    std::vector<std::array<int, 4>> memoKeys;
-    for (int i = 0; i < nPlans; ++i)
-        if (plans[i].memoLevel > 0) {
-            const DevStep& a = plans[i].steps[plans[i].memoLevel - 1];
-            memoKeys.push_back({a.pred, a.dir, plans[i].memoP2, plans[i].memoD2});
+    std::vector<std::array<int, 6>> memoKeys;
+    auto memo_key_of = [](const DevPlan& P) -> std::array<int, 6> {
+        const DevStep& a = P.steps[P.memoLevel - 1];
+        if (P.memoSteps == 3) {
+            const DevStep& c3 = P.steps[P.memoLevel + 1];
+            return {a.pred, a.dir, P.memoP2, P.memoD2, c3.pred, c3.dir};
         }
+        return {a.pred, a.dir, P.memoP2, P.memoD2, -1, 0};
+    };
+    for (int i = 0; i < nPlans; ++i) {
+        if (plans[i].memoSteps == 3 && !c.memo3) {   // three-step memos switched off: enumerate
+            plans[i].memoLevel = 0;
+            plans[i].memoSteps = 0;
+        }
+        if (plans[i].memoLevel > 0 && dedup[i] != kDedupSort) memoKeys.push_back(memo_key_of(plans[i]));
+    }
     if (!memoKeys.empty()) c.ensure_memos(memoKeys, s);
     std::vector<PhaseTasks> pts;
     c.tasks->build(phases, c.grid, true, pts, walkBudget, costAware, &lim);
@@ -192,9 +202,10 @@ void Staged::stage(Context& c, std::vector<DevPlan>& plans, const std::vector<co
         plans[i].memoTab = nullptr;
         plans[i].memoBits = nullptr;
         if (plans[i].memoLevel > 0) {
-            const DevStep& a = plans[i].steps[plans[i].memoLevel - 1];
-            const SuffixMemo* m = c.memo_for(a.pred, a.dir, plans[i].memoP2, plans[i].memoD2);
-            if (m && (plans[i].mode != kPairs || m->words == plans[i].rowWords)) {
+            const std::array<int, 6> k = memo_key_of(plans[i]);
+            const SuffixMemo* m = c.memo_for(k[0], k[1], k[2], k[3], k[4], k[5]);
+            if (m && (plans[i].mode != kPairs || m->words == plans[i].rowWords) &&
+                (plans[i].memoSteps != 3 || m->wo == plans[i].wo)) {
                 plans[i].memoTab = m->tab;
                 plans[i].memoBits = m->bits;
                 plans[i].memoWords = m->words;
@@ -299,57 +310,78 @@ void Staged::stage(Context& c, std::vector<DevPlan>& plans, const std::vector<co
 }
 
 namespace {
-uint64_t memo_key(int p1, int d1, int p2, int d2) {
-    return ((uint64_t)(uint32_t)(p1 * 2 + d1) << 32) | (uint32_t)(p2 * 2 + d2);
+// Two-step memos keep the task builder's key ((p1, d1) and (p2, d2) in 32
+// bits each); three-step keys set the top bit and pack 21 bits per step.
+uint64_t memo_key(int p1, int d1, int p2, int d2, int p3 = -1, int d3 = 0) {
+    if (p3 < 0) return ((uint64_t)(uint32_t)(p1 * 2 + d1) << 32) | (uint32_t)(p2 * 2 + d2);
+    return (1ull << 63) | ((uint64_t)(uint32_t)(p1 * 2 + d1) << 42) | ((uint64_t)(uint32_t)(p2 * 2 + d2) << 21) |
+           (uint64_t)(uint32_t)(p3 * 2 + d3);
 }
 }  // namespace
 
-const SuffixMemo* Context::memo_for(int p1, int d1, int p2, int d2) const {
-    auto it = memos.find(memo_key(p1, d1, p2, d2));
+const SuffixMemo* Context::memo_for(int p1, int d1, int p2, int d2, int p3, int d3) const {
+    auto it = memos.find(memo_key(p1, d1, p2, d2, p3, d3));
     return it == memos.end() ? nullptr : it->second.get();
 }
 
-void Context::ensure_memos(const std::vector<std::array<int, 4>>& keys, cudaStream_t s) {
+void Context::ensure_memos(const std::vector<std::array<int, 6>>& keys, cudaStream_t s) {
     const HostIndex& h = hix;
     const int nHub = (int)h.hubOff.size();
-    std::vector<std::array<int, 4>> fresh;
+    std::vector<std::array<int, 6>> fresh;
     for (const auto& k : keys) {
-        const int p1 = k[0], d1 = k[1], p2 = k[2], d2 = k[3];
-        const uint64_t key = memo_key(p1, d1, p2, d2);
+        const int p1 = k[0], p2 = k[2], p3 = k[4];
+        const uint64_t key = memo_key(k[0], k[1], k[2], k[3], k[4], k[5]);
         if (memos.count(key)) continue;
         memos[key] = nullptr;
-        if (memoGain < 0 || nHub == 0 || p1 < 0 || p2 < 0 || p1 >= h.nPred || p2 >= h.nPred) continue;
+        if (memoGain < 0 || nHub == 0 || p1 < 0 || p2 < 0 || p1 >= h.nPred || p2 >= h.nPred || p3 >= h.nPred) continue;
+        if (p3 >= 0 && h.nPred >= (1 << 20)) continue;
         fresh.push_back(k);
     }
     if (fresh.empty()) return;
-    // the hub rows of (p1, d1) worth a memo, per new transition, on host
-    // threads: a row's suffix candidates are the second-step degrees of its
-    // values summed
+    // the rank domain of a memo: the rows of its last step's predicate in
+    // the other direction
+    auto domain = [&](const std::array<int, 6>& k) -> int64_t {
+        return k[4] >= 0 ? h.pred_rows(k[4], 1 - k[5]) : h.pred_rows(k[2], 1 - k[3]);
+    };
+    // the hub rows of (p1, d1) worth a memo, per new key, on host threads:
+    // a row's suffix candidates are what enumeration would visit after x
     std::vector<std::vector<int32_t>> rowsOf(fresh.size());
     parallel_for(fresh.size(), [&](size_t i) {
         const int p1 = fresh[i][0], d1 = fresh[i][1], p2 = fresh[i][2], d2 = fresh[i][3];
-        const int words = (int)((h.pred_rows(p2, 1 - d2) + 31) / 32);
-        const int32_t* deg = tasks->degrees(p2, d2);
+        const int p3 = fresh[i][4], d3 = fresh[i][5];
+        const int words = (int)((domain(fresh[i]) + 31) / 32);
+        const int32_t* deg = tasks->degrees(p3 >= 0 ? p3 : p2, p3 >= 0 ? d3 : d2);
         for (int32_t r = h.predRow[d1][p1]; r < h.predRow[d1][p1 + 1]; ++r) {
             if (h.hubOf[d1][r] < 0) continue;
             double cand = 0;
-            for (int32_t e = h.rowBeg[d1][r]; e < h.rowBeg[d1][r + 1]; ++e) cand += deg[h.val[d1][e]];
+            for (int32_t e = h.rowBeg[d1][r]; e < h.rowBeg[d1][r + 1]; ++e) {
+                if (p3 < 0) {
+                    cand += deg[h.val[d1][e]];
+                } else {
+                    const auto r2 = h.row_range(p2, d2, h.val[d1][e]);
+                    for (int32_t e2 = r2.first; e2 < r2.second; ++e2) cand += 1.0 + deg[h.val[d2][e2]];
+                }
+            }
             if (cand >= memoGain * words) rowsOf[i].push_back(r);
         }
     }, 1);
+    // per memo slot: S1 and S2 (two steps), or S1 and one count per rank
+    auto slot_words = [&](const std::array<int, 6>& k) -> size_t {
+        const size_t words = (size_t)((domain(k) + 31) / 32);
+        return k[4] >= 0 ? words + (size_t)domain(k) : 2 * words;
+    };
     // within the memory budget, in key order: one device allocation holding
     // every new memo's hub table, then every new memo's bits
     const size_t tabBytes = ((size_t)nHub * 4 + 255) & ~size_t(255);
     std::vector<size_t> take, bitOff;
     size_t bitTotal = 0;
     for (size_t i = 0; i < fresh.size(); ++i) {
-        const int words = (int)((h.pred_rows(fresh[i][2], 1 - fresh[i][3]) + 31) / 32);
-        const size_t bytes = tabBytes + rowsOf[i].size() * 2 * (size_t)words * 4;
+        const size_t bytes = tabBytes + rowsOf[i].size() * slot_words(fresh[i]) * 4;
         if (rowsOf[i].empty() || memoBytes + bytes > kMemoBudgetBytes) continue;
         memoBytes += bytes;
         take.push_back(i);
         bitOff.push_back(bitTotal);
-        bitTotal += rowsOf[i].size() * 2 * (size_t)words * 4;
+        bitTotal += rowsOf[i].size() * slot_words(fresh[i]) * 4;
     }
     if (take.empty()) return;
     const size_t tabTotal = tabBytes * take.size();
@@ -363,7 +395,10 @@ void Context::ensure_memos(const std::vector<std::array<int, 4>>& keys, cudaStre
     for (size_t t = 0; t < take.size(); ++t) {
         const size_t i = take[t];
         const int p1 = fresh[i][0], d1 = fresh[i][1], p2 = fresh[i][2], d2 = fresh[i][3];
-        const int words = (int)((h.pred_rows(p2, 1 - d2) + 31) / 32);
+        const int p3 = fresh[i][4], d3 = fresh[i][5];
+        const int wo = (int)domain(fresh[i]);
+        const int words = (wo + 31) / 32;
+        const size_t stride = slot_words(fresh[i]);
         int32_t* tab = tabs.data() + t * (tabBytes / 4);
         uint32_t* bits = reinterpret_cast<uint32_t*>(base + tabTotal + bitOff[t]);
         auto m = std::make_unique<SuffixMemo>();
@@ -372,13 +407,14 @@ void Context::ensure_memos(const std::vector<std::array<int, 4>>& keys, cudaStre
         for (size_t j = 0; j < rows.size(); ++j) {
             tab[h.hubOf[d1][rows[j]]] = (int32_t)j;
             m->rowHasMemo[(size_t)(rows[j] - h.predRow[d1][p1])] = 1;
-            all.push_back(MemoJob{p1, d1, p2, d2, rows[j], words, bits + j * 2 * (size_t)words});
+            all.push_back(MemoJob{p1, d1, p2, d2, rows[j], words, p3, d3, wo, 0, bits + j * stride});
         }
         m->tab = reinterpret_cast<const int32_t*>(base + t * tabBytes);
         m->bits = bits;
         m->words = words;
+        m->wo = p3 >= 0 ? wo : 0;
         m->slots = (int)rows.size();
-        memos[memo_key(p1, d1, p2, d2)] = std::move(m);
+        memos[memo_key(p1, d1, p2, d2, p3, d3)] = std::move(m);
     }
     ck(cudaMemcpyAsync(base, tabs.data(), tabTotal, cudaMemcpyHostToDevice, s), "H2D memo tables");
     ck(cudaMemsetAsync(base + tabTotal, 0, bitTotal, s), "clear memo bits");
@@ -727,12 +763,16 @@ namespace {
 // The rest of a load, whichever source the index came from: the state built
 // on the index, and its upload.
 void finish_load(Context* c) {
+    // GPU_RULES_MEMO3=0 switches the three-step suffix memos off
+    if (const char* m = std::getenv("GPU_RULES_MEMO3")) c->memo3 = std::atoi(m) != 0;
     c->tasks.reset(new TaskBuilder(c->hix));
-    c->tasks->memoRows = [c](int p1, int d1, int p2, int d2, double* cost) -> const std::vector<uint8_t>* {
-        const uint64_t key = ((uint64_t)(uint32_t)(p1 * 2 + d1) << 32) | (uint32_t)(p2 * 2 + d2);
-        auto it = c->memos.find(key);
+    c->tasks->memoRows = [c](int p1, int d1, int p2, int d2, int p3, int d3,
+                             double* cost) -> const std::vector<uint8_t>* {
+        auto it = c->memos.find(memo_key(p1, d1, p2, d2, p3, d3));
         if (it == c->memos.end() || !it->second) return nullptr;
-        *cost = it->second->words / 4.0 + 8.0;   // a memo word costs about a quarter of a candidate
+        // a memo word costs about a quarter of a candidate; a three-step item
+        // also looks up the rows its root reaches
+        *cost = it->second->words / 4.0 + (p3 >= 0 ? 32.0 : 8.0);
         return &it->second->rowHasMemo;
     };
     c->parser.reset(new RuleParser(c->ents, c->preds, c->prefixes));

@@ -235,6 +235,7 @@ struct SuffixMemo {   // its table and bits live in one of Context::memoChunks
     const int32_t* tab = nullptr;
     const uint32_t* bits = nullptr;
     int words = 0;
+    int wo = 0;          // three-step memos: ranks of the domain (one path count each)
     int slots = 0;
     std::vector<uint8_t> rowHasMemo;   // per row of (p1, d1), from the predicate's first row
 };
@@ -258,16 +259,19 @@ struct Context {
     // suffix memos: a hub row gets one when its suffix candidates are at
     // least memoGain x the memo's words (negative: no memos)
     double memoGain = 0.25;
+    bool memo3 = true;         // three-step suffix memos (memo3_item) for the plans that admit one
     std::unordered_map<uint64_t, std::unique_ptr<SuffixMemo>> memos;
     std::vector<std::unique_ptr<DevBuf>> memoChunks;   // one allocation per ensure_memos call
     size_t memoBytes = 0;
-    // Builds the memos of the transitions (p1, d1) -> (p2, d2) in `keys`
-    // that do not exist yet: one kernel over all their hub rows, one
-    // synchronisation of stream s (memos are shared by every stream after).
-    void ensure_memos(const std::vector<std::array<int, 4>>& keys, cudaStream_t s);
-    // The memo of (p1, d1) -> (p2, d2) if built, null when none exists or no
-    // hub row of (p1, d1) is worth one.
-    const SuffixMemo* memo_for(int p1, int d1, int p2, int d2) const;
+    // Builds the memos in `keys` that do not exist yet, {p1, d1, p2, d2, p3,
+    // d3}: the transitions (p1, d1) -> (p2, d2), or with p3 >= 0 the
+    // three-step suffixes (p1, d1) -> (p2, d2) -> (p3, d3): one kernel over
+    // all their hub rows, one synchronisation of stream s (memos are shared
+    // by every stream afterwards).
+    void ensure_memos(const std::vector<std::array<int, 6>>& keys, cudaStream_t s);
+    // The memo of a key if built, null when none exists or no hub row of
+    // (p1, d1) is worth one.
+    const SuffixMemo* memo_for(int p1, int d1, int p2, int d2, int p3 = -1, int d3 = 0) const;
     DevBuf memoJobs;
     int serveLanes = 1;        // servers started on this context keep a heavy lane
     int serveHeavyShare = 2;   // the heavy lane launches on grid / serveHeavyShare blocks

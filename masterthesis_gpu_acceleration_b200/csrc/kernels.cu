@@ -229,6 +229,122 @@ __device__ __forceinline__ unsigned long long block_sum(unsigned long long x, Bl
     return t;  // valid in thread 0
 }
 
+// List capacity of a three-step memo item's exceptions (plus one slot for
+// the root's own rank) in the warp's kMaxVars-int buffer.
+constexpr int kMemo3List = kMaxVars - 1;
+
+// Three-step suffix memos, for body-size plans hS -> x -> v2 -> v3 -> hO
+// (memoSteps == 3) at an item (a, x) whose x is a memoised hub row.  The
+// memo of x holds S1 = {h : C(h) > 0} and C(h), the number of paths
+// x -> v2 -> v3 -> h with x, v2, v3, h distinct.  The item's pairs are the
+// h != a with a path that also avoids a, i.e. with C(h) > C_a(h), C_a(h)
+// the paths through a:
+//   a = v2 (when a is a neighbour of x): v3 in N2(a) \ {x, a, h}, h in N3(v3);
+//   a = v3: v2 in N1(x) with a in N2(v2), v2 not in {x, a, h}, and h in N3(a).
+// Only h reached that way (listed, at most kMemo3List by the check in
+// classify_item) can have C_a(h) > 0; every other bit of S1 stands.
+// memo3_exceptions lists the ranks to clear from S1 and memo_item applies
+// them.  Its parts are small leaf functions called one after the other, so
+// that few of the caller's registers need to be free for them.
+//
+// memo3_count (whole warp): 2 * K + [a in N1(x)], K = #{v2 in N1(x) : a in
+// N2(v2), v2 not in {x, a}} (lanes split a's reverse row under step 2).
+template <bool kC>
+__device__ __noinline__ int memo3_count(const DevPlan& P, const DevIndex& ix, const int* par, int lenK, int lane,
+                                        Meter<kC>& mt) {
+    const int p2 = P.steps[2].pred, d2 = P.steps[2].dir;
+    const int* v1 = ix.val[P.steps[1].dir];
+    const int a = par[kTupleHead], x = par[kTupleHead + 1];
+    const int segBeg = par[lenK], segLen = par[lenK + 1];   // x's row under step 1
+    const int2 rInv = row_lookup(ix, p2, 1 - d2, a, mt);
+    int k = 0;
+    for (int e = rInv.x + lane; e < rInv.y; e += 32) {
+        const int u = __ldg(ix.val[1 - d2] + e);
+        mt.add(4);
+        if (u != x && u != a && seg_has(v1, segBeg, segLen, u, mt)) ++k;
+    }
+    return 2 * __reduce_add_sync(0xffffffffu, k) + (seg_has(v1, segBeg, segLen, a, mt) ? 1 : 0);
+}
+
+// memo3_list (one lane): the ranks of the h a path through a reaches, into
+// ex[0..n) (repeats allowed), and a's own rank (h != a) into ex[n] (-1 when
+// a is outside hO's domain); returns n.
+template <bool kC>
+__device__ __noinline__ int memo3_list(const DevPlan& P, const DevIndex& ix, const int* par, int kv, int* ex,
+                                       Meter<kC>& mt) {
+    const int p2 = P.steps[2].pred, d2 = P.steps[2].dir;
+    const int p3 = P.steps[3].pred, d3 = P.steps[3].dir;
+    const int a = par[kTupleHead], x = par[kTupleHead + 1];
+    int n = 0;
+    if (kv & 1) {
+        const int2 r2a = row_lookup(ix, p2, d2, a, mt);
+        for (int e2 = r2a.x; e2 < r2a.y; ++e2) {
+            const int v3 = __ldg(ix.val[d2] + e2);
+            if (v3 == x || v3 == a) continue;
+            const int2 r3 = row_lookup(ix, p3, d3, v3, mt);
+            for (int e3 = r3.x; e3 < r3.y && n < kMemo3List; ++e3) {
+                const int h = __ldg(ix.val[d3] + e3);
+                if (h != x && h != a && h != v3) ex[n++] = __ldg(ix.valRank[d3] + e3);
+            }
+        }
+    }
+    const int2 r3a = row_lookup(ix, p3, d3, a, mt);
+    for (int e3 = r3a.x; e3 < r3a.y && n < kMemo3List; ++e3) {
+        const int h = __ldg(ix.val[d3] + e3);
+        if (h != x && h != a) ex[n++] = __ldg(ix.valRank[d3] + e3);
+    }
+    const int2 ra = row_lookup(ix, p3, 1 - d3, a, mt);
+    ex[n] = ra.y > ra.x ? __ldg(ix.srcRank[1 - d3] + ra.x) : -1;
+    return n;
+}
+
+// memo3_keep (one lane per listed rank r): whether a path avoiding a still
+// reaches r's value h, i.e. C(h) > C_a(h).
+template <bool kC>
+__device__ __noinline__ bool memo3_keep(const DevPlan& P, const DevIndex& ix, const int* par, int lenK, int r,
+                                        int kv, const uint32_t* C, Meter<kC>& mt) {
+    const unsigned c = __ldg(C + r);
+    mt.add(4);
+    const int p3 = P.steps[3].pred, d3 = P.steps[3].dir;
+    const int a = par[kTupleHead];
+    const int h = __ldg(ix.rowKey[1 - d3] + __ldg(ix.predRow[1 - d3] + p3) + r);
+    unsigned ca = 0;
+    if (has_edge(ix, p3, d3, a, h, mt)) {   // paths with v3 = a
+        const int p2 = P.steps[2].pred, d2 = P.steps[2].dir;
+        const bool hIsV2 = has_edge(ix, p2, 1 - d2, a, h, mt) &&
+                           seg_has(ix.val[P.steps[1].dir], par[lenK], par[lenK + 1], h, mt);
+        ca = (unsigned)((kv >> 1) - (hIsV2 ? 1 : 0));
+    }
+    if (kv & 1) {   // paths with v2 = a
+        const int p2 = P.steps[2].pred, d2 = P.steps[2].dir;
+        const int x = par[kTupleHead + 1];
+        const int2 r2a = row_lookup(ix, p2, d2, a, mt);
+        for (int e2 = r2a.x; e2 < r2a.y && ca < c; ++e2) {
+            const int v3 = __ldg(ix.val[d2] + e2);
+            if (v3 != x && v3 != a && v3 != h && has_edge(ix, p3, d3, v3, h, mt)) ++ca;
+        }
+    }
+    return c > ca;
+}
+
+// The exceptions of an item (whole warp): ex[0..n] holds the ranks to clear
+// from S1 of memo slot `slot` (-1: none); returns n + 1.
+template <bool kC>
+__device__ __forceinline__ int memo3_exceptions(const DevPlan& P, const DevIndex& ix, const int* par, int lenK,
+                                                int slot, int words, int* ex, int lane, Meter<kC>& mt) {
+    const int kv = memo3_count(P, ix, par, lenK, lane, mt);
+    int n = 0;
+    if (lane == 0) n = memo3_list(P, ix, par, kv, ex, mt);
+    n = __shfl_sync(0xffffffffu, n, 0);
+    __syncwarp();
+    if (lane < n) {
+        const uint32_t* C = P.memoBits + (long long)slot * ((long long)words + P.wo) + words;
+        if (memo3_keep(P, ix, par, lenK, ex[lane], kv, C, mt)) ex[lane] = -1;   // still reached: keep its bit
+    }
+    __syncwarp();
+    return n + 1;
+}
+
 // One level-k item whose first suffix step expands a hub row x with a memo:
 // for the plan suffix x -[stA]-> y -[stB]-> hO, the memo holds, over hO's
 // rank domain, S1 = {h : at least one y in N1(x) with h in N2(y), h != y}
@@ -244,27 +360,33 @@ template <bool kC>
 __device__ __noinline__ unsigned long long memo_item(const DevPlan& P, const DevIndex& ix, const DevStep stA,
                                                      const DevStep stB, const int* par, int lenK, int slot,
                                                      uint32_t* dst, int words, int* ex, int lane, Meter<kC>& mt,
-                                                     bool sharedDst) {
+                                                     bool sharedDst, int nEx3) {
     unsigned long long myNew = 0;
-    const int nEx = lenK - kTupleHead;
-    const int exDir = 1 - stB.dir;
-    const int segBeg = par[lenK], segLen = par[lenK + 1];
-    bool isW = false;
-    if (lane < nEx) {
-        const int u = par[kTupleHead + lane];
-        const int2 r = row_lookup(ix, stB.pred, exDir, u, mt);
-        ex[lane] = r.y > r.x ? __ldg(ix.srcRank[exDir] + r.x) : -1;
-        isW = seg_has(ix.val[stA.dir], segBeg, segLen, u, mt);
+    const bool three = nEx3 > 0;
+    const uint32_t* S1 = P.memoBits + (long long)slot * (three ? (long long)words + P.wo : 2LL * words);
+    int nEx = lenK - kTupleHead;
+    unsigned wmask = 0;
+    if (three) {
+        nEx = nEx3;
+    } else {
+        const int exDir = 1 - stB.dir;
+        const int segBeg = par[lenK], segLen = par[lenK + 1];
+        bool isW = false;
+        if (lane < nEx) {
+            const int u = par[kTupleHead + lane];
+            const int2 r = row_lookup(ix, stB.pred, exDir, u, mt);
+            ex[lane] = r.y > r.x ? __ldg(ix.srcRank[exDir] + r.x) : -1;
+            isW = seg_has(ix.val[stA.dir], segBeg, segLen, u, mt);
+        }
+        wmask = __ballot_sync(0xffffffffu, isW);
+        __syncwarp();
     }
-    const unsigned wmask = __ballot_sync(0xffffffffu, isW);
-    __syncwarp();
     int e0 = 0, e1 = 0;
     if (wmask) {
         const int2 r = row_lookup(ix, stB.pred, stB.dir, par[kTupleHead + __ffs(wmask) - 1], mt);
         e0 = r.x;
         e1 = r.y;
     }
-    const uint32_t* S1 = P.memoBits + (long long)slot * 2 * words;
     const uint32_t* S2 = S1 + words;
     const int* rk = ix.valRank[stB.dir];
     const int per = (words + 31) >> 5;
@@ -334,6 +456,25 @@ __device__ __noinline__ int memo_exists(const DevPlan& P, const DevIndex& ix, co
     return (int)((__ldg(S + (rank >> 5)) >> (rank & 31)) & 1u);
 }
 
+// Whether an item (a, x) of a three-step memo plan is answered by its memo:
+// the paths through a must reach at most kMemo3List values (the warp's
+// list) and a's reverse row under the second step must be short.
+template <bool kC>
+__device__ __forceinline__ bool memo3_fits(const DevPlan& P, const DevIndex& ix, int a, Meter<kC>& mt) {
+    const DevStep s2 = P.steps[2], s3 = P.steps[3];
+    const int2 rInv = row_lookup(ix, s2.pred, 1 - s2.dir, a, mt);
+    if (rInv.y - rInv.x > 64) return false;
+    const int2 r2 = row_lookup(ix, s2.pred, s2.dir, a, mt);
+    if (r2.y - r2.x > kMemo3List) return false;
+    const int2 r3a = row_lookup(ix, s3.pred, s3.dir, a, mt);
+    int reach = r3a.y - r3a.x;
+    for (int e2 = r2.x; e2 < r2.y && reach <= kMemo3List; ++e2) {
+        const int2 r3 = row_lookup(ix, s3.pred, s3.dir, __ldg(ix.val[s2.dir] + e2), mt);
+        reach += r3.y - r3.x;
+    }
+    return reach <= kMemo3List;
+}
+
 // Items of a round that may skip enumeration, kept out of line so that the
 // main loop's registers stay free.  kind 1: a leaf item whose segment is a
 // whole hub row (returns the hub index); 2: an item at the memo level whose
@@ -354,6 +495,7 @@ __device__ __noinline__ int classify_item(const DevPlan& P, const DevIndex& ix, 
     const int slot = __ldg(P.memoTab + h);
     if (slot < 0) return -1;
     if (kind == 2) {
+        if (P.memoSteps == 3) return memo3_fits(P, ix, it[kTupleHead], mt) ? slot : -1;
         // bound values that are also first-step neighbours are witnesses the
         // memo must not count; one is corrected exactly, more enumerate
         int nR = 0;
@@ -783,9 +925,12 @@ __device__ __forceinline__ void run_task(Smem<B>& sm, const DevIndex& ix, const 
                         if (perWarp && mine % kWarps != warp) continue;
                         const int* par = baseK + (w0 + item) * strideK;
                         if (!leaf) {
-                            myNew += memo_item(P, ix, stp, P.steps[k + 1], par, lenK, -2 - sm.wBeg[item],
+                            const int slot = -2 - sm.wBeg[item];
+                            const int nEx3 = P.memoSteps == 3
+                                ? memo3_exceptions(P, ix, par, lenK, slot, words, S.exRank[warp], lane, mt) : 0;
+                            myNew += memo_item(P, ix, stp, P.steps[k + 1], par, lenK, slot,
                                                bm + (rowBase + par[0]) * (long long)words, words, S.exRank[warp],
-                                               lane, mt, shared);
+                                               lane, mt, shared, nEx3);
                             continue;
                         }
                         // hO must differ from every bound value: their ranks in hO's domain
@@ -986,6 +1131,32 @@ __global__ void memo_build_kernel(DevIndex ix, const MemoJob* jobs, int nJobs) {
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nWarps = blockDim.x >> 5;
     const int b = ix.rowBeg[job.d1][job.row], e = ix.rowBeg[job.d1][job.row + 1];
     Meter<false> mt;
+    if (job.p3 >= 0) {
+        // three steps: warps take the v2 in N1(x), lanes the v3 in N2(v2);
+        // every path x -> v2 -> v3 -> h with x, v2, v3, h distinct counts
+        // once for h (its S1 bit and its count)
+        const int x = ix.rowKey[job.d1][job.row];
+        uint32_t* cnt = S1 + job.words;
+        for (int i = b + warp; i < e; i += nWarps) {
+            const int v2 = __ldg(ix.val[job.d1] + i);
+            if (v2 == x) continue;
+            const int2 r2 = row_lookup(ix, job.p2, job.d2, v2, mt);
+            for (int j = r2.x + lane; j < r2.y; j += 32) {
+                const int v3 = __ldg(ix.val[job.d2] + j);
+                if (v3 == x || v3 == v2) continue;
+                const int2 r3 = row_lookup(ix, job.p3, job.d3, v3, mt);
+                for (int t = r3.x; t < r3.y; ++t) {
+                    const int h = __ldg(ix.val[job.d3] + t);
+                    if (h == x || h == v2 || h == v3) continue;
+                    const int rank = __ldg(ix.valRank[job.d3] + t);
+                    if (rank < 0 || rank >= job.wo) continue;
+                    atomicAdd(cnt + rank, 1u);
+                    atomicOr(S1 + (rank >> 5), 1u << (rank & 31));
+                }
+            }
+        }
+        return;
+    }
     for (int i = b + warp; i < e; i += nWarps) {
         const int y = __ldg(ix.val[job.d1] + i);
         const int2 r = row_lookup(ix, job.p2, job.d2, y, mt);

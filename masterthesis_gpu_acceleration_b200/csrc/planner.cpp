@@ -389,6 +389,25 @@ RulePlan plan_rule(const Rule& rule, const HostIndex& ix, const Geom& geom) {
                         P.memoD2 = c.dir;
                     }
                 }
+                // three-step suffix memo: hS -> x, then x -> v2 -> v3 -> hO,
+                // each step keyed by the value the one before bound, and no
+                // test after x but injectivity; items (hS, x) whose x is a
+                // memoised hub row are answered by memo3_item (kernels.cu)
+                if (pairs && P.m == 4 && P.tupleLen[0] == kTupleHead + 1) {
+                    bool ok = true;
+                    for (int l = 0; l < 4 && ok; ++l) {
+                        const DevStep& st = P.steps[l];
+                        ok = st.kind == kExpand && st.nNew == 1 && st.keyRef == P.tupleLen[l] - 1 &&
+                             (st.hoWhich != 0) == (l == 3);
+                    }
+                    for (int l = 2; l <= 4 && ok; ++l) ok = P.chkN[l] == 0 && P.usedN[l] == 0;
+                    if (ok) {
+                        P.memoLevel = 2;
+                        P.memoP2 = P.steps[2].pred;
+                        P.memoD2 = P.steps[2].dir;
+                        P.memoSteps = 3;
+                    }
+                }
                 B.how = kDevice;
                 B.rootBeg = ix.predRow[seedDir][seedPred];
                 B.rootEnd = ix.predRow[seedDir][seedPred + 1];

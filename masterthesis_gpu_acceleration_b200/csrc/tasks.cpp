@@ -229,13 +229,18 @@ TaskBuilder::Walk TaskBuilder::compute_walk(const PhasePlan& ph) {
     const bool chain = chain_shaped(P);
     const Hop2* h = chain ? &hop2(P.steps[0].pred, P.steps[0].dir, P.steps[1].pred, P.steps[1].dir) : nullptr;
     const int32_t* deg2 = (!chain && P.m >= 2 && P.steps[1].kind == kExpand) ? degrees(P.steps[1].pred, P.steps[1].dir) : nullptr;
-    // three-step plans whose last two steps are memoised: an item of level
-    // 1 costs the memo's price when its row has a memo, else its enumeration
+    // plans whose last two (three) steps are memoised: an item of level 1
+    // costs the memo's price when its row has a memo, else its enumeration
     const std::vector<uint8_t>* memo = nullptr;
     double memoCost = 0.0;
     const DevStep& s1 = P.steps[1];
-    if (chain && P.mode == kPairs && P.m == 3 && P.memoLevel == 2 && memoRows)
-        memo = memoRows(s1.pred, s1.dir, P.steps[2].pred, P.steps[2].dir, &memoCost);
+    if (chain && P.mode == kPairs && P.memoLevel == 2 && memoRows) {
+        if (P.m == 3)
+            memo = memoRows(s1.pred, s1.dir, P.steps[2].pred, P.steps[2].dir, -1, 0, &memoCost);
+        else if (P.m == 4 && P.memoSteps == 3)
+            memo = memoRows(s1.pred, s1.dir, P.steps[2].pred, P.steps[2].dir, P.steps[3].pred, P.steps[3].dir,
+                            &memoCost);
+    }
     // a second step that scans, or expands from a root value or a constant,
     // costs the same after every edge of the first step
     const bool uniformChild = P.m >= 2 && (s1.kind == kScan || s1.keyRef < P.tupleLen[0]);

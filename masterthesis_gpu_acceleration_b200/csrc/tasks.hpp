@@ -102,10 +102,11 @@ public:
     std::vector<int32_t> split_roots(const PhasePlan& ph, int n);
 
     // Suffix memos known to the context: per-row flags of (p1, d1) for the
-    // memo of (p1, d1) -> (p2, d2) and its cost per item in work units, or
-    // null.  Walks of plans that end in such a suffix weigh memoised items
-    // by that cost instead of their enumeration.
-    std::function<const std::vector<uint8_t>*(int, int, int, int, double*)> memoRows;
+    // memo of (p1, d1) -> (p2, d2), or with p3 >= 0 of the three-step suffix
+    // (p1, d1) -> (p2, d2) -> (p3, d3), and its cost per item in work units,
+    // or null.  Walks of plans that end in such a suffix weigh memoised
+    // items by that cost instead of their enumeration.
+    std::function<const std::vector<uint8_t>*(int, int, int, int, int, int, double*)> memoRows;
 
     // Overrides: a fixed task work target (0 = automatic) and the hub-aware
     // estimate above which a phase is walked.
