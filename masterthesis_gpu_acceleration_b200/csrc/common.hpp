@@ -18,6 +18,7 @@ constexpr int kTupleHead = 2;                  // [root index, hO rank]
 constexpr int kMaxTuple = kTupleHead + kMaxVars;
 constexpr int kMaxChecks = 16;
 constexpr int kMaxUsed = 40;
+constexpr int kMaxSupFused = 4;   // rules whose support one body-size plan counts
 
 // One slot of the (predicate, direction, key) -> edge range table.
 // tag = pred * 2 + dir; tag 0xffffffff marks an empty slot.
@@ -162,6 +163,21 @@ struct DevPlan {
     unsigned long long keyBase;     // sort mode: the plan's key prefix (its sort index, shifted)
     int32_t rankBits;               // sort mode: bits of the hO rank field
     int32_t pad3;
+    // Fused support (kPairs plans with rows in shared memory or block rows):
+    // for j < supN, results[supSlot[j]] gains the number of head triples
+    // (hS, supPred[j], b), b != hS, whose pair (hS, b) the plan's rows hold;
+    // b's rank is that of its row in (supDomPred, supDomDir), hO's domain.
+    int32_t supN;
+    int32_t supDomPred, supDomDir;
+    int32_t supPred[kMaxSupFused];
+    int32_t supSlot[kMaxSupFused];
+    int32_t pad4;
+};
+
+// A split heavy root of a plan with fused support: its global row gRow is
+// complete only after the launch, when support_rows_kernel counts it.
+struct SupJob {
+    int32_t plan, root, gRow, pad;
 };
 
 // How a kPairs phase deduplicates its (hS row, hO rank) pairs.

@@ -150,6 +150,29 @@ void Staged::stage(Context& c, std::vector<DevPlan>& plans, const std::vector<co
             blockWords = (need + 3) & ~size_t(3);
         }
     }
+    // fused support: a body-size plan whose pair rows are complete at the
+    // end of each task (shared rows or block rows) counts the support of the
+    // rules in `fuse`; their support plans get no tasks
+    std::vector<char> skip(nPlans, 0);
+    for (int i = 0; i < nPlans; ++i) {
+        DevPlan& P = plans[i];
+        P.supN = P.supDomPred = P.supDomDir = 0;
+        for (int j = 0; j < kMaxSupFused; ++j) P.supPred[j] = P.supSlot[j] = 0;
+    }
+    for (const auto& f : fuse) {
+        const int sp = f[0], bp = f[1];
+        if (sp < 0 || bp < 0 || sp >= nPlans || bp >= nPlans || skip[sp] || skip[bp]) continue;
+        DevPlan& B = plans[bp];
+        if (B.mode != kPairs || B.supN >= kMaxSupFused || plans[sp].mode != kExist) continue;
+        if (dedup[bp] != kDedupShared && dedup[bp] != kDedupBlockRows) continue;
+        const auto dom = ho_domain(B);
+        B.supDomPred = dom.first;
+        B.supDomDir = dom.second;
+        B.supPred[B.supN] = f[2];
+        B.supSlot[B.supN] = sp;
+        ++B.supN;
+        skip[sp] = 1;
+    }
     std::vector<size_t> gOff(nPlans, 0);
     for (int i = 0; i < nPlans; ++i) {
         if (dedup[i] != kDedupRows) continue;
@@ -186,8 +209,36 @@ void Staged::stage(Context& c, std::vector<DevPlan>& plans, const std::vector<co
         if (plans[i].memoLevel > 0 && dedup[i] != kDedupSort) memoKeys.push_back(memo_key_of(plans[i]));
     }
     if (!memoKeys.empty()) c.ensure_memos(memoKeys, s);
-    std::vector<PhaseTasks> pts;
-    c.tasks->build(phases, c.grid, true, pts, walkBudget, costAware, &lim);
+    std::vector<PhaseTasks> pts(nPlans);
+    {
+        std::vector<const PhasePlan*> ph;
+        std::vector<PhaseLimits> li;
+        std::vector<int> at;
+        for (int i = 0; i < nPlans; ++i)
+            if (!skip[i]) {
+                ph.push_back(phases[i]);
+                li.push_back(lim[i]);
+                at.push_back(i);
+            }
+        std::vector<PhaseTasks> built;
+        c.tasks->build(ph, c.grid, true, built, walkBudget, costAware, &li);
+        for (size_t k = 0; k < at.size(); ++k) {
+            for (DevTask& t : built[k].tasks) t.plan = at[k];
+            pts[at[k]] = std::move(built[k]);
+        }
+    }
+    // split heavy roots of plans with fused support: counted after the launch
+    std::vector<SupJob> supJobs;
+    for (int i = 0; i < nPlans; ++i) {
+        if (plans[i].supN == 0 || pts[i].heavyRows == 0) continue;
+        std::vector<char> seenRow((size_t)pts[i].heavyRows, 0);
+        for (const DevTask& t : pts[i].tasks)
+            if (t.gRow >= 0 && !seenRow[(size_t)t.gRow]) {
+                seenRow[(size_t)t.gRow] = 1;
+                supJobs.push_back(SupJob{i, t.beg, t.gRow, 0});
+            }
+    }
+    nSupJobs = (int)supJobs.size();
     std::vector<size_t> hOff(nPlans, 0);
     heavyWords = 0;
     for (int i = 0; i < nPlans; ++i) {
@@ -288,11 +339,15 @@ void Staged::stage(Context& c, std::vector<DevPlan>& plans, const std::vector<co
     }
     size_t planBytes = (size_t)nPlans * sizeof(DevPlan);
     size_t taskBytes = (size_t)nTasks * sizeof(DevTask);
-    size_t blob = planBytes + taskBytes + (size_t)nSort * sizeof(int32_t);
+    const size_t sortBytes = ((size_t)nSort * sizeof(int32_t) + 15) & ~size_t(15);
+    size_t blob = planBytes + taskBytes + sortBytes + (size_t)nSupJobs * sizeof(SupJob);
     hBlob.ensure(blob);
     std::memcpy(hBlob.p, plans.data(), planBytes);
     std::memcpy(static_cast<char*>(hBlob.p) + planBytes, tasks.data(), taskBytes);
     if (nSort) std::memcpy(static_cast<char*>(hBlob.p) + planBytes + taskBytes, sortPlans.data(), nSort * sizeof(int32_t));
+    if (nSupJobs)
+        std::memcpy(static_cast<char*>(hBlob.p) + planBytes + taskBytes + sortBytes, supJobs.data(),
+                    (size_t)nSupJobs * sizeof(SupJob));
     hTasks = std::move(tasks);   // kept for profiles and task-time learning
     hCost = std::move(cost);
     dBlob.ensure(blob, as);
@@ -305,6 +360,9 @@ void Staged::stage(Context& c, std::vector<DevPlan>& plans, const std::vector<co
     dTasks = reinterpret_cast<const DevTask*>(static_cast<const char*>(dBlob.p) + planBytes);
     dSortSlots = nSort ? reinterpret_cast<const int32_t*>(static_cast<const char*>(dBlob.p) + planBytes + taskBytes)
                        : nullptr;
+    dSupJobs = nSupJobs ? reinterpret_cast<const SupJob*>(static_cast<const char*>(dBlob.p) + planBytes + taskBytes +
+                                                          sortBytes)
+                        : nullptr;
     h2dBytes = blob;
     d2hBytes = (size_t)nPlans * sizeof(unsigned long long) + 8;
 }
@@ -477,6 +535,8 @@ void Staged::enqueue(Context& c, cudaStream_t s, int instr, int gridCap, unsigne
                      static_cast<unsigned long long*>(dResults.p), static_cast<int*>(dCtl.p) + 1, grid,
                      c.geom.block, s, instr ? &prof : nullptr),
        "engine launch");
+    ck(support_rows(c.dix, dPlans, dSupJobs, nSupJobs, static_cast<unsigned long long*>(dResults.p), s),
+       "fused support of split roots");
     enqueue_sort(c, s, static_cast<unsigned long long*>(dResults.p), static_cast<int*>(dCtl.p) + 1);
 }
 
@@ -502,6 +562,9 @@ void Staged::enqueue_per_plan(Context& c, cudaStream_t s) {
                          grid, c.geom.block, s, &prof),
            "engine launch");
     }
+    ck(support_rows(c.dix, dPlans, dSupJobs, nSupJobs,
+                    reinterpret_cast<unsigned long long*>(static_cast<char*>(dCtl.p) + kPerPlanResults), s),
+       "fused support of split roots");
     enqueue_sort(c, s, reinterpret_cast<unsigned long long*>(static_cast<char*>(dCtl.p) + kPerPlanResults), ctl + 2);
 }
 
@@ -679,6 +742,18 @@ void prepare(Batch& b, Context& c, const char* const* rules, int n, int isJson, 
             b.owner.push_back(2 * i + k);
         }
     }
+    // fused support: the rules whose support their body-size plan counts
+    b.st.fuse.clear();
+    if (c.fuseSupport && (c.batchPhases & 3) == 3) {
+        std::vector<int> planOf(2 * (size_t)n, -1);
+        for (size_t k = 0; k < b.owner.size(); ++k) planOf[(size_t)b.owner[k]] = (int)k;
+        for (const auto& sh : b.shared) planOf[(size_t)sh.first] = sh.second;
+        for (int i = 0; i < n; ++i) {
+            if (b.parseStatus[i] != 0 || b.rps[i].status != kRuleOk || b.rps[i].supFuse < 0) continue;
+            const int sp = planOf[2 * (size_t)i], bp = planOf[2 * (size_t)i + 1];
+            if (sp >= 0 && bp >= 0) b.st.fuse.push_back({sp, bp, b.rps[i].supFuse});
+        }
+    }
     if (!b.stream) ck(cudaStreamCreateWithFlags(&b.stream, cudaStreamNonBlocking), "cudaStreamCreate");
     if (!b.ev0) ck(cudaEventCreate(&b.ev0), "cudaEventCreate");
     if (!b.ev1) ck(cudaEventCreate(&b.ev1), "cudaEventCreate");
@@ -763,8 +838,10 @@ namespace {
 // The rest of a load, whichever source the index came from: the state built
 // on the index, and its upload.
 void finish_load(Context* c) {
-    // GPU_RULES_MEMO3=0 switches the three-step suffix memos off
+    // GPU_RULES_MEMO3=0 switches the three-step suffix memos off,
+    // GPU_RULES_FUSE_SUPPORT=0 the fused support of batches
     if (const char* m = std::getenv("GPU_RULES_MEMO3")) c->memo3 = std::atoi(m) != 0;
+    if (const char* f = std::getenv("GPU_RULES_FUSE_SUPPORT")) c->fuseSupport = std::atoi(f) != 0;
     c->tasks.reset(new TaskBuilder(c->hix));
     c->tasks->memoRows = [c](int p1, int d1, int p2, int d2, int p3, int d3,
                              double* cost) -> const std::vector<uint8_t>* {

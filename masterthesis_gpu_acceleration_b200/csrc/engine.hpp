@@ -27,6 +27,10 @@ namespace gr {
 size_t engine_smem_bytes(int block);
 cudaError_t engine_configure();
 cudaError_t memo_build(const DevIndex& ix, const MemoJob* jobs, int nJobs, cudaStream_t stream);
+// Fused support of split heavy roots, after the engine launch that filled
+// their rows (see DevPlan::supN).
+cudaError_t support_rows(const DevIndex& ix, const DevPlan* plans, const SupJob* jobs, int nJobs,
+                         unsigned long long* results, cudaStream_t stream);
 cudaError_t engine_launch(const DevIndex& ix, const DevPlan* plans, const DevTask* tasks, int nTasks,
                           int* taskCounter, unsigned long long* results, int* status, int grid, int block,
                           cudaStream_t stream, const EngineProfile* prof);
@@ -136,6 +140,14 @@ struct Staged {
     unsigned long long keyCap = 0;
     unsigned long long keyHint = 0;     // exact keys of a run that overflowed keyCap
     const int32_t* dSortSlots = nullptr;   // result slot of each sort index (in dBlob)
+    // Fused support, set before staging: {support plan, body-size plan, head
+    // predicate} of rules whose support the body-size plan may count (see
+    // RulePlan::supFuse).  Staging fuses those whose body-size rows are
+    // complete at the end of each task and gives their support plans no
+    // tasks; split heavy roots are counted by support_rows after the launch.
+    std::vector<std::array<int, 3>> fuse;
+    int nSupJobs = 0;
+    const SupJob* dSupJobs = nullptr;      // in dBlob
     HostBuf hSort;                      // the downloaded append cursor
     HostBuf hIncomplete;                // per plan: a task was abandoned at the deadline
     bool budgeted = false;              // the last enqueue ran under a deadline
@@ -260,6 +272,7 @@ struct Context {
     // least memoGain x the memo's words (negative: no memos)
     double memoGain = 0.25;
     bool memo3 = true;         // three-step suffix memos (memo3_item) for the plans that admit one
+    bool fuseSupport = true;   // batches count a rule's support in its body-size plan where it can
     std::unordered_map<uint64_t, std::unique_ptr<SuffixMemo>> memos;
     std::vector<std::unique_ptr<DevBuf>> memoChunks;   // one allocation per ensure_memos call
     size_t memoBytes = 0;

@@ -537,6 +537,36 @@ __device__ __forceinline__ void emit_pair(const DevPlan& P, long long row, int r
     if (slot < P.keyCap) P.pairKeys[slot] = key;
 }
 
+// Fused support (plans with supN > 0): the head triples (hS, supPred[j],
+// b), b != hS, of rule j whose pair (hS, b) is set in the plan's row of
+// root i (rows at bm + i * rowWords for the roots rootBeg + i, i < G).
+// Warps take the roots, lanes a root's head triples; returns this lane's
+// count.  Out of line and small: it runs once per task, after the search.
+template <bool kC>
+__device__ __noinline__ unsigned long long fused_support(const DevPlan& P, const DevIndex& ix, int j, int rootBeg,
+                                                         int G, const uint32_t* bm, int warp, int nWarps, int lane,
+                                                         Meter<kC>& mt) {
+    unsigned long long n = 0;
+    const int hp = P.supPred[j], dp = P.supDomPred, dd = P.supDomDir;
+    for (int i = warp; i < G; i += nWarps) {
+        const int a = __ldg(ix.rowKey[P.rootDir] + rootBeg + i);
+        mt.add(4);
+        const int2 hr = row_lookup(ix, hp, 0, a, mt);
+        const uint32_t* row = bm + (long long)i * P.rowWords;
+        for (int e = hr.x + lane; e < hr.y; e += 32) {
+            const int b = __ldg(ix.val[0] + e);
+            mt.add(4);
+            if (b == a) continue;
+            const int2 br = row_lookup(ix, dp, dd, b, mt);
+            if (br.y <= br.x) continue;   // b never binds hO
+            const int rank = __ldg(ix.srcRank[dd] + br.x);
+            mt.add(8);
+            if ((row[rank >> 5] >> (rank & 31)) & 1u) ++n;
+        }
+    }
+    return n;
+}
+
 template <int B, bool kC, bool kD>
 __device__ __forceinline__ void run_task(Smem<B>& sm, const DevIndex& ix, const DevTask& task,
                                          unsigned long long* results, int* status, Meter<kC>& mt) {
@@ -998,6 +1028,18 @@ __device__ __forceinline__ void run_task(Smem<B>& sm, const DevIndex& ix, const 
     }
     __syncthreads();
 
+    // ---- fused support: every pair row of the task is complete here (a
+    // split heavy root's row only after the launch: support_rows_kernel) ----
+    if (P.supN > 0 && !heavy) {
+        const int lane = tid & 31;
+        for (int j = 0; j < P.supN; ++j) {
+            unsigned long long n = fused_support(P, ix, j, task.beg, G, bm, tid >> 5, B / 32, lane, mt);
+#pragma unroll
+            for (int d = 16; d; d >>= 1) n += __shfl_down_sync(0xffffffffu, n, d);
+            if (lane == 0 && n) atomicAdd(results + P.supSlot[j], n);
+        }
+    }
+
     // ---- result ----
     unsigned long long mine = 0;
     if (!pairs && !heavy) {
@@ -1169,6 +1211,32 @@ __global__ void memo_build_kernel(DevIndex ix, const MemoJob* jobs, int nJobs) {
             if (old & bit) atomicOr(S2 + (rank >> 5), bit);
         }
     }
+}
+
+// Fused support of split heavy roots: one warp per job counts the head
+// triples of the job's root against its completed global row.
+__global__ void support_rows_kernel(const __grid_constant__ DevIndex ix, const DevPlan* plans, const SupJob* jobs,
+                                    int nJobs, unsigned long long* results) {
+    const int w = (int)((blockIdx.x * (long long)blockDim.x + threadIdx.x) >> 5);
+    const int lane = threadIdx.x & 31;
+    if (w >= nJobs) return;
+    const SupJob jb = jobs[w];
+    const DevPlan& P = plans[jb.plan];
+    if (!P.gHeavy) return;
+    const uint32_t* row = P.gHeavy + (long long)jb.gRow * P.rowWords;
+    Meter<false> mt;
+    for (int j = 0; j < P.supN; ++j) {
+        unsigned long long n = fused_support(P, ix, j, jb.root, 1, row, 0, 1, lane, mt);
+        for (int d = 16; d; d >>= 1) n += __shfl_down_sync(0xffffffffu, n, d);
+        if (lane == 0 && n) atomicAdd(results + P.supSlot[j], n);
+    }
+}
+
+cudaError_t support_rows(const DevIndex& ix, const DevPlan* plans, const SupJob* jobs, int nJobs,
+                         unsigned long long* results, cudaStream_t stream) {
+    if (nJobs <= 0) return cudaSuccess;
+    support_rows_kernel<<<(nJobs + 7) / 8, 256, 0, stream>>>(ix, plans, jobs, nJobs, results);
+    return cudaGetLastError();
 }
 
 cudaError_t memo_build(const DevIndex& ix, const MemoJob* jobs, int nJobs, cudaStream_t stream) {

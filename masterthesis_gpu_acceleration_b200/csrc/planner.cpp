@@ -422,8 +422,23 @@ RulePlan plan_rule(const Rule& rule, const HostIndex& ix, const Geom& geom) {
         rp.support = PhasePlan{};
         rp.body = PhasePlan{};
         rp.headSupport = rp.headSize;
+    } else if (S.how == kDevice && B.how == kDevice && h.s.isVar && h.o.isVar && h.s.id != h.o.id &&
+               B.plan.mode == kPairs && B.plan.rootKind == kRootRows && B.plan.hoLevel >= 1) {
+        // support from the body-size pairs: the support plan is the body
+        // grounded from a head triple (a, b) with a != b, and with no
+        // used-triple test the head triple never constrains it, so a head
+        // triple has a grounding exactly when (a, b) is a body pair
+        bool used = false;
+        for (int l = 0; l <= kMaxBody; ++l) used |= S.plan.usedN[l] != 0;
+        if (!used) rp.supFuse = h.pred;
     }
     return rp;
+}
+
+std::pair<int32_t, int32_t> ho_domain(const DevPlan& P) {
+    const DevStep& st = P.steps[P.hoLevel - 1];
+    if (st.kind == kExpand) return {st.pred, 1 - st.dir};
+    return {st.pred, st.hoWhich == 1 ? 0 : 1};
 }
 
 }  // namespace gr

@@ -1,6 +1,7 @@
 // planner.hpp — rule -> device plans (support phase and body-size phase).
 #pragma once
 #include <cstdint>
+#include <utility>
 #include <vector>
 
 #include "common.hpp"
@@ -33,7 +34,17 @@ struct RulePlan {
     int32_t status = kRuleOk;
     int64_t headSize = 0, headSupport = 0;
     PhasePlan support, body;
+    // >= 0 when the support is the number of head triples (hS, supFuse, hO),
+    // hS != hO, among the body-size phase's (hS, hO) pairs: both head terms
+    // are distinct variables and no body atom can ground to the head triple
+    // (the support plan has no used-triple test), so a body-size plan that
+    // keeps its pair rows can count the support too (fused support).
+    int32_t supFuse = -1;
 };
+
+// Where a kPairs plan ranks hO: the rows of (pred, dir) in the returned
+// pair (the step binding hO looks its value up there).
+std::pair<int32_t, int32_t> ho_domain(const DevPlan& P);
 
 // Plans both phases.  Semantics follow CPU_01_nonparallel/SupportCounting.cpp:
 // support (474-552) with the head triple counted as used, body size
