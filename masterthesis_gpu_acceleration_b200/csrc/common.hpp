@@ -216,7 +216,8 @@ struct Geom {
 // One suffix memo to build for hub row `row` of (p1, d1).  Two steps
 // (p3 < 0): through (p2, d2), bitmaps S1 then S2 of `words` words at `bits`.
 // Three steps: through (p2, d2) then (p3, d3), the bitmap S1 (`words`
-// words) then one 32-bit path count per rank of the domain (`wo` ranks).
+// words) then one path count per rank of the domain (`wo` ranks), a byte
+// each (four to a word) that saturates at 255.
 struct MemoJob {
     int32_t p1, d1, p2, d2, row, words;
     int32_t p3, d3, wo, pad;

@@ -402,7 +402,9 @@ void Context::ensure_memos(const std::vector<std::array<int, 6>>& keys, cudaStre
         return k[4] >= 0 ? h.pred_rows(k[4], 1 - k[5]) : h.pred_rows(k[2], 1 - k[3]);
     };
     // the hub rows of (p1, d1) worth a memo, per new key, on host threads:
-    // a row's suffix candidates are what enumeration would visit after x
+    // a row's candidates are what enumeration would visit from x on (its
+    // own values, most of which may fail the next step's signature test,
+    // and what they lead to)
     std::vector<std::vector<int32_t>> rowsOf(fresh.size());
     parallel_for(fresh.size(), [&](size_t i) {
         const int p1 = fresh[i][0], d1 = fresh[i][1], p2 = fresh[i][2], d2 = fresh[i][3];
@@ -411,7 +413,7 @@ void Context::ensure_memos(const std::vector<std::array<int, 6>>& keys, cudaStre
         const int32_t* deg = tasks->degrees(p3 >= 0 ? p3 : p2, p3 >= 0 ? d3 : d2);
         for (int32_t r = h.predRow[d1][p1]; r < h.predRow[d1][p1 + 1]; ++r) {
             if (h.hubOf[d1][r] < 0) continue;
-            double cand = 0;
+            double cand = (double)(h.rowBeg[d1][r + 1] - h.rowBeg[d1][r]);
             for (int32_t e = h.rowBeg[d1][r]; e < h.rowBeg[d1][r + 1]; ++e) {
                 if (p3 < 0) {
                     cand += deg[h.val[d1][e]];
@@ -426,7 +428,7 @@ void Context::ensure_memos(const std::vector<std::array<int, 6>>& keys, cudaStre
     // per memo slot: S1 and S2 (two steps), or S1 and one count per rank
     auto slot_words = [&](const std::array<int, 6>& k) -> size_t {
         const size_t words = (size_t)((domain(k) + 31) / 32);
-        return k[4] >= 0 ? words + (size_t)domain(k) : 2 * words;
+        return k[4] >= 0 ? words + (size_t)(domain(k) + 3) / 4 : 2 * words;
     };
     // within the memory budget, in key order: one device allocation holding
     // every new memo's hub table, then every new memo's bits

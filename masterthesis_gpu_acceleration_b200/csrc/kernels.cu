@@ -236,13 +236,16 @@ constexpr int kMemo3List = kMaxVars - 1;
 // Three-step suffix memos, for body-size plans hS -> x -> v2 -> v3 -> hO
 // (memoSteps == 3) at an item (a, x) whose x is a memoised hub row.  The
 // memo of x holds S1 = {h : C(h) > 0} and C(h), the number of paths
-// x -> v2 -> v3 -> h with x, v2, v3, h distinct.  The item's pairs are the
-// h != a with a path that also avoids a, i.e. with C(h) > C_a(h), C_a(h)
-// the paths through a:
+// x -> v2 -> v3 -> h with x, v2, v3, h distinct, as a byte that saturates
+// at 255.  The item's pairs are the h != a with a path that also avoids a,
+// i.e. with C(h) > C_a(h), C_a(h) the paths through a:
 //   a = v2 (when a is a neighbour of x): v3 in N2(a) \ {x, a, h}, h in N3(v3);
 //   a = v3: v2 in N1(x) with a in N2(v2), v2 not in {x, a, h}, and h in N3(a).
 // Only h reached that way (listed, at most kMemo3List by the check in
-// classify_item) can have C_a(h) > 0; every other bit of S1 stands.
+// classify_item) can have C_a(h) > 0; every other bit of S1 stands.  The
+// same check bounds C_a(h) by kMemo3List + 64 < 255 (at most one path per
+// v3 in N2(a), and per v2 in a's reverse row), so a saturated count still
+// compares exactly.
 // memo3_exceptions lists the ranks to clear from S1 and memo_item applies
 // them.  Its parts are small leaf functions called one after the other, so
 // that few of the caller's registers need to be free for them.
@@ -303,7 +306,7 @@ __device__ __noinline__ int memo3_list(const DevPlan& P, const DevIndex& ix, con
 template <bool kC>
 __device__ __noinline__ bool memo3_keep(const DevPlan& P, const DevIndex& ix, const int* par, int lenK, int r,
                                         int kv, const uint32_t* C, Meter<kC>& mt) {
-    const unsigned c = __ldg(C + r);
+    const unsigned c = (__ldg(C + (r >> 2)) >> ((r & 3) * 8)) & 0xffu;   // saturates at 255
     mt.add(4);
     const int p3 = P.steps[3].pred, d3 = P.steps[3].dir;
     const int a = par[kTupleHead];
@@ -338,7 +341,7 @@ __device__ __forceinline__ int memo3_exceptions(const DevPlan& P, const DevIndex
     n = __shfl_sync(0xffffffffu, n, 0);
     __syncwarp();
     if (lane < n) {
-        const uint32_t* C = P.memoBits + (long long)slot * ((long long)words + P.wo) + words;
+        const uint32_t* C = P.memoBits + (long long)slot * ((long long)words + ((P.wo + 3) >> 2)) + words;
         if (memo3_keep(P, ix, par, lenK, ex[lane], kv, C, mt)) ex[lane] = -1;   // still reached: keep its bit
     }
     __syncwarp();
@@ -363,7 +366,7 @@ __device__ __noinline__ unsigned long long memo_item(const DevPlan& P, const Dev
                                                      bool sharedDst, int nEx3) {
     unsigned long long myNew = 0;
     const bool three = nEx3 > 0;
-    const uint32_t* S1 = P.memoBits + (long long)slot * (three ? (long long)words + P.wo : 2LL * words);
+    const uint32_t* S1 = P.memoBits + (long long)slot * (three ? (long long)words + ((P.wo + 3) >> 2) : 2LL * words);
     int nEx = lenK - kTupleHead;
     unsigned wmask = 0;
     if (three) {
@@ -1192,7 +1195,15 @@ __global__ void memo_build_kernel(DevIndex ix, const MemoJob* jobs, int nJobs) {
                     if (h == x || h == v2 || h == v3) continue;
                     const int rank = __ldg(ix.valRank[job.d3] + t);
                     if (rank < 0 || rank >= job.wo) continue;
-                    atomicAdd(cnt + rank, 1u);
+                    // saturating byte increment of the rank's path count
+                    uint32_t* cw = cnt + (rank >> 2);
+                    const int sh = (rank & 3) * 8;
+                    uint32_t old = *cw;
+                    while (((old >> sh) & 0xffu) != 0xffu) {
+                        const uint32_t seen = atomicCAS(cw, old, old + (1u << sh));
+                        if (seen == old) break;
+                        old = seen;
+                    }
                     atomicOr(S1 + (rank >> 5), 1u << (rank & 31));
                 }
             }

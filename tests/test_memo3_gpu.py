@@ -96,9 +96,63 @@ def memo3_graph(out_dir, seed=11):
     return ttl, rules, counts
 
 
+def saturating_graph(out_dir, seed=5):
+    """One hub x (entity 0) with 500 neighbours v2 among R = 1..600; every
+    entity of R has two second-step values in V3 = 401..420 and V3 three
+    third-step values in H = 421..430, so about 300 paths reach each h
+    (path counts saturate at 255).  Every entity of R is a root a -> x, so
+    a is often a neighbour of x and sometimes in V3 or H.  Returns (ttl,
+    rules, int64 counts [n, 4])."""
+    import oracle
+    rng = np.random.default_rng(seed)
+    R = np.arange(1, 601)
+    V3, H = np.arange(401, 421), np.arange(421, 431)
+    trip = {(int(a), P_ROOT, 0) for a in R}
+    trip |= {(0, P_HUB, int(v)) for v in R[:500]}
+    for v in R:
+        for w in rng.choice(V3, 2, replace=False):
+            if w != v:
+                trip.add((int(v), P_STEP2, int(w)))
+    for v in V3:
+        for w in rng.choice(H, 3, replace=False):
+            trip.add((int(v), P_STEP3, int(w)))
+    heads = set()
+    while len(heads) < 1500:
+        heads.add((int(rng.choice(R)), P_HEAD, int(rng.choice(H))))
+    trip = np.array(sorted(trip | heads), dtype=np.int32)
+    out_dir.mkdir(parents=True, exist_ok=True)
+    ttl = out_dir / "saturating.ttl"
+    with open(ttl, "w") as f:
+        for s_, p_, o_ in trip.tolist():
+            f.write(f"<http://m/e{s_}> <http://m/p{p_}> <http://m/e{o_}> .\n")
+    terms = [[(P_ROOT, ("v", "a"), ("v", "x")), (P_HUB, ("v", "x"), ("v", "v2")),
+              (P_STEP2, ("v", "v2"), ("v", "v3")), (P_STEP3, ("v", "v3"), ("v", "b")),
+              (P_HEAD, ("v", "a"), ("v", "b"))]]
+    rules = ["(?a <http://m/p0> ?x) ^ (?x <http://m/p1> ?v2) ^ (?v2 <http://m/p3> ?v3) ^ "
+             "(?v3 <http://m/p4> ?b) => (?a <http://m/p5> ?b)"]
+    g = oracle.OracleGraph(trip, P_HEAD + 1)
+    counts, st = g.evaluate_ir(terms_to_ir(terms), len(rules))
+    g.close()
+    assert (st == 0).all()
+    return ttl, rules, counts
+
+
 @pytest.fixture(scope="module")
 def memo3_case(tmp_path_factory):
     return memo3_graph(tmp_path_factory.mktemp("memo3"))
+
+
+@pytest.mark.parametrize("memo3", ["1", "0"])
+def test_three_step_memo_saturated_counts(tmp_path, memo3, monkeypatch):
+    ttl, rules, exp = saturating_graph(tmp_path)
+    assert exp[0, 3] > 0
+    monkeypatch.setenv("GPU_RULES_MEMO3", memo3)
+    monkeypatch.setenv("GPU_RULES_MEMO_GAIN", "0")
+    with eng.GpuRulesLib(ttl) as lib:
+        got = _counts(lib, rules)
+        assert got[0].tolist() == exp[0].tolist()
+        r = lib.evaluate_rule(rules[0])
+        assert [r.support, r.headSize, r.headSupport, r.bodySize] == exp[0].tolist()
 
 
 def _counts(lib, rules):
