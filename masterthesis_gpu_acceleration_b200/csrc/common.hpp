@@ -172,7 +172,25 @@ struct DevPlan {
     int32_t supPred[kMaxSupFused];
     int32_t supSlot[kMaxSupFused];
     int32_t pad4;
+    // Hub items of the leaf (see kHubSeen): per resident block kHubSeen
+    // claim entries at hubSeen + blockIdx.x * kHubSeen (null: every hub item
+    // is OR-ed).  Set for plans whose leaf items are (hS, u, w) expanding
+    // from u or w with nothing to test but injectivity.
+    unsigned long long* hubSeen;
 };
+
+// Leaf hub items of one root and one hub row differ only in the one bound
+// value that is neither the root nor the row key (the middle value), and
+// each excludes only its own bound values from the row: two items with
+// different middle values already cover every value any further one would
+// add.  A task claims its (root, hub) pairs in a direct-mapped table of
+// kHubSeen 64-bit entries [root 10 bits | hub 20 | state 2 | first middle
+// value 32] (state 1: one middle value seen, 2: two) and skips the items
+// that come after two different middle values.  The same item may come
+// twice (a wide round makes some items again); it never counts as a second
+// value, and a displaced entry only costs repeats.
+constexpr int kHubSeenBits = 8;
+constexpr int kHubSeen = 1 << kHubSeenBits;
 
 // A split heavy root of a plan with fused support: its global row gRow is
 // complete only after the launch, when support_rows_kernel counts it.

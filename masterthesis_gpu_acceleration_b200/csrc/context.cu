@@ -39,6 +39,16 @@ void set_error(const std::string& s) {
 }
 
 namespace {
+// Plans whose leaf hub items may skip repeats (see kHubSeen): the leaf
+// tuple holds hS and two more values, the leaf step expands from one of
+// those two, binds hO and tests nothing but injectivity.
+bool hub_leaf_claims(const DevPlan& P) {
+    if (P.mode != kPairs || P.m < 1) return false;
+    const DevStep& st = P.steps[P.m - 1];
+    return P.tupleLen[P.m - 1] == kTupleHead + 3 && st.kind == kExpand && st.nNew == 1 && st.hoWhich != 0 &&
+           (st.keyRef == kTupleHead + 1 || st.keyRef == kTupleHead + 2) && P.chkN[P.m] == 0 && P.usedN[P.m] == 0;
+}
+
 // Bits that hold the values 0 .. n - 1 (at least one).
 int bits_for(uint64_t n) {
     int b = 1;
@@ -249,6 +259,9 @@ void Staged::stage(Context& c, std::vector<DevPlan>& plans, const std::vector<co
     if (heavyWords) dHeavy.ensure(heavyWords * 4, as);
     std::vector<DevTask> tasks;
     std::vector<double> cost;
+    bool anyClaims = false;
+    for (int i = 0; i < nPlans; ++i) anyClaims |= c.hubClaims && dedup[i] != kDedupSort && hub_leaf_claims(plans[i]);
+    if (anyClaims) dHubSeen.ensure((size_t)std::max(c.grid, 1) * kHubSeen * 8, as);
     for (int i = 0; i < nPlans; ++i) {
         plans[i].memoTab = nullptr;
         plans[i].memoBits = nullptr;
@@ -269,6 +282,8 @@ void Staged::stage(Context& c, std::vector<DevPlan>& plans, const std::vector<co
         plans[i].gRowBase = (dm == kDedupRows || dm == kDedupSort) ? phases[i]->rootBeg : 0;
         plans[i].gBlockWords = dm == kDedupBlockRows ? (int64_t)blockWords : 0;
         plans[i].gHeavy = (pts[i].heavyRows && dm != kDedupSort) ? static_cast<uint32_t*>(dHeavy.p) + hOff[i] : nullptr;
+        plans[i].hubSeen = (anyClaims && dm != kDedupSort && hub_leaf_claims(plans[i]))
+                               ? static_cast<unsigned long long*>(dHubSeen.p) : nullptr;
         plans[i].pairKeys = nullptr;
         plans[i].keyCursor = nullptr;
         plans[i].keyCap = 0;
@@ -841,9 +856,11 @@ namespace {
 // on the index, and its upload.
 void finish_load(Context* c) {
     // GPU_RULES_MEMO3=0 switches the three-step suffix memos off,
-    // GPU_RULES_FUSE_SUPPORT=0 the fused support of batches
+    // GPU_RULES_FUSE_SUPPORT=0 the fused support of batches,
+    // GPU_RULES_HUB_CLAIMS=0 the skipping of repeated leaf hub items
     if (const char* m = std::getenv("GPU_RULES_MEMO3")) c->memo3 = std::atoi(m) != 0;
     if (const char* f = std::getenv("GPU_RULES_FUSE_SUPPORT")) c->fuseSupport = std::atoi(f) != 0;
+    if (const char* h = std::getenv("GPU_RULES_HUB_CLAIMS")) c->hubClaims = std::atoi(h) != 0;
     c->tasks.reset(new TaskBuilder(c->hix));
     c->tasks->memoRows = [c](int p1, int d1, int p2, int d2, int p3, int d3,
                              double* cost) -> const std::vector<uint8_t>* {

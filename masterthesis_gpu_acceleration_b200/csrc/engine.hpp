@@ -148,6 +148,7 @@ struct Staged {
     std::vector<std::array<int, 3>> fuse;
     int nSupJobs = 0;
     const SupJob* dSupJobs = nullptr;      // in dBlob
+    DevBuf dHubSeen;                       // leaf hub claims: kHubSeen words per resident block
     HostBuf hSort;                      // the downloaded append cursor
     HostBuf hIncomplete;                // per plan: a task was abandoned at the deadline
     bool budgeted = false;              // the last enqueue ran under a deadline
@@ -273,6 +274,7 @@ struct Context {
     double memoGain = 0.25;
     bool memo3 = true;         // three-step suffix memos (memo3_item) for the plans that admit one
     bool fuseSupport = true;   // batches count a rule's support in its body-size plan where it can
+    bool hubClaims = true;     // repeated leaf hub items of a root are skipped (see kHubSeen)
     std::unordered_map<uint64_t, std::unique_ptr<SuffixMemo>> memos;
     std::vector<std::unique_ptr<DevBuf>> memoChunks;   // one allocation per ensure_memos call
     size_t memoBytes = 0;

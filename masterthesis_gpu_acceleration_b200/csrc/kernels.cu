@@ -540,6 +540,45 @@ __device__ __forceinline__ void emit_pair(const DevPlan& P, long long row, int r
     if (slot < P.keyCap) P.pairKeys[slot] = key;
 }
 
+// Claims a leaf hub item of (root, hub) with middle value `mid` in the
+// task's table (see kHubSeen); false when two other middle values are
+// claimed already.
+__device__ __forceinline__ bool hub_claim(unsigned long long* seen, int root, int hub, int mid) {
+    const unsigned long long key = ((unsigned long long)root << 20) | (unsigned long long)hub;   // 30 bits
+    unsigned long long* w = seen + (((uint32_t)key * 0x9E3779B1u) >> (32 - kHubSeenBits));
+    const unsigned long long m = (uint32_t)mid;
+    unsigned long long old = __ldcg(w);
+    for (int t = 0; t < 8; ++t) {
+        unsigned long long want;
+        const unsigned state = (unsigned)(old >> 32) & 3u;
+        if ((old >> 34) == key && state != 0u) {
+            if (state >= 2u) return false;
+            if ((old & 0xffffffffull) == m) return true;   // the first value again
+            want = (old & ~(3ull << 32)) | (2ull << 32);
+        } else {
+            want = (key << 34) | (1ull << 32) | m;   // displaces another pair: it may repeat items, never lose one
+        }
+        const unsigned long long prev = atomicCAS(w, old, want);
+        if (prev == old) return true;
+        old = prev;
+    }
+    return true;
+}
+
+// The claims of a round's leaf hub items [0, cut) (items at `items`,
+// `stride` ints apart): items that add nothing get wBeg -1.  Out of line,
+// so that the caller's loop keeps its registers.
+__device__ __noinline__ void hub_claims(unsigned long long* seen, const int* items, int stride, int cut, int midAt,
+                                        int* wBeg, int nThreads) {
+    for (int i = threadIdx.x; i < cut; i += nThreads) {
+        const int wb = wBeg[i];
+        if (wb <= -2) {
+            const int* it = items + i * stride;
+            if (!hub_claim(seen, it[0], -2 - wb, it[midAt])) wBeg[i] = -1;
+        }
+    }
+}
+
 // Fused support (plans with supN > 0): the head triples (hS, supPred[j],
 // b), b != hS, of rule j whose pair (hS, b) is set in the plan's row of
 // root i (rows at bm + i * rowWords for the roots rootBeg + i, i < G).
@@ -621,6 +660,10 @@ __device__ __forceinline__ void run_task(Smem<B>& sm, const DevIndex& ix, const 
         for (long long i = tid; i < n4; i += B) b4[i] = make_uint4(0u, 0u, 0u, 0u);
         if (tid == 0) mt.add(16 * (unsigned long long)n4);
     }
+    // leaf hub items: the task's claim table (roots and hubs must fit its fields)
+    const bool claims = P.hubSeen && G <= 1024 && ix.nHub <= (1 << 20);
+    if (claims)
+        for (int i = tid; i < kHubSeen; i += B) P.hubSeen[(long long)blockIdx.x * kHubSeen + i] = 0ull;
     if (tid == 0) {
         S.firstFail = INT_MAX;
         S.safeLevels = 0;
@@ -938,6 +981,12 @@ __device__ __forceinline__ void run_task(Smem<B>& sm, const DevIndex& ix, const 
                     cut = c.item;
                     cutOff = take - c.first(sm) + (c.item == 0 ? off : 0);
                 }
+            }
+            if (anyHub && leaf && claims) {
+                // leaf hub items of a (root, hub) after two middle values add nothing
+                hub_claims(P.hubSeen + (long long)blockIdx.x * kHubSeen, baseK + w0 * strideK, strideK, cut,
+                           stp.keyRef == kTupleHead + 1 ? kTupleHead + 2 : kTupleHead + 1, sm.wBeg, B);
+                __syncthreads();
             }
             if (anyHub) {
                 // hub items of the consumed part of the window: [0, cut)
