@@ -17,6 +17,7 @@
 #include <cstdio>
 #include <cstdlib>
 #include <cstring>
+#include <chrono>
 #include <memory>
 #include <mutex>
 #include <numeric>
@@ -39,6 +40,10 @@ void set_error(const std::string& s) {
 }
 
 namespace {
+double host_ms() {
+    return std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now().time_since_epoch()).count();
+}
+
 // Plans whose leaf hub items may skip repeats (see kHubSeen): the leaf
 // tuple holds hS and two more values, the leaf step expands from one of
 // those two, binds hO and tests nothing but injectivity.
@@ -73,6 +78,7 @@ void Staged::stage(Context& c, std::vector<DevPlan>& plans, const std::vector<co
     if (hint > kMaxSortKeys) allowSort = false;
     if (!nPlans) return;
 
+    double tSect = host_ms();
     // ---- how each kPairs plan deduplicates ----
     // Per-phase global rows (one bitmap row per root, cleared before the
     // launch) while all of them fit the budget.  Beyond it, per plan: sort
@@ -201,6 +207,8 @@ void Staged::stage(Context& c, std::vector<DevPlan>& plans, const std::vector<co
         dSort.ensure(256 + (size_t)keyCap * 16 + pairs_sort_hist_words(keyCap) * 4, as);
         hSort.ensure(8);
     }
+    hostSect[0] += host_ms() - tSect;
+    tSect = host_ms();
     // suffix memos first: the task builder weighs memoised roots by them
     std::vector<std::array<int, 6>> memoKeys;
     auto memo_key_of = [](const DevPlan& P) -> std::array<int, 6> {
@@ -219,6 +227,8 @@ void Staged::stage(Context& c, std::vector<DevPlan>& plans, const std::vector<co
         if (plans[i].memoLevel > 0 && dedup[i] != kDedupSort) memoKeys.push_back(memo_key_of(plans[i]));
     }
     if (!memoKeys.empty()) c.ensure_memos(memoKeys, s);
+    hostSect[1] += host_ms() - tSect;
+    tSect = host_ms();
     std::vector<PhaseTasks> pts(nPlans);
     {
         std::vector<const PhasePlan*> ph;
@@ -237,6 +247,8 @@ void Staged::stage(Context& c, std::vector<DevPlan>& plans, const std::vector<co
             pts[at[k]] = std::move(built[k]);
         }
     }
+    hostSect[2] += host_ms() - tSect;
+    tSect = host_ms();
     // split heavy roots of plans with fused support: counted after the launch
     std::vector<SupJob> supJobs;
     for (int i = 0; i < nPlans; ++i) {
@@ -303,6 +315,8 @@ void Staged::stage(Context& c, std::vector<DevPlan>& plans, const std::vector<co
         tasks.insert(tasks.end(), pts[i].tasks.begin(), pts[i].tasks.end());
         cost.insert(cost.end(), pts[i].cost.begin(), pts[i].cost.end());
     }
+    hostSect[3] += host_ms() - tSect;
+    tSect = host_ms();
     if (sortTasks && tasks.size() > 1) {
         // longest (estimated device time) first, so the tail of the launch is
         // short: a stable counting sort by quarter-octaves of the estimate
@@ -352,6 +366,8 @@ void Staged::stage(Context& c, std::vector<DevPlan>& plans, const std::vector<co
             planTaskEnd.push_back(acc = e);
         }
     }
+    hostSect[4] += host_ms() - tSect;
+    tSect = host_ms();
     size_t planBytes = (size_t)nPlans * sizeof(DevPlan);
     size_t taskBytes = (size_t)nTasks * sizeof(DevTask);
     const size_t sortBytes = ((size_t)nSort * sizeof(int32_t) + 15) & ~size_t(15);
@@ -380,6 +396,7 @@ void Staged::stage(Context& c, std::vector<DevPlan>& plans, const std::vector<co
                         : nullptr;
     h2dBytes = blob;
     d2hBytes = (size_t)nPlans * sizeof(unsigned long long) + 8;
+    hostSect[5] += host_ms() - tSect;
 }
 
 namespace {
@@ -704,6 +721,7 @@ void evaluate_shard(Context& c, const Rule& rule, int shard, int nShards, long l
 // keepPlans: keep a copy of the plans for restaging (prepared batches that
 // may be autotuned); one-shot chunks skip it.
 void prepare(Batch& b, Context& c, const char* const* rules, int n, int isJson, bool keepPlans = true) {
+    const double tStart = host_ms();
     b.c = &c;
     b.n = n;
     b.owner.clear();
@@ -780,7 +798,10 @@ void prepare(Batch& b, Context& c, const char* const* rules, int n, int isJson, 
     // a one-shot batch walks a phase only when the walk costs less host time
     // than the phase is expected to take on the device; a prepared batch,
     // replayed many times, walks every phase the budget allows
+    const double tPlanned = host_ms();
     b.st.stage(c, plans, phases, true, b.stream, b.walkBudget, !keepPlans);
+    b.hostPlanMs = tPlanned - tStart;
+    b.hostStageMs = host_ms() - tPlanned;
 }
 
 void collect(const Batch& b, GpuRuleResult* out, int* status) {
@@ -861,6 +882,8 @@ void finish_load(Context* c) {
     if (const char* m = std::getenv("GPU_RULES_MEMO3")) c->memo3 = std::atoi(m) != 0;
     if (const char* f = std::getenv("GPU_RULES_FUSE_SUPPORT")) c->fuseSupport = std::atoi(f) != 0;
     if (const char* h = std::getenv("GPU_RULES_HUB_CLAIMS")) c->hubClaims = std::atoi(h) != 0;
+    // GPU_RULES_HOST_PROFILE=1: one stderr line of host-side times per one-shot batch
+    if (const char* h = std::getenv("GPU_RULES_HOST_PROFILE")) c->hostProfile = std::atoi(h) != 0;
     c->tasks.reset(new TaskBuilder(c->hix));
     c->tasks->memoRows = [c](int p1, int d1, int p2, int d2, int p3, int d3,
                              double* cost) -> const std::vector<uint8_t>* {
@@ -1013,15 +1036,20 @@ int gpu_evaluate_rules_batch(void* ctx, const char* const* rules, int n, int isJ
         const int K = c.batchChunks > 0 ? std::max(1, std::min(c.batchChunks, std::max(n, 1)))
                                         : std::max(1, std::min(8, (n + 1249) / 1250));
         while ((int)c.pipe.size() < K) c.pipe.push_back(new Batch());
+        const double t0 = host_ms();
+        double planMs = 0, stageMs = 0;
         for (int k = 0; k < K; ++k) {
             const int lo = (int)((long long)n * k / K), hi = (int)((long long)n * (k + 1) / K);
             Batch& b = *c.pipe[k];
             prepare(b, c, rules + lo, hi - lo, isJson, false);
+            planMs += b.hostPlanMs;
+            stageMs += b.hostStageMs;
             ck(cudaEventRecord(b.ev0, b.stream), "event");
             b.st.enqueue(c, b.stream, 0);
             ck(cudaEventRecord(b.ev1, b.stream), "event");
             b.st.download(b.stream);
         }
+        const double t1 = host_ms();
         float span = 0.f;
         for (int k = 0; k < K; ++k) {
             Batch& b = *c.pipe[k];
@@ -1043,6 +1071,19 @@ int gpu_evaluate_rules_batch(void* ctx, const char* const* rules, int n, int isJ
             collect(b, out + lo, status ? status + lo : nullptr);
         }
         if (deviceMs) *deviceMs = span;
+        if (c.hostProfile) {
+            double sect[6] = {0, 0, 0, 0, 0, 0};
+            for (int k = 0; k < K; ++k)
+                for (int j = 0; j < 6; ++j) {
+                    sect[j] += c.pipe[k]->st.hostSect[j];
+                    c.pipe[k]->st.hostSect[j] = 0.0;
+                }
+            std::fprintf(stderr, "[gpu_rules] batch of %d in %d chunks: parse+plan %.2f ms, staging %.2f ms "
+                         "(dedup %.2f, memos %.2f, tasks %.2f, plans %.2f, order %.2f, upload %.2f), enqueue loop "
+                         "%.2f ms, wait+collect %.2f ms, device span %.2f ms\n",
+                         n, K, planMs, stageMs, sect[0], sect[1], sect[2], sect[3], sect[4], sect[5],
+                         t1 - t0 - planMs - stageMs, host_ms() - t1, (double)span);
+        }
         return 0;
     } catch (const std::exception& e) {
         set_error(std::string("gpu_evaluate_rules_batch error: ") + e.what());

@@ -149,6 +149,9 @@ struct Staged {
     int nSupJobs = 0;
     const SupJob* dSupJobs = nullptr;      // in dBlob
     DevBuf dHubSeen;                       // leaf hub claims: kHubSeen words per resident block
+    // host ms of the staging sections (dedup and fusion, memos, task build,
+    // plan fields, task order, upload), summed until read
+    double hostSect[6] = {0, 0, 0, 0, 0, 0};
     HostBuf hSort;                      // the downloaded append cursor
     HostBuf hIncomplete;                // per plan: a task was abandoned at the deadline
     bool budgeted = false;              // the last enqueue ran under a deadline
@@ -275,6 +278,7 @@ struct Context {
     bool memo3 = true;         // three-step suffix memos (memo3_item) for the plans that admit one
     bool fuseSupport = true;   // batches count a rule's support in its body-size plan where it can
     bool hubClaims = true;     // repeated leaf hub items of a root are skipped (see kHubSeen)
+    bool hostProfile = false;  // one-shot batches print their host-side times
     std::unordered_map<uint64_t, std::unique_ptr<SuffixMemo>> memos;
     std::vector<std::unique_ptr<DevBuf>> memoChunks;   // one allocation per ensure_memos call
     size_t memoBytes = 0;
@@ -425,6 +429,7 @@ struct Batch {
     DevBuf flush;
     double lastMs = 0.0;
     double walkBudget = 4.0e6;
+    double hostPlanMs = 0.0, hostStageMs = 0.0;   // host time of the last prepare
 
     ~Batch() {
         if (c) cudaSetDevice(c->device);

@@ -1,14 +1,97 @@
 // parallel.hpp — a blocking parallel loop over host threads for the batch
 // preparation (parsing, planning and task building of large rule batches).
 #pragma once
+#include <unistd.h>
+
 #include <algorithm>
 #include <atomic>
+#include <condition_variable>
+#include <cstdint>
 #include <exception>
+#include <functional>
 #include <mutex>
 #include <thread>
 #include <vector>
 
 namespace gr {
+
+// Worker threads started once per process and reused by every parallel
+// loop: starting threads per loop cost about as much as the preparation of
+// a batch chunk itself.  One loop runs on the pool at a time; a loop that
+// finds it busy (another host thread's loop, or one nested in a loop body)
+// runs on its calling thread alone, as does any loop in a process forked
+// after the pool started.
+class HostPool {
+public:
+    // Never destroyed: its workers end with the process (a forked child,
+    // which has none of them, must not wait for them either).
+    static HostPool& get() {
+        static HostPool* pool = new HostPool();
+        return *pool;
+    }
+    // Runs work() on the calling thread and on up to n - 1 workers and
+    // returns when all have returned; false (nothing run) when the pool is
+    // busy or belongs to another process.
+    bool run(unsigned n, const std::function<void()>& work) {
+        if (inWorker() || ::getpid() != pid_) return false;
+        std::unique_lock<std::mutex> region(regionMu_, std::try_to_lock);
+        if (!region.owns_lock()) return false;
+        const unsigned helpers = std::min<unsigned>(n > 0 ? n - 1 : 0, nWorkers_);
+        job_ = &work;
+        want_ = helpers;
+        pending_.store(helpers, std::memory_order_relaxed);
+        {
+            std::lock_guard<std::mutex> lk(mu_);   // a sleeping worker sees the new generation
+            gen_.fetch_add(1, std::memory_order_release);
+        }
+        cv_.notify_all();
+        work();
+        while (pending_.load(std::memory_order_acquire) != 0) std::this_thread::yield();
+        job_ = nullptr;
+        return true;
+    }
+private:
+    HostPool() : pid_(::getpid()) {
+        const unsigned hw = std::max(1u, std::thread::hardware_concurrency());
+        for (unsigned i = 0; i + 1 < std::min(hw, 64u); ++i) std::thread([this, i] { loop(i); }).detach();
+        nWorkers_ = std::max(1u, std::min(hw, 64u)) - 1;
+    }
+    static bool& inWorker() {
+        static thread_local bool w = false;
+        return w;
+    }
+    // After each loop a worker polls for the next one for a while (the
+    // loops of one batch come a few hundred microseconds apart), then
+    // sleeps until woken.
+    void loop(unsigned idx) {
+        inWorker() = true;
+        uint64_t seen = 0;   // the generation when the pool started (a loop may come before this thread runs)
+        for (;;) {
+            uint64_t g = gen_.load(std::memory_order_acquire);
+            for (int spin = 0; g == seen && spin < 20000; ++spin) {
+                std::this_thread::yield();
+                g = gen_.load(std::memory_order_acquire);
+            }
+            if (g == seen) {
+                std::unique_lock<std::mutex> lk(mu_);
+                cv_.wait(lk, [&] { return gen_.load(std::memory_order_acquire) != seen; });
+                g = gen_.load(std::memory_order_acquire);
+            }
+            seen = g;
+            if (idx >= want_) continue;
+            (*job_)();
+            pending_.fetch_sub(1, std::memory_order_acq_rel);
+        }
+    }
+    unsigned nWorkers_ = 0;
+    std::mutex mu_, regionMu_;
+    std::condition_variable cv_;
+    const std::function<void()>* job_ = nullptr;   // written before gen_ is raised
+    unsigned want_ = 0;
+    std::atomic<unsigned> pending_{0};
+    std::atomic<uint64_t> gen_{0};
+    const pid_t pid_;
+};
 
 // Calls fn(i) for i in [0, n) on up to maxThreads threads (the calling
 // thread included), in chunks of `grain`; serial below 2 * grain items.
@@ -38,11 +121,8 @@ void parallel_for(size_t n, Fn fn, size_t grain = 64, unsigned maxThreads = 16) 
             next = n;
         }
     };
-    std::vector<std::thread> pool;
-    pool.reserve(t - 1);
-    for (unsigned k = 1; k < t; ++k) pool.emplace_back(work);
-    work();
-    for (auto& th : pool) th.join();
+    const std::function<void()> job(work);
+    if (!HostPool::get().run(t, job)) work();
     if (err) std::rethrow_exception(err);
 }
 
