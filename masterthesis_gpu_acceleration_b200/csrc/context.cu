@@ -66,6 +66,7 @@ constexpr unsigned long long kMaxSortKeys = 0xffffffffull;   // the sort's 32-bi
 void Staged::stage(Context& c, std::vector<DevPlan>& plans, const std::vector<const PhasePlan*>& phases,
                    bool sortTasks, cudaStream_t s, double walkBudget, bool costAware, bool allowSort) {
     nPlans = (int)plans.size();
+    nResults = nPlans + extraResults;
     nTasks = 0;
     bitmapWords = 0;
     blockWords = blockRegions = 0;
@@ -166,29 +167,6 @@ void Staged::stage(Context& c, std::vector<DevPlan>& plans, const std::vector<co
             blockWords = (need + 3) & ~size_t(3);
         }
     }
-    // fused support: a body-size plan whose pair rows are complete at the
-    // end of each task (shared rows or block rows) counts the support of the
-    // rules in `fuse`; their support plans get no tasks
-    std::vector<char> skip(nPlans, 0);
-    for (int i = 0; i < nPlans; ++i) {
-        DevPlan& P = plans[i];
-        P.supN = P.supDomPred = P.supDomDir = 0;
-        for (int j = 0; j < kMaxSupFused; ++j) P.supPred[j] = P.supSlot[j] = 0;
-    }
-    for (const auto& f : fuse) {
-        const int sp = f[0], bp = f[1];
-        if (sp < 0 || bp < 0 || sp >= nPlans || bp >= nPlans || skip[sp] || skip[bp]) continue;
-        DevPlan& B = plans[bp];
-        if (B.mode != kPairs || B.supN >= kMaxSupFused || plans[sp].mode != kExist) continue;
-        if (dedup[bp] != kDedupShared && dedup[bp] != kDedupBlockRows) continue;
-        const auto dom = ho_domain(B);
-        B.supDomPred = dom.first;
-        B.supDomDir = dom.second;
-        B.supPred[B.supN] = f[2];
-        B.supSlot[B.supN] = sp;
-        ++B.supN;
-        skip[sp] = 1;
-    }
     std::vector<size_t> gOff(nPlans, 0);
     for (int i = 0; i < nPlans; ++i) {
         if (dedup[i] != kDedupRows) continue;
@@ -229,24 +207,8 @@ void Staged::stage(Context& c, std::vector<DevPlan>& plans, const std::vector<co
     if (!memoKeys.empty()) c.ensure_memos(memoKeys, s);
     hostSect[1] += host_ms() - tSect;
     tSect = host_ms();
-    std::vector<PhaseTasks> pts(nPlans);
-    {
-        std::vector<const PhasePlan*> ph;
-        std::vector<PhaseLimits> li;
-        std::vector<int> at;
-        for (int i = 0; i < nPlans; ++i)
-            if (!skip[i]) {
-                ph.push_back(phases[i]);
-                li.push_back(lim[i]);
-                at.push_back(i);
-            }
-        std::vector<PhaseTasks> built;
-        c.tasks->build(ph, c.grid, true, built, walkBudget, costAware, &li);
-        for (size_t k = 0; k < at.size(); ++k) {
-            for (DevTask& t : built[k].tasks) t.plan = at[k];
-            pts[at[k]] = std::move(built[k]);
-        }
-    }
+    std::vector<PhaseTasks> pts;
+    c.tasks->build(phases, c.grid, true, pts, walkBudget, costAware, &lim);
     hostSect[2] += host_ms() - tSect;
     tSect = host_ms();
     // split heavy roots of plans with fused support: counted after the launch
@@ -382,9 +344,10 @@ void Staged::stage(Context& c, std::vector<DevPlan>& plans, const std::vector<co
     hTasks = std::move(tasks);   // kept for profiles and task-time learning
     hCost = std::move(cost);
     dBlob.ensure(blob, as);
-    dResults.ensure((size_t)nPlans * sizeof(unsigned long long), as);
+    nResults = nPlans + extraResults;
+    dResults.ensure((size_t)nResults * sizeof(unsigned long long), as);
     dCtl.ensure(64, as);
-    hResults.ensure((size_t)nPlans * sizeof(unsigned long long));
+    hResults.ensure((size_t)nResults * sizeof(unsigned long long));
     hCtl.ensure(64);
     ck(cudaMemcpyAsync(dBlob.p, hBlob.p, blob, cudaMemcpyHostToDevice, s), "H2D plans");
     dPlans = static_cast<const DevPlan*>(dBlob.p);
@@ -395,7 +358,7 @@ void Staged::stage(Context& c, std::vector<DevPlan>& plans, const std::vector<co
                                                           sortBytes)
                         : nullptr;
     h2dBytes = blob;
-    d2hBytes = (size_t)nPlans * sizeof(unsigned long long) + 8;
+    d2hBytes = (size_t)nResults * sizeof(unsigned long long) + 8;
     hostSect[5] += host_ms() - tSect;
 }
 
@@ -540,7 +503,7 @@ void Staged::restage(Context& c, cudaStream_t s) {
 void Staged::enqueue(Context& c, cudaStream_t s, int instr, int gridCap, unsigned long long budgetNs) {
     budgeted = false;
     if (!nPlans) return;
-    ck(cudaMemsetAsync(dResults.p, 0, (size_t)nPlans * sizeof(unsigned long long), s), "memset results");
+    ck(cudaMemsetAsync(dResults.p, 0, (size_t)nResults * sizeof(unsigned long long), s), "memset results");
     ck(cudaMemsetAsync(dCtl.p, 0, 8, s), "memset ctl");
     if (bitmapWords) ck(cudaMemsetAsync(dBitmap.p, 0, bitmapWords * 4, s), "memset bitmap");
     if (heavyWords) ck(cudaMemsetAsync(dHeavy.p, 0, heavyWords * 4, s), "memset heavy rows");
@@ -751,13 +714,46 @@ void prepare(Batch& b, Context& c, const char* const* rules, int n, int isJson, 
             b.parseStatus[i] = -1;
         }
     }, 128);
+    // fused support: a rule whose support its body-size plan can count (see
+    // RulePlan::supFuse) gets no support plan when that plan keeps its pair
+    // rows in shared memory (no global dedup bitmap, no forced mode); the
+    // count lands in a result slot after the plans' own
+    const bool fuse = c.fuseSupport && (c.batchPhases & 3) == 3 && c.dedupForce == 0;
+    b.supOf.assign(n, -1);
+    std::vector<std::array<int, 3>> fused;   // {body plan, head predicate, first rule}
+    std::unordered_map<uint64_t, int> fusedAt;
     for (int i = 0; i < n; ++i) {
         if (b.parseStatus[i] != 0) continue;
         RulePlan& rp = b.rps[i];
         if (rp.status != kRuleOk) continue;
-        for (int k = 0; k < 2; ++k) {
+        int bodyPlan = -1;
+        for (int k : {1, 0}) {
             const PhasePlan& ph = k == 0 ? rp.support : rp.body;
             if (ph.how != kDevice || !(c.batchPhases & (1 << k))) continue;
+            if (k == 0 && fuse && rp.supFuse >= 0 && bodyPlan >= 0 && phases[bodyPlan]->plan.mode == kPairs &&
+                !phases[bodyPlan]->needsGlobalBitmap) {
+                const uint64_t key = ((uint64_t)(uint32_t)bodyPlan << 32) | (uint32_t)rp.supFuse;
+                auto it = fusedAt.find(key);
+                if (it != fusedAt.end()) {
+                    b.supOf[i] = it->second;
+                    continue;
+                }
+                DevPlan& B = plans[(size_t)bodyPlan];
+                if (B.supN < kMaxSupFused) {
+                    if (B.supN == 0) {
+                        const auto dom = ho_domain(B);
+                        B.supDomPred = dom.first;
+                        B.supDomDir = dom.second;
+                    }
+                    B.supPred[B.supN] = rp.supFuse;
+                    B.supSlot[B.supN] = (int32_t)fused.size();   // made absolute below
+                    ++B.supN;
+                    fusedAt.emplace(key, (int)fused.size());
+                    b.supOf[i] = (int)fused.size();
+                    fused.push_back({bodyPlan, rp.supFuse, i});
+                    continue;
+                }
+            }
             // identical computations (same plan and roots, e.g. one body under
             // several heads) run once; the others share the count
             // keyed by hash, confirmed by the full signature (plans are
@@ -769,26 +765,23 @@ void prepare(Batch& b, Context& c, const char* const* rules, int n, int isJson, 
                 if (phase_equal(*phases[it->second], ph)) same = it->second;
             if (same >= 0) {
                 b.shared.emplace_back(2 * i + k, same);
+                if (k == 1) bodyPlan = same;
                 continue;
             }
             seen.emplace(h, (int)plans.size());
+            if (k == 1) bodyPlan = (int)plans.size();
             plans.push_back(ph.plan);
             phases.push_back(&ph);
             b.owner.push_back(2 * i + k);
         }
     }
-    // fused support: the rules whose support their body-size plan counts
-    b.st.fuse.clear();
-    if (c.fuseSupport && (c.batchPhases & 3) == 3) {
-        std::vector<int> planOf(2 * (size_t)n, -1);
-        for (size_t k = 0; k < b.owner.size(); ++k) planOf[(size_t)b.owner[k]] = (int)k;
-        for (const auto& sh : b.shared) planOf[(size_t)sh.first] = sh.second;
-        for (int i = 0; i < n; ++i) {
-            if (b.parseStatus[i] != 0 || b.rps[i].status != kRuleOk || b.rps[i].supFuse < 0) continue;
-            const int sp = planOf[2 * (size_t)i], bp = planOf[2 * (size_t)i + 1];
-            if (sp >= 0 && bp >= 0) b.st.fuse.push_back({sp, bp, b.rps[i].supFuse});
-        }
-    }
+    // fused counts follow the plans' own result slots
+    const int nPlansOwn = (int)plans.size();
+    for (DevPlan& P : plans)
+        for (int j = 0; j < P.supN; ++j) P.supSlot[j] += nPlansOwn;
+    for (int i = 0; i < n; ++i)
+        if (b.supOf[i] >= 0) b.supOf[i] += nPlansOwn;
+    b.st.extraResults = (int)fused.size();
     if (!b.stream) ck(cudaStreamCreateWithFlags(&b.stream, cudaStreamNonBlocking), "cudaStreamCreate");
     if (!b.ev0) ck(cudaEventCreate(&b.ev0), "cudaEventCreate");
     if (!b.ev1) ck(cudaEventCreate(&b.ev1), "cudaEventCreate");
@@ -804,8 +797,11 @@ void prepare(Batch& b, Context& c, const char* const* rules, int n, int isJson, 
     b.hostStageMs = host_ms() - tPlanned;
 }
 
-void collect(const Batch& b, GpuRuleResult* out, int* status) {
-    std::vector<int64_t> sup(b.n), body(b.n);
+// Each rule's support and body size after a run: static values, the plans'
+// own counts (shared ones included) and fused support counts.
+void phase_counts(const Batch& b, std::vector<int64_t>& sup, std::vector<int64_t>& body) {
+    sup.resize(b.n);
+    body.resize(b.n);
     for (int i = 0; i < b.n; ++i) { sup[i] = b.rps[i].support.value; body[i] = b.rps[i].body.value; }
     const unsigned long long* cnt = b.st.counts();
     for (size_t k = 0; k < b.owner.size(); ++k) {
@@ -818,6 +814,13 @@ void collect(const Batch& b, GpuRuleResult* out, int* status) {
         if (sh.first % 2 == 0) sup[i] = (int64_t)cnt[sh.second];
         else body[i] = (int64_t)cnt[sh.second];
     }
+    for (int i = 0; i < b.n && i < (int)b.supOf.size(); ++i)
+        if (b.supOf[i] >= 0) sup[i] = (int64_t)cnt[b.supOf[i]];
+}
+
+void collect(const Batch& b, GpuRuleResult* out, int* status) {
+    std::vector<int64_t> sup, body;
+    phase_counts(b, sup, body);
     for (int i = 0; i < b.n; ++i) {
         if (status) status[i] = b.parseStatus[i];
         if (b.parseStatus[i] != 0) { out[i] = GpuRuleResult{}; continue; }
@@ -1136,19 +1139,8 @@ int gpu_batch_run(void* batch, long long flushBytes, GpuRuleResult* out, int* st
 int gpu_batch_counts(void* batch, long long* counts, int* status) {
     if (!batch || !counts) return -1;
     const Batch& b = *static_cast<const Batch*>(batch);
-    std::vector<int64_t> sup(b.n), body(b.n);
-    for (int i = 0; i < b.n; ++i) { sup[i] = b.rps[i].support.value; body[i] = b.rps[i].body.value; }
-    const unsigned long long* cnt = b.st.counts();
-    for (size_t k = 0; k < b.owner.size(); ++k) {
-        int i = b.owner[k] / 2;
-        if (b.owner[k] % 2 == 0) sup[i] = (int64_t)cnt[k];
-        else body[i] = (int64_t)cnt[k];
-    }
-    for (const auto& sh : b.shared) {
-        int i = sh.first / 2;
-        if (sh.first % 2 == 0) sup[i] = (int64_t)cnt[sh.second];
-        else body[i] = (int64_t)cnt[sh.second];
-    }
+    std::vector<int64_t> sup, body;
+    phase_counts(b, sup, body);
     for (int i = 0; i < b.n; ++i) {
         const RulePlan& rp = b.rps[i];
         const bool ok = b.parseStatus[i] == 0;

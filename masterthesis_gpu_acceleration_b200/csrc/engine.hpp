@@ -140,12 +140,10 @@ struct Staged {
     unsigned long long keyCap = 0;
     unsigned long long keyHint = 0;     // exact keys of a run that overflowed keyCap
     const int32_t* dSortSlots = nullptr;   // result slot of each sort index (in dBlob)
-    // Fused support, set before staging: {support plan, body-size plan, head
-    // predicate} of rules whose support the body-size plan may count (see
-    // RulePlan::supFuse).  Staging fuses those whose body-size rows are
-    // complete at the end of each task and gives their support plans no
-    // tasks; split heavy roots are counted by support_rows after the launch.
-    std::vector<std::array<int, 3>> fuse;
+    // Result slots after the plans' own (fused support counts, see
+    // RulePlan::supFuse), set before staging; nResults = nPlans + extraResults.
+    int extraResults = 0;
+    int nResults = 0;
     int nSupJobs = 0;
     const SupJob* dSupJobs = nullptr;      // in dBlob
     DevBuf dHubSeen;                       // leaf hub claims: kHubSeen words per resident block
@@ -222,7 +220,8 @@ struct Staged {
     }
     void download(cudaStream_t s) {
         if (!nPlans) return;
-        ck(cudaMemcpyAsync(hResults.p, dResults.p, nPlans * sizeof(unsigned long long), cudaMemcpyDeviceToHost, s), "D2H results");
+        ck(cudaMemcpyAsync(hResults.p, dResults.p, nResults * sizeof(unsigned long long), cudaMemcpyDeviceToHost, s),
+           "D2H results");
         ck(cudaMemcpyAsync(hCtl.p, dCtl.p, 8, cudaMemcpyDeviceToHost, s), "D2H status");
         download_cursor(s);
         if (budgeted)
@@ -416,6 +415,7 @@ struct Batch {
     std::vector<RulePlan> rps;
     std::vector<int> parseStatus;
     std::vector<int> owner;  // plan -> rule * 2 + phase
+    std::vector<int> supOf;  // rule -> result slot of its fused support count, or -1
     // phases identical to an earlier one of the batch (same plan and roots):
     // (rule * 2 + phase, plan whose count they share); computed once per run
     std::vector<std::pair<int, int>> shared;
