@@ -231,16 +231,21 @@ struct Geom {
 // Profiling outputs of the instrumented kernel variant (null members are
 // skipped): requested global-memory bytes, and per task its start and end
 // time (globaltimer ns).
-// One suffix memo to build for hub row `row` of (p1, d1).  Two steps
-// (p3 < 0): through (p2, d2), bitmaps S1 then S2 of `words` words at `bits`.
-// Three steps: through (p2, d2) then (p3, d3), the bitmap S1 (`words`
-// words) then one path count per rank of the domain (`wo` ranks), a byte
-// each (four to a word) that saturates at 255.
+// One suffix memo to build for hub row `row` of (p1, d1), or the part that
+// starts from the row's values [b0, b1) (b1 < 0: all of them; the parts of
+// one memo add into the same bits).  Two steps (p3 < 0): through (p2, d2),
+// bitmaps S1 then S2 of `words` words at `bits`.  Three steps: through
+// (p2, d2) then (p3, d3), the bitmap S1 (`words` words) then one path count
+// per rank of the domain (`wo` ranks), a byte each (four to a word) that
+// saturates at 255.
 struct MemoJob {
     int32_t p1, d1, p2, d2, row, words;
-    int32_t p3, d3, wo, pad;
+    int32_t p3, d3, wo, b0, b1, pad;
     uint32_t* bits;
 };
+// Three-step memo parts count paths in shared memory (one 32-bit counter
+// per rank) when the domain has at most this many ranks.
+constexpr int kMemoSmemRanks = 16384;
 
 struct EngineProfile {
     unsigned long long* bytes = nullptr;

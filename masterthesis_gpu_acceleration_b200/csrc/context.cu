@@ -462,7 +462,17 @@ void Context::ensure_memos(const std::vector<std::array<int, 6>>& keys, cudaStre
         for (size_t j = 0; j < rows.size(); ++j) {
             tab[h.hubOf[d1][rows[j]]] = (int32_t)j;
             m->rowHasMemo[(size_t)(rows[j] - h.predRow[d1][p1])] = 1;
-            all.push_back(MemoJob{p1, d1, p2, d2, rows[j], words, p3, d3, wo, 0, bits + j * stride});
+            if (p3 < 0) {
+                all.push_back(MemoJob{p1, d1, p2, d2, rows[j], words, p3, d3, wo, 0, -1, 0, bits + j * stride});
+                continue;
+            }
+            // three steps: one block per slice of the row's values, so that
+            // the paths of a long row spread over the SMs
+            constexpr int32_t kSlice = 64;
+            const int32_t len = h.rowBeg[d1][rows[j] + 1] - h.rowBeg[d1][rows[j]];
+            for (int32_t b0 = 0; b0 < len; b0 += kSlice)
+                all.push_back(MemoJob{p1, d1, p2, d2, rows[j], words, p3, d3, wo, b0, std::min(len, b0 + kSlice), 0,
+                                      bits + j * stride});
         }
         m->tab = reinterpret_cast<const int32_t*>(base + t * tabBytes);
         m->bits = bits;
@@ -476,7 +486,10 @@ void Context::ensure_memos(const std::vector<std::array<int, 6>>& keys, cudaStre
     memoJobs.ensure(all.size() * sizeof(MemoJob));
     ck(cudaMemcpyAsync(memoJobs.p, all.data(), all.size() * sizeof(MemoJob), cudaMemcpyHostToDevice, s),
        "H2D memo jobs");
-    ck(memo_build(dix, static_cast<const MemoJob*>(memoJobs.p), (int)all.size(), s), "memo build");
+    int maxWo = 0;
+    for (const MemoJob& j : all)
+        if (j.p3 >= 0) maxWo = std::max(maxWo, j.wo);
+    ck(memo_build(dix, static_cast<const MemoJob*>(memoJobs.p), (int)all.size(), maxWo, s), "memo build");
     ck(cudaStreamSynchronize(s), "memo build");   // memos are shared by every stream afterwards
 }
 

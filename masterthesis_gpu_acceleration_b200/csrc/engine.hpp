@@ -26,7 +26,9 @@ namespace gr {
 
 size_t engine_smem_bytes(int block);
 cudaError_t engine_configure();
-cudaError_t memo_build(const DevIndex& ix, const MemoJob* jobs, int nJobs, cudaStream_t stream);
+// maxWo: the largest three-step domain among the jobs (0: none), which
+// sizes the shared path counters.
+cudaError_t memo_build(const DevIndex& ix, const MemoJob* jobs, int nJobs, int maxWo, cudaStream_t stream);
 // Fused support of split heavy roots, after the engine launch that filled
 // their rows (see DevPlan::supN).
 cudaError_t support_rows(const DevIndex& ix, const DevPlan* plans, const SupJob* jobs, int nJobs,

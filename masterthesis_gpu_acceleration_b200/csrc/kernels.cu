@@ -36,6 +36,7 @@
 #include <cooperative_groups.h>
 #include <cuda_runtime.h>
 
+#include <algorithm>
 #include <climits>
 #include <cstdint>
 
@@ -584,10 +585,11 @@ __device__ __noinline__ void hub_claims(unsigned long long* seen, const int* ite
 // root i (rows at bm + i * rowWords for the roots rootBeg + i, i < G).
 // Warps take the roots, lanes a root's head triples; returns this lane's
 // count.  Out of line and small: it runs once per task, after the search.
+// `part` of `nParts` takes every nParts-th group of 32 head triples.
 template <bool kC>
 __device__ __noinline__ unsigned long long fused_support(const DevPlan& P, const DevIndex& ix, int j, int rootBeg,
                                                          int G, const uint32_t* bm, int warp, int nWarps, int lane,
-                                                         Meter<kC>& mt) {
+                                                         int part, int nParts, Meter<kC>& mt) {
     unsigned long long n = 0;
     const int hp = P.supPred[j], dp = P.supDomPred, dd = P.supDomDir;
     for (int i = warp; i < G; i += nWarps) {
@@ -595,7 +597,7 @@ __device__ __noinline__ unsigned long long fused_support(const DevPlan& P, const
         mt.add(4);
         const int2 hr = row_lookup(ix, hp, 0, a, mt);
         const uint32_t* row = bm + (long long)i * P.rowWords;
-        for (int e = hr.x + lane; e < hr.y; e += 32) {
+        for (int e = hr.x + 32 * part + lane; e < hr.y; e += 32 * nParts) {
             const int b = __ldg(ix.val[0] + e);
             mt.add(4);
             if (b == a) continue;
@@ -1085,7 +1087,7 @@ __device__ __forceinline__ void run_task(Smem<B>& sm, const DevIndex& ix, const 
     if (P.supN > 0 && !heavy) {
         const int lane = tid & 31;
         for (int j = 0; j < P.supN; ++j) {
-            unsigned long long n = fused_support(P, ix, j, task.beg, G, bm, tid >> 5, B / 32, lane, mt);
+            unsigned long long n = fused_support(P, ix, j, task.beg, G, bm, tid >> 5, B / 32, lane, 0, 1, mt);
 #pragma unroll
             for (int d = 16; d; d >>= 1) n += __shfl_down_sync(0xffffffffu, n, d);
             if (lane == 0 && n) atomicAdd(results + P.supSlot[j], n);
@@ -1217,44 +1219,98 @@ static void launch_b(const DevIndex& ix, const DevPlan* plans, const DevTask* ta
 // transition); warps take the y in N1(x), lanes the h in N2(y).  The first
 // witness of h sets its S1 bit, any later one its S2 bit (atomicOr returns
 // the old word).
+// Adds one path ending at `rank` to a three-step memo's counts: a 32-bit
+// shared counter, or the saturating byte in global memory.
+__device__ __forceinline__ void memo3_count_path(uint32_t* smemCnt, uint32_t* cnt, uint32_t* S1, int rank) {
+    if (smemCnt) {
+        atomicAdd(smemCnt + rank, 1u);
+        return;
+    }
+    uint32_t* cw = cnt + (rank >> 2);
+    const int sh = (rank & 3) * 8;
+    uint32_t old = *cw;
+    while (((old >> sh) & 0xffu) != 0xffu) {
+        const uint32_t seen = atomicCAS(cw, old, old + (1u << sh));
+        if (seen == old) break;
+        old = seen;
+    }
+    atomicOr(S1 + (rank >> 5), 1u << (rank & 31));
+}
+
 __global__ void memo_build_kernel(DevIndex ix, const MemoJob* jobs, int nJobs) {
+    extern __shared__ uint32_t memoSmem[];
     if ((int)blockIdx.x >= nJobs) return;
     const MemoJob job = jobs[blockIdx.x];
     uint32_t* S1 = job.bits;
     uint32_t* S2 = S1 + job.words;
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nWarps = blockDim.x >> 5;
-    const int b = ix.rowBeg[job.d1][job.row], e = ix.rowBeg[job.d1][job.row + 1];
+    const int rb = ix.rowBeg[job.d1][job.row], re = ix.rowBeg[job.d1][job.row + 1];
+    const int b = rb + job.b0, e = job.b1 < 0 ? re : rb + job.b1;
     Meter<false> mt;
     if (job.p3 >= 0) {
-        // three steps: warps take the v2 in N1(x), lanes the v3 in N2(v2);
-        // every path x -> v2 -> v3 -> h with x, v2, v3, h distinct counts
-        // once for h (its S1 bit and its count)
+        // three steps: warps take the v2 of the slice, lanes the v3 in
+        // N2(v2) and their N3 rows (a long one by the whole warp); every
+        // path x -> v2 -> v3 -> h with x, v2, v3, h distinct counts once for
+        // h, in shared counters added into the memo's bytes at the end
         const int x = ix.rowKey[job.d1][job.row];
         uint32_t* cnt = S1 + job.words;
+        uint32_t* sc = job.wo <= kMemoSmemRanks ? memoSmem : nullptr;
+        if (sc) {
+            for (int r = threadIdx.x; r < job.wo; r += blockDim.x) sc[r] = 0u;
+            __syncthreads();
+        }
         for (int i = b + warp; i < e; i += nWarps) {
             const int v2 = __ldg(ix.val[job.d1] + i);
             if (v2 == x) continue;
             const int2 r2 = row_lookup(ix, job.p2, job.d2, v2, mt);
-            for (int j = r2.x + lane; j < r2.y; j += 32) {
-                const int v3 = __ldg(ix.val[job.d2] + j);
-                if (v3 == x || v3 == v2) continue;
-                const int2 r3 = row_lookup(ix, job.p3, job.d3, v3, mt);
-                for (int t = r3.x; t < r3.y; ++t) {
-                    const int h = __ldg(ix.val[job.d3] + t);
-                    if (h == x || h == v2 || h == v3) continue;
-                    const int rank = __ldg(ix.valRank[job.d3] + t);
-                    if (rank < 0 || rank >= job.wo) continue;
-                    // saturating byte increment of the rank's path count
-                    uint32_t* cw = cnt + (rank >> 2);
-                    const int sh = (rank & 3) * 8;
-                    uint32_t old = *cw;
-                    while (((old >> sh) & 0xffu) != 0xffu) {
-                        const uint32_t seen = atomicCAS(cw, old, old + (1u << sh));
-                        if (seen == old) break;
-                        old = seen;
-                    }
-                    atomicOr(S1 + (rank >> 5), 1u << (rank & 31));
+            for (int j0 = r2.x; j0 < r2.y; j0 += 32) {
+                const int j = j0 + lane;
+                int v3 = -1;
+                int2 r3 = make_int2(0, 0);
+                if (j < r2.y) {
+                    v3 = __ldg(ix.val[job.d2] + j);
+                    if (v3 != x && v3 != v2) r3 = row_lookup(ix, job.p3, job.d3, v3, mt);
                 }
+                const bool longRow = r3.y - r3.x >= 32;
+                if (!longRow)
+                    for (int t = r3.x; t < r3.y; ++t) {
+                        const int h = __ldg(ix.val[job.d3] + t);
+                        if (h == x || h == v2 || h == v3) continue;
+                        const int rank = __ldg(ix.valRank[job.d3] + t);
+                        if (rank >= 0 && rank < job.wo) memo3_count_path(sc, cnt, S1, rank);
+                    }
+                unsigned big = __ballot_sync(0xffffffffu, longRow);
+                while (big) {   // long N3 rows: the whole warp walks each
+                    const int src = __ffs(big) - 1;
+                    big &= big - 1;
+                    const int w3 = __shfl_sync(0xffffffffu, v3, src);
+                    const int t0 = __shfl_sync(0xffffffffu, r3.x, src), t1 = __shfl_sync(0xffffffffu, r3.y, src);
+                    for (int t = t0 + lane; t < t1; t += 32) {
+                        const int h = __ldg(ix.val[job.d3] + t);
+                        if (h == x || h == v2 || h == w3) continue;
+                        const int rank = __ldg(ix.valRank[job.d3] + t);
+                        if (rank >= 0 && rank < job.wo) memo3_count_path(sc, cnt, S1, rank);
+                    }
+                }
+            }
+        }
+        if (sc) {
+            __syncthreads();
+            for (int r = threadIdx.x; r < job.wo; r += blockDim.x) {
+                const uint32_t add = min(sc[r], 255u);
+                if (!add) continue;
+                uint32_t* cw = cnt + (r >> 2);
+                const int sh = (r & 3) * 8;
+                uint32_t old = *cw;
+                for (;;) {
+                    const uint32_t cur = (old >> sh) & 0xffu;
+                    const uint32_t nv = min(cur + add, 255u);
+                    if (nv == cur) break;
+                    const uint32_t seen = atomicCAS(cw, old, (old & ~(0xffu << sh)) | (nv << sh));
+                    if (seen == old) break;
+                    old = seen;
+                }
+                atomicOr(S1 + (r >> 5), 1u << (r & 31));
             }
         }
         return;
@@ -1273,20 +1329,19 @@ __global__ void memo_build_kernel(DevIndex ix, const MemoJob* jobs, int nJobs) {
     }
 }
 
-// Fused support of split heavy roots: one warp per job counts the head
-// triples of the job's root against its completed global row.
+// Fused support of split heavy roots: one block per job, its warps share the
+// head triples of the job's root, counted against its completed global row.
 __global__ void support_rows_kernel(const __grid_constant__ DevIndex ix, const DevPlan* plans, const SupJob* jobs,
                                     int nJobs, unsigned long long* results) {
-    const int w = (int)((blockIdx.x * (long long)blockDim.x + threadIdx.x) >> 5);
-    const int lane = threadIdx.x & 31;
-    if (w >= nJobs) return;
-    const SupJob jb = jobs[w];
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nWarps = blockDim.x >> 5;
+    if ((int)blockIdx.x >= nJobs) return;
+    const SupJob jb = jobs[blockIdx.x];
     const DevPlan& P = plans[jb.plan];
     if (!P.gHeavy) return;
     const uint32_t* row = P.gHeavy + (long long)jb.gRow * P.rowWords;
     Meter<false> mt;
     for (int j = 0; j < P.supN; ++j) {
-        unsigned long long n = fused_support(P, ix, j, jb.root, 1, row, 0, 1, lane, mt);
+        unsigned long long n = fused_support(P, ix, j, jb.root, 1, row, 0, 1, lane, warp, nWarps, mt);
         for (int d = 16; d; d >>= 1) n += __shfl_down_sync(0xffffffffu, n, d);
         if (lane == 0 && n) atomicAdd(results + P.supSlot[j], n);
     }
@@ -1295,13 +1350,19 @@ __global__ void support_rows_kernel(const __grid_constant__ DevIndex ix, const D
 cudaError_t support_rows(const DevIndex& ix, const DevPlan* plans, const SupJob* jobs, int nJobs,
                          unsigned long long* results, cudaStream_t stream) {
     if (nJobs <= 0) return cudaSuccess;
-    support_rows_kernel<<<(nJobs + 7) / 8, 256, 0, stream>>>(ix, plans, jobs, nJobs, results);
+    support_rows_kernel<<<nJobs, 256, 0, stream>>>(ix, plans, jobs, nJobs, results);
     return cudaGetLastError();
 }
 
-cudaError_t memo_build(const DevIndex& ix, const MemoJob* jobs, int nJobs, cudaStream_t stream) {
+cudaError_t memo_build(const DevIndex& ix, const MemoJob* jobs, int nJobs, int maxWo, cudaStream_t stream) {
     if (nJobs <= 0) return cudaSuccess;
-    memo_build_kernel<<<nJobs, 256, 0, stream>>>(ix, jobs, nJobs);
+    const size_t smem = (size_t)std::min(maxWo, kMemoSmemRanks) * 4;
+    if (smem > 48 * 1024) {
+        const cudaError_t e =
+            cudaFuncSetAttribute(memo_build_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+        if (e != cudaSuccess) return e;
+    }
+    memo_build_kernel<<<nJobs, 256, smem, stream>>>(ix, jobs, nJobs);
     return cudaGetLastError();
 }
 
