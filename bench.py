@@ -572,7 +572,7 @@ def engine_arm(args):
                          "algorithmic_bytes_per_launch": alg_bytes, "peak_source": peaks["source"] + " (burst copy)"},
             "cpu_baseline": cpu,
             "clocks": clk,
-            "gpu_launches": args.steps,
+            "gpu_launches": args.steps * max(1, info.get("kernels_per_run", 1)),
             "reference_gpu03_per_rule": gpu03,
             "dense_confidence": dense,
             "serving_c5": serving,

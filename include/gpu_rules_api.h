@@ -110,6 +110,12 @@ int gpu_evaluate_rule_shard(void* ctx, const char* ruleText, int shard, int nSha
  * copied device->host per run. */
 int gpu_batch_info(void* batch, long long* plans, long long* tasks, long long* h2dBytes, long long* d2hBytes);
 
+/* Kernels one gpu_batch_run launches on the device (the engine, the fused
+ * support of split heavy roots, the pair sort when staged), or -1 for a
+ * null batch.  No counterpart in the reference (its batch is one kernel
+ * launch per rule phase). */
+int gpu_batch_kernels(void* batch);
+
 /* Runs the batch once with the byte-counting variant of the kernel and
  * returns the global-memory bytes the algorithm requested (the roofline's
  * algorithmic bytes).  Not timed. */

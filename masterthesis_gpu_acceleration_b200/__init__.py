@@ -31,6 +31,7 @@ API_SYMBOLS = (
     "gpu_batch_prepare",
     "gpu_batch_run",
     "gpu_batch_info",
+    "gpu_batch_kernels",
     "gpu_batch_count_bytes",
     "gpu_batch_free",
     "gpu_evaluate_rule_noalloc",
@@ -120,6 +121,8 @@ def load_library(path: os.PathLike | str | None = None) -> ctypes.CDLL:
                                   ctypes.POINTER(ctypes.c_int), ctypes.POINTER(ctypes.c_double)]
     lib.gpu_batch_info.restype = ctypes.c_int
     lib.gpu_batch_info.argtypes = [ctypes.c_void_p] + [ctypes.POINTER(ctypes.c_longlong)] * 4
+    lib.gpu_batch_kernels.restype = ctypes.c_int
+    lib.gpu_batch_kernels.argtypes = [ctypes.c_void_p]
     lib.gpu_batch_count_bytes.restype = ctypes.c_int
     lib.gpu_batch_count_bytes.argtypes = [ctypes.c_void_p, ctypes.POINTER(ctypes.c_ulonglong)]
     lib.gpu_batch_free.restype = None
@@ -346,7 +349,9 @@ class PreparedBatch:
     def info(self) -> dict:
         v = [ctypes.c_longlong() for _ in range(4)]
         self._lib.gpu_batch_info(self._h, *[ctypes.byref(x) for x in v])
-        return dict(zip(("plans", "tasks", "h2d_bytes", "d2h_bytes"), (x.value for x in v)))
+        d = dict(zip(("plans", "tasks", "h2d_bytes", "d2h_bytes"), (x.value for x in v)))
+        d["kernels_per_run"] = int(self._lib.gpu_batch_kernels(self._h))
+        return d
 
     def dedup(self):
         """(modes, sort keys): per rule, how its body size deduplicates pairs

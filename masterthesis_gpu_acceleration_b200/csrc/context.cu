@@ -1190,6 +1190,11 @@ int gpu_batch_info(void* batch, long long* plans, long long* tasks, long long* h
     return 0;
 }
 
+int gpu_batch_kernels(void* batch) {
+    if (!batch) return -1;
+    return static_cast<const Batch*>(batch)->st.kernels_per_enqueue();
+}
+
 int gpu_batch_dedup(void* batch, int* modes, long long* sortKeys) {
     if (!batch || !modes) return -1;
     const Batch& b = *static_cast<const Batch*>(batch);

@@ -176,6 +176,13 @@ struct Staged {
         return nSort > 0 && *static_cast<const unsigned long long*>(hSort.p) > keyCap;
     }
     void restage(Context& c, cudaStream_t s);
+    // Kernels one enqueue() launches: the engine, the fused support of split
+    // roots when there are any, and the pair sort (three kernels per 8-bit
+    // pass and the count) when sort mode is staged.
+    int kernels_per_enqueue() const {
+        if (!nPlans) return 0;
+        return (nTasks > 0 ? 1 : 0) + (nSupJobs > 0 ? 1 : 0) + (nSort ? 3 * ((sortBits + 7) / 8) + 1 : 0);
+    }
     // instr: 0 plain, 1 task times into dTaskNs, 2 also algorithmic bytes
     // into dBytes.  gridCap > 0 limits the launch to that many blocks (a
     // share of the SMs).  budgetNs > 0 (with instr 1): blocks stop that long
