@@ -30,7 +30,8 @@ typedef struct {
     double headCoverage;  /* support / headSize (0 when headSize is 0)         */
     int    bodySize;      /* distinct (hS, hO) pairs with a body grounding     */
     double confidence;    /* support / bodySize (0 when bodySize is 0)         */
-    double supportMs;     /* device time of the support phase (ms)             */
+    double supportMs;     /* device time of the support phase (ms); 0 when the */
+                          /* body-size launch counted the support too          */
     double confidenceMs;  /* device time of the body-size phase (ms)           */
 } GpuRuleResult;
 

@@ -635,8 +635,14 @@ void with_rule_block(Context& c, Fn fn) {
     fn();
 }
 
+// Whether supports may be counted by their body-size plans (fused
+// support, see RulePlan::supFuse): both phases run and no dedup mode is
+// forced.
+bool fusing(const Context& c) { return c.fuseSupport && (c.batchPhases & 3) == 3 && c.dedupForce == 0; }
+
 // Both phases of one rule, each in its own launch timed by its own events,
-// issued back to back with one host synchronisation.
+// issued back to back with one host synchronisation; a fused support takes
+// no launch of its own.
 int evaluate_parsed(Context& c, const Rule& rule, GpuRuleResult* out) {
     RulePlan rp = plan_rule(rule, c.hix, c.geom);
     int64_t sup = rp.support.value, body = rp.body.value;
@@ -645,8 +651,21 @@ int evaluate_parsed(Context& c, const Rule& rule, GpuRuleResult* out) {
     const bool runB = rp.status == kRuleOk && rp.body.how == kDevice;
     std::vector<DevPlan> plans;
     std::vector<const PhasePlan*> phases;
-    if (runS) { plans.push_back(rp.support.plan); phases.push_back(&rp.support); }
+    // fused support (see prepare): the body-size launch also counts the
+    // support, into per-plan result slot 1; the support takes no launch
+    const bool fused = runS && runB && fusing(c) && rp.supFuse >= 0 && rp.body.plan.mode == kPairs &&
+                       !rp.body.needsGlobalBitmap;
+    if (runS && !fused) { plans.push_back(rp.support.plan); phases.push_back(&rp.support); }
     if (runB) { plans.push_back(rp.body.plan); phases.push_back(&rp.body); }
+    if (fused) {
+        DevPlan& B = plans.back();
+        const auto dom = ho_domain(B);
+        B.supN = 1;
+        B.supDomPred = dom.first;
+        B.supDomDir = dom.second;
+        B.supPred[0] = rp.supFuse;
+        B.supSlot[0] = 1;
+    }
     if (!plans.empty()) {
         // one upload, one launch per phase (each timed on the device), one download
         c.one.stage(c, plans, phases, false, c.stream, c.ruleWalkBudget, true);
@@ -660,8 +679,9 @@ int evaluate_parsed(Context& c, const Rule& rule, GpuRuleResult* out) {
         if (static_cast<const int*>(c.one.hCtl.p)[2] != 0)
             throw CudaError("engine reported internal status " + std::to_string(static_cast<const int*>(c.one.hCtl.p)[2]));
         int k = 0;
-        if (runS) { sup = (int64_t)c.one.per_plan_count(k); supMs = (float)c.one.span_ms(k); ++k; }
+        if (runS && !fused) { sup = (int64_t)c.one.per_plan_count(k); supMs = (float)c.one.span_ms(k); ++k; }
         if (runB) { body = (int64_t)c.one.per_plan_count(k); confMs = (float)c.one.span_ms(k); }
+        if (fused) sup = (int64_t)c.one.per_plan_count(1);   // counted by the body-size launch (supportMs 0)
     }
     compose(rp, sup, body, supMs, confMs, out);
     return 0;
@@ -731,7 +751,7 @@ void prepare(Batch& b, Context& c, const char* const* rules, int n, int isJson, 
     // RulePlan::supFuse) gets no support plan when that plan keeps its pair
     // rows in shared memory (no global dedup bitmap, no forced mode); the
     // count lands in a result slot after the plans' own
-    const bool fuse = c.fuseSupport && (c.batchPhases & 3) == 3 && c.dedupForce == 0;
+    const bool fuse = fusing(c);
     b.supOf.assign(n, -1);
     std::vector<std::array<int, 3>> fused;   // {body plan, head predicate, first rule}
     std::unordered_map<uint64_t, int> fusedAt;
