@@ -18,9 +18,9 @@ namespace gr {
 // Worker threads started once per process and reused by every parallel
 // loop: starting threads per loop cost about as much as the preparation of
 // a batch chunk itself.  One loop runs on the pool at a time; a loop that
-// finds it busy (another host thread's loop, or one nested in a loop body)
-// runs on its calling thread alone, as does any loop in a process forked
-// after the pool started.
+// finds it busy with another host thread's loop starts threads of its own,
+// and a loop nested in a pool loop's body, or in a process forked after the
+// pool started, runs on its calling thread alone.
 class HostPool {
 public:
     // Never destroyed: its workers end with the process (a forked child,
@@ -50,6 +50,11 @@ public:
         job_ = nullptr;
         return true;
     }
+    // Whether this process started the pool (not a forked child).
+    bool own_process() const { return ::getpid() == pid_; }
+    // Whether the calling thread is one of the pool's workers.
+    static bool in_worker() { return inWorker(); }
+
 private:
     HostPool() : pid_(::getpid()) {
         const unsigned hw = std::max(1u, std::thread::hardware_concurrency());
@@ -122,7 +127,19 @@ void parallel_for(size_t n, Fn fn, size_t grain = 64, unsigned maxThreads = 16) 
         }
     };
     const std::function<void()> job(work);
-    if (!HostPool::get().run(t, job)) work();
+    if (!HostPool::get().run(t, job)) {
+        if (HostPool::in_worker() || !HostPool::get().own_process()) {
+            work();   // nested in a pool loop's body: the pool's threads are busy with it
+        } else {
+            // the pool runs another host thread's loop (two servers planning
+            // at once, say): this loop starts threads of its own
+            std::vector<std::thread> extra;
+            extra.reserve(t - 1);
+            for (unsigned k = 1; k < t; ++k) extra.emplace_back(work);
+            work();
+            for (auto& th : extra) th.join();
+        }
+    }
     if (err) std::rethrow_exception(err);
 }
 
