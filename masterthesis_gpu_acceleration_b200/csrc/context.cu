@@ -746,7 +746,7 @@ void prepare(Batch& b, Context& c, const char* const* rules, int n, int isJson, 
         } catch (const RuleError&) {
             b.parseStatus[i] = -1;
         }
-    }, 128);
+    }, 16);
     // fused support: a rule whose support its body-size plan can count (see
     // RulePlan::supFuse) gets no support plan when that plan keeps its pair
     // rows in shared memory (no global dedup bitmap, no forced mode); the
@@ -1067,10 +1067,11 @@ int gpu_evaluate_rules_batch(void* ctx, const char* const* rules, int n, int isJ
         cudaSetDevice(c.device);
         // Pipelined: chunk k+1 is parsed, planned and staged on the host
         // while chunk k runs on the device (each chunk on its own stream).
-        // automatic: up to 8 chunks of at least 1,250 rules (c3, 10,000 rules:
-        // 2, 4, 8 and 16 chunks measured 149k, 164k, 169k and 160k rules/s)
+        // automatic: up to 6 chunks of at least 1,667 rules (c3, 10,000 rules:
+        // 1, 2, 4, 6, 8 and 12 chunks measured 53.6, 36.3, 29.0, 27.8, 30.0
+        // and 34.1 ms a call)
         const int K = c.batchChunks > 0 ? std::max(1, std::min(c.batchChunks, std::max(n, 1)))
-                                        : std::max(1, std::min(8, (n + 1249) / 1250));
+                                        : std::max(1, std::min(6, (n + 1666) / 1667));
         while ((int)c.pipe.size() < K) c.pipe.push_back(new Batch());
         const double t0 = host_ms();
         double planMs = 0, stageMs = 0;

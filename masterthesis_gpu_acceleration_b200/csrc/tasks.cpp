@@ -56,50 +56,62 @@ uint64_t phase_hash(const PhasePlan& ph) {
     static_assert(sizeof(DevPlan) % 8 == 0, "plan hashed in 8-byte words");
     const DevPlan p = plan_identity(ph);
     const unsigned char* b = reinterpret_cast<const unsigned char*>(&p);
-    uint64_t h = 0x243F6A8885A308D3ull ^ ((uint64_t)(uint32_t)ph.rootBeg << 32 | (uint32_t)ph.rootEnd);
-    for (size_t i = 0; i < sizeof(DevPlan); i += 8) {
+    // four independent lanes (a quarter of the dependent multiplies each),
+    // combined at the end
+    uint64_t h[4] = {0x243F6A8885A308D3ull ^ ((uint64_t)(uint32_t)ph.rootBeg << 32 | (uint32_t)ph.rootEnd),
+                     0x13198A2E03707344ull, 0xA4093822299F31D0ull, 0x082EFA98EC4E6C89ull};
+    size_t i = 0;
+    for (; i + 32 <= sizeof(DevPlan); i += 32)
+        for (int k = 0; k < 4; ++k) {
+            uint64_t w;
+            std::memcpy(&w, b + i + 8 * k, 8);
+            h[k] = (h[k] ^ w) * 0x9E3779B97F4A7C15ull;
+            h[k] ^= h[k] >> 29;
+        }
+    for (int k = 0; i < sizeof(DevPlan); i += 8, ++k) {
         uint64_t w;
         std::memcpy(&w, b + i, 8);
-        h = (h ^ w) * 0x9E3779B97F4A7C15ull;
-        h ^= h >> 29;
+        h[k] = (h[k] ^ w) * 0x9E3779B97F4A7C15ull;
+        h[k] ^= h[k] >> 29;
     }
-    h ^= h >> 32;
-    h *= 0xD6E8FEB86659FD93ull;
-    return h ^ (h >> 32);
+    uint64_t r = h[0];
+    for (int k = 1; k < 4; ++k) {
+        r = (r ^ h[k]) * 0xD6E8FEB86659FD93ull;
+        r ^= r >> 32;
+    }
+    return r;
+}
+
+TaskBuilder::TaskBuilder(const HostIndex& ix)
+    : ix_(ix), degAt_((size_t)std::max(ix.nPred, 0) * 2), sbFan_((size_t)std::max(ix.nPred, 0) * 2, 0.0),
+      hop2_(new Hop2Shard[kHop2Shards]) {
+    for (auto& a : degAt_) a.store(nullptr, std::memory_order_relaxed);
+    for (int32_t p = 0; p < ix.nPred; ++p)
+        for (int dir = 0; dir < 2; ++dir) {
+            double s1 = 0, s2 = 0;
+            for (int32_t r = ix.predRow[dir][p]; r < ix.predRow[dir][p + 1]; ++r) {
+                const double d = ix.rowBeg[dir][r + 1] - ix.rowBeg[dir][r];
+                s1 += d;
+                s2 += d * d;
+            }
+            sbFan_[(size_t)p * 2 + dir] = s1 > 0 ? s2 / s1 : 0.0;
+        }
 }
 
 const int32_t* TaskBuilder::degrees(int32_t pred, int dir) {
-    {
-        std::shared_lock<std::shared_mutex> lk(cacheMu_);
-        auto it = deg_.find(pd_key(pred, dir));
-        if (it != deg_.end()) return it->second.data();
-    }
+    const size_t at = (size_t)pred * 2 + (size_t)dir;
+    if (const int32_t* d = degAt_[at].load(std::memory_order_acquire)) return d;
     std::vector<int32_t> d((size_t)std::max(ix_.nEnt, 1), 0);
     for (int32_t r = ix_.predRow[dir][pred]; r < ix_.predRow[dir][pred + 1]; ++r)
         d[ix_.rowKey[dir][r]] = ix_.rowBeg[dir][r + 1] - ix_.rowBeg[dir][r];
     std::unique_lock<std::shared_mutex> lk(cacheMu_);
     auto ins = deg_.emplace(pd_key(pred, dir), std::move(d));
     if (ins.second) cacheBytes_ += ins.first->second.size() * 4;
+    degAt_[at].store(ins.first->second.data(), std::memory_order_release);
     return ins.first->second.data();
 }
 
-double TaskBuilder::sb_fan(int32_t pred, int dir) {
-    {
-        std::shared_lock<std::shared_mutex> lk(cacheMu_);
-        auto it = sbFan_.find(pd_key(pred, dir));
-        if (it != sbFan_.end()) return it->second;
-    }
-    double s1 = 0, s2 = 0;
-    for (int32_t r = ix_.predRow[dir][pred]; r < ix_.predRow[dir][pred + 1]; ++r) {
-        double d = ix_.rowBeg[dir][r + 1] - ix_.rowBeg[dir][r];
-        s1 += d;
-        s2 += d * d;
-    }
-    double v = s1 > 0 ? s2 / s1 : 0.0;
-    std::unique_lock<std::shared_mutex> lk(cacheMu_);
-    sbFan_.emplace(pd_key(pred, dir), v);
-    return v;
-}
+double TaskBuilder::sb_fan(int32_t pred, int dir) { return sbFan_[(size_t)pred * 2 + (size_t)dir]; }
 
 double TaskBuilder::avg_fan(const DevStep& st) const {
     if (st.kind == kScan) return (double)ix_.pred_size(st.pred);
@@ -121,10 +133,11 @@ double TaskBuilder::estimate(const PhasePlan& ph, bool hubAware) {
 
 const TaskBuilder::Hop2& TaskBuilder::hop2(int32_t p0, int d0, int32_t p1, int d1) {
     const uint64_t key = ((uint64_t)(uint32_t)p0 << 33) | ((uint64_t)d0 << 32) | ((uint64_t)(uint32_t)p1 << 1) | (uint64_t)d1;
+    Hop2Shard& sh = hop2_[(key * 0x9E3779B97F4A7C15ull) >> 58];
     {
-        std::shared_lock<std::shared_mutex> lk(cacheMu_);
-        auto it = hop2_.find(key);
-        if (it != hop2_.end()) return it->second;
+        std::shared_lock<std::shared_mutex> lk(sh.mu);
+        auto it = sh.map.find(key);
+        if (it != sh.map.end()) return it->second;
     }
     const int32_t* deg = degrees(p1, d1);
     Hop2 h;
@@ -136,8 +149,8 @@ const TaskBuilder::Hop2& TaskBuilder::hop2(int32_t p0, int d0, int32_t p1, int d
         h.perRow[r - r0] = (float)acc;
         h.total += acc;
     }
-    std::unique_lock<std::shared_mutex> lk(cacheMu_);
-    auto ins = hop2_.emplace(key, std::move(h));
+    std::unique_lock<std::shared_mutex> lk(sh.mu);
+    auto ins = sh.map.emplace(key, std::move(h));
     if (ins.second) cacheBytes_ += ins.first->second.perRow.size() * sizeof(float);
     return ins.first->second;
 }
@@ -294,7 +307,8 @@ void TaskBuilder::build(const std::vector<const PhasePlan*>& phases, int blocks,
     if (cacheBytes_ > kCacheLimit) {  // only here: walks hand out references into the cache
         walks_.clear();
         deg_.clear();
-        hop2_.clear();
+        for (auto& a : degAt_) a.store(nullptr, std::memory_order_relaxed);
+        for (int k = 0; k < kHop2Shards; ++k) hop2_[k].map.clear();
         cacheBytes_ = 0;
     }
     std::vector<double> estAvg(n), estHub(n), scale(n, defaultCalib_);
@@ -316,7 +330,7 @@ void TaskBuilder::build(const std::vector<const PhasePlan*>& phases, int blocks,
             forced[i] = mustWalk_.count(sig[i]) ? 1 : 0;
         }
         if (split) cached[i] = walks_.count(sig[i]) ? 1 : 0;
-    }, 128);
+    }, 16);
     if (split) {
         std::vector<size_t> ord(n);
         std::iota(ord.begin(), ord.end(), 0);
@@ -473,7 +487,7 @@ void TaskBuilder::build(const std::vector<const PhasePlan*>& phases, int blocks,
             accUnits += wu;
         }
         flush(ph.rootEnd);
-    });
+    }, 8);
 }
 
 std::vector<int32_t> TaskBuilder::split_roots(const PhasePlan& ph, int n) {

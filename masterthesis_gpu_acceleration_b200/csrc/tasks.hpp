@@ -1,6 +1,8 @@
 // tasks.hpp — splitting device phases into balanced tasks (the autotuner).
 #pragma once
+#include <atomic>
 #include <cstdint>
+#include <memory>
 #include <functional>
 #include <shared_mutex>
 #include <string>
@@ -52,7 +54,7 @@ uint64_t phase_hash(const PhasePlan& ph);
 
 class TaskBuilder {
 public:
-    explicit TaskBuilder(const HostIndex& ix) : ix_(ix) {}
+    explicit TaskBuilder(const HostIndex& ix);
 
     // phases[i] is planned as plan number i.  blocks: resident blocks of the
     // launch.  split=false keeps every root in shared-memory tasks.
@@ -116,7 +118,10 @@ public:
 private:
     const HostIndex& ix_;
     std::unordered_map<int64_t, std::vector<int32_t>> deg_;      // (pred, dir) -> degree by entity
-    std::unordered_map<int64_t, double> sbFan_;                  // (pred, dir) -> size-biased fan-out
+    // per pred * 2 + dir: deg_'s array once built (read without a lock), and
+    // the size-biased fan-out (computed once, at construction)
+    std::vector<std::atomic<const int32_t*>> degAt_;
+    std::vector<double> sbFan_;
     // Per-root work, and its sum and maximum over blocks of kWalkBlock
     // roots, so that task building steps over runs of light roots a block
     // at a time.
@@ -132,14 +137,21 @@ private:
         std::vector<float> perRow;   // per row of (p0, d0): sum over its edges of the next degree
         double total = 0.0;
     };
-    std::unordered_map<uint64_t, Hop2> hop2_;                    // (p0, d0, p1, d1) -> two-hop sums
+    // (p0, d0, p1, d1) -> two-hop sums, in shards with a lock each, so that
+    // the threads estimating a batch's phases do not all take one lock
+    static constexpr int kHop2Shards = 64;
+    struct Hop2Shard {
+        std::shared_mutex mu;
+        std::unordered_map<uint64_t, Hop2> map;
+    };
+    std::unique_ptr<Hop2Shard[]> hop2_;
     std::unordered_map<uint64_t, double> calib_;                // phase hash -> ns per work unit
     std::unordered_map<uint64_t, bool> mustWalk_;               // phase hash -> walk next time
     double defaultCalib_ = 1.0;
-    size_t cacheBytes_ = 0;
-    // guards deg_, sbFan_, hop2_ and cacheBytes_ while the estimates of a
-    // build run on several threads (entries are never erased during a build,
-    // so references handed out stay valid)
+    std::atomic<size_t> cacheBytes_{0};
+    // guards deg_ while the estimates of a build run on several threads
+    // (entries are never erased during a build, so references handed out
+    // stay valid)
     mutable std::shared_mutex cacheMu_;
 
     double sb_fan(int32_t pred, int dir);
