@@ -1104,6 +1104,13 @@ int gpu_evaluate_rules_batch(void* ctx, const char* const* rules, int n, int isJ
             float ms = 0.f;
             ck(cudaEventElapsedTime(&ms, c.pipe[0]->ev0, b.ev1), "elapsed");
             span = std::max(span, ms);
+            if (c.hostProfile) {
+                float own = 0.f, at = 0.f;
+                ck(cudaEventElapsedTime(&own, b.ev0, b.ev1), "elapsed");
+                ck(cudaEventElapsedTime(&at, c.pipe[0]->ev0, b.ev0), "elapsed");
+                std::fprintf(stderr, "[gpu_rules]   chunk %d: %d rules, %d tasks, enqueued at %.2f ms, %.2f ms on the device\n",
+                             k, b.n, b.st.nTasks, (double)at, (double)own);
+            }
             const int lo = (int)((long long)n * k / K);
             collect(b, out + lo, status ? status + lo : nullptr);
         }

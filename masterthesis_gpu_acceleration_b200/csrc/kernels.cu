@@ -995,7 +995,10 @@ __device__ __forceinline__ void run_task(Smem<B>& sm, const DevIndex& ix, const 
                 const int lane = tid & 31, warp = tid >> 5;
                 constexpr int kWarps = B / 32;
                 const int words = P.rowWords;
-                const bool perWarp = !leaf || words <= 128;   // memo items and small domains: one warp per item
+                // memo items and domains up to 1,024 words: one warp per item
+                // (a round's hub items in parallel); larger rows: the whole
+                // block on each item in turn
+                const bool perWarp = !leaf || words <= 1024;
                 const int nEx = lenK - kTupleHead;
                 const int exDir = 1 - stp.dir;
                 int ordinal = 0;

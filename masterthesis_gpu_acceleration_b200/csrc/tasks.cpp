@@ -353,7 +353,7 @@ void TaskBuilder::build(const std::vector<const PhasePlan*>& phases, int blocks,
             if (!forced[i] && !cached[i] && used + edges > walkBudget) continue;
             // a walk whose own cost exceeds the phase's expected device time
             // cannot pay for itself (a single rule on the whole GPU)
-            if (costAware && !cached[i] && estAvg[i] * scale[i] < kWalkNsPerEdge * edges) continue;
+            if (costAware && !cached[i] && std::max(estAvg[i], estHub[i]) * scale[i] < kWalkNsPerEdge * edges) continue;
             if (!cached[i]) used += edges;   // cached walks cost nothing
             sel.push_back(i);
         }
