@@ -91,6 +91,36 @@ class GpuServeResult(ctypes.Structure):
 _lib = None
 
 
+def _c_strings(texts: Sequence[str]):
+    """A char*[] over texts: one encoded buffer of NUL-terminated strings and
+    its pointer array, built without a Python object per string.  Returns
+    (what must stay alive during the call, the pointer array)."""
+    import numpy as np
+    n = len(texts)
+    if n == 0:
+        return None, (ctypes.c_char_p * 1)()
+    joined = "\0".join(texts) + "\0"
+    buf = joined.encode()
+    lens = np.fromiter(map(len, texts), dtype=np.int64, count=n)
+    if joined.count("\0") != n:
+        ends = None
+    elif len(buf) == len(joined):   # one byte per character: string ends follow from the lengths
+        ends = np.cumsum(lens + 1) - 1
+    else:
+        ends = np.flatnonzero(np.frombuffer(buf, dtype=np.uint8) == 0)
+        if len(ends) != n:
+            ends = None
+    if ends is None:   # a text holds a NUL: one object per string
+        arr = (ctypes.c_char_p * n)(*[t.encode() for t in texts])
+        return arr, arr
+    cbuf = ctypes.create_string_buffer(buf, len(buf))
+    ptrs = np.empty(n, dtype=np.uint64)
+    ptrs[0] = 0
+    ptrs[1:] = (ends[:-1] + 1).astype(np.uint64)
+    ptrs += np.uint64(ctypes.addressof(cbuf))
+    return (cbuf, ptrs), ptrs.ctypes.data_as(ctypes.POINTER(ctypes.c_char_p))
+
+
 def load_library(path: os.PathLike | str | None = None) -> ctypes.CDLL:
     """Loads libgpu_rules.so (built in-tree); raises if it is missing."""
     global _lib
@@ -218,17 +248,21 @@ class GpuRulesLib:
 
     # -- additive entry points ---------------------------------------------------
     def evaluate_rules_batch(self, rules: Sequence[str], is_json: bool = False):
-        """Returns (results, statuses, device_ms) for all rules in one launch."""
+        """Returns (results, statuses, device_ms) for all rules in one launch.
+
+        results is a ctypes array of n GpuRuleResult (indexable, iterable,
+        sliceable), statuses a list of n ints."""
         n = len(rules)
-        arr = (ctypes.c_char_p * max(n, 1))(*[r.encode() for r in rules])
+        keep, arr = _c_strings(rules)
         out = (GpuRuleResult * max(n, 1))()
         st = (ctypes.c_int * max(n, 1))()
         ms = ctypes.c_double()
         rc = self._lib.gpu_evaluate_rules_batch(self._handle(), arr, n, int(is_json), out, st, ctypes.byref(ms))
+        del keep
         if rc != 0:
             raise RuntimeError(f"gpu_evaluate_rules_batch failed "
                                f"({self._lib.gpu_last_error().decode(errors='replace')})")
-        return list(out)[:n], list(st)[:n], ms.value
+        return (out if n else []), st[:n], ms.value
 
     def evaluate_rule_noalloc(self, rule_text: str) -> GpuRuleResult:
         """gpu_evaluate_rule without any device allocation (fixed in-library
