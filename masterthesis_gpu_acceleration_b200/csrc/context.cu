@@ -67,6 +67,7 @@ void Staged::stage(Context& c, std::vector<DevPlan>& plans, const std::vector<co
                    bool sortTasks, cudaStream_t s, double walkBudget, bool costAware, bool allowSort) {
     nPlans = (int)plans.size();
     nResults = nPlans + extraResults;
+    stagedBlock = c.geom.block;
     nTasks = 0;
     bitmapWords = 0;
     blockWords = blockRegions = 0;
@@ -513,9 +514,20 @@ void Staged::restage(Context& c, cudaStream_t s) {
     stage(c, p, ph, inSortTasks, s, inWalk, inCostAware, inAllowSort);
 }
 
+void Staged::check_geometry(const Context& c) const {
+    // plans are laid out for the shared pool of the block size they were
+    // staged at; a larger block's pool starts with it, a smaller one's is
+    // too short (and its larger grid would outrun the per-block tables)
+    if (c.geom.block < stagedBlock)
+        throw CudaError("the launch's block size (" + std::to_string(c.geom.block) +
+                        " threads) is below the one the plans were staged for (" + std::to_string(stagedBlock) +
+                        "); prepare the batch again after changing the block size");
+}
+
 void Staged::enqueue(Context& c, cudaStream_t s, int instr, int gridCap, unsigned long long budgetNs) {
     budgeted = false;
     if (!nPlans) return;
+    check_geometry(c);
     ck(cudaMemsetAsync(dResults.p, 0, (size_t)nResults * sizeof(unsigned long long), s), "memset results");
     ck(cudaMemsetAsync(dCtl.p, 0, 8, s), "memset ctl");
     if (bitmapWords) ck(cudaMemsetAsync(dBitmap.p, 0, bitmapWords * 4, s), "memset bitmap");
@@ -552,6 +564,7 @@ void Staged::enqueue(Context& c, cudaStream_t s, int instr, int gridCap, unsigne
 
 void Staged::enqueue_per_plan(Context& c, cudaStream_t s) {
     if (!nPlans) return;
+    check_geometry(c);
     if (nPlans > kMaxPerPlan || (int)planTaskEnd.size() != nPlans) throw CudaError("bad per-plan staging");
     // control words: [0..1] task counters, [2] status (int), per plan two
     // u64 span words at byte 16 + 16 * i and its u64 result at

@@ -188,6 +188,9 @@ struct Staged {
     // share of the SMs).  budgetNs > 0 (with instr 1): blocks stop that long
     // after they start, and plan_incomplete() tells which plans lost work.
     void enqueue(Context& c, cudaStream_t s, int instr, int gridCap = 0, unsigned long long budgetNs = 0);
+    int stagedBlock = 0;   // block size whose shared pool the staged plans are laid out for
+    // Throws when the context's block size is below stagedBlock.
+    void check_geometry(const Context& c) const;
     bool plan_incomplete(int i) const {
         return budgeted && static_cast<const int*>(hIncomplete.p)[i] != 0;
     }

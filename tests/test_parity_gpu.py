@@ -228,3 +228,29 @@ def test_graph_file_loads_identically(name, tmp_path):
     (tmp_path / "cut.bin").write_bytes(f.read_bytes()[:1000])
     with pytest.raises(RuntimeError):
         eng.GpuRulesLib(index_path=tmp_path / "cut.bin")
+
+
+def test_batch_refuses_a_smaller_block_than_staged(tmp_path):
+    """Plans are laid out for the shared pool of the block size they were
+    staged at.  After the block size is lowered, a prepared batch replays
+    its captured launch unchanged (same counts), while a launch issued anew
+    (the instrumented run of profile()) is refused with an error; at the
+    staged size it works again."""
+    fx = load_fixture("fuzz_0.json")
+    p = tmp_path / "graph.ttl"
+    p.write_text(fx["ttl"])
+    with eng.GpuRulesLib(p) as lib:
+        lib.set_option("block", 256)
+        b = lib.prepare_batch(fx["rules"])
+        b.run()
+        want = b.counts().copy()
+        lib.set_option("block", 128)
+        b.run()
+        assert (b.counts() == want).all()
+        with pytest.raises(RuntimeError):
+            b.profile()
+        lib.set_option("block", 256)
+        b.profile()
+        b.run()
+        assert (b.counts() == want).all()
+        b.close()
