@@ -38,11 +38,13 @@ public:
         if (!region.owns_lock()) return false;
         const unsigned helpers = std::min<unsigned>(n > 0 ? n - 1 : 0, nWorkers_);
         job_ = &work;
-        want_ = helpers;
         pending_.store(helpers, std::memory_order_relaxed);
         {
+            // generation and helper count in one word: a worker that sees a
+            // generation late reads the count of that same generation
             std::lock_guard<std::mutex> lk(mu_);   // a sleeping worker sees the new generation
-            gen_.fetch_add(1, std::memory_order_release);
+            const uint64_t g = (ctl_.load(std::memory_order_relaxed) >> 8) + 1;
+            ctl_.store((g << 8) | helpers, std::memory_order_release);
         }
         cv_.notify_all();
         work();
@@ -72,18 +74,20 @@ private:
         inWorker() = true;
         uint64_t seen = 0;   // the generation when the pool started (a loop may come before this thread runs)
         for (;;) {
-            uint64_t g = gen_.load(std::memory_order_acquire);
-            for (int spin = 0; g == seen && spin < 20000; ++spin) {
+            uint64_t c = ctl_.load(std::memory_order_acquire);
+            for (int spin = 0; (c >> 8) == seen && spin < 4000; ++spin) {
                 std::this_thread::yield();
-                g = gen_.load(std::memory_order_acquire);
+                c = ctl_.load(std::memory_order_acquire);
             }
-            if (g == seen) {
+            if ((c >> 8) == seen) {
                 std::unique_lock<std::mutex> lk(mu_);
-                cv_.wait(lk, [&] { return gen_.load(std::memory_order_acquire) != seen; });
-                g = gen_.load(std::memory_order_acquire);
+                cv_.wait(lk, [&] { return (ctl_.load(std::memory_order_acquire) >> 8) != seen; });
+                c = ctl_.load(std::memory_order_acquire);
             }
-            seen = g;
-            if (idx >= want_) continue;
+            seen = c >> 8;
+            // a helper of this generation: the caller waits for it, so job_
+            // still holds this generation's loop
+            if (idx >= (unsigned)(c & 0xffu)) continue;
             (*job_)();
             pending_.fetch_sub(1, std::memory_order_acq_rel);
         }
@@ -91,10 +95,9 @@ private:
     unsigned nWorkers_ = 0;
     std::mutex mu_, regionMu_;
     std::condition_variable cv_;
-    const std::function<void()>* job_ = nullptr;   // written before gen_ is raised
-    unsigned want_ = 0;
+    const std::function<void()>* job_ = nullptr;   // written before ctl_ is raised
     std::atomic<unsigned> pending_{0};
-    std::atomic<uint64_t> gen_{0};
+    std::atomic<uint64_t> ctl_{0};   // generation << 8 | helpers wanted (at most 63)
     const pid_t pid_;
 };
 
