@@ -33,9 +33,13 @@ public:
     // returns when all have returned; false (nothing run) when the pool is
     // busy or belongs to another process.
     bool run(unsigned n, const std::function<void()>& work) {
-        if (inWorker() || ::getpid() != pid_) return false;
+        if (inWorker() || inRegion() || ::getpid() != pid_) return false;
         std::unique_lock<std::mutex> region(regionMu_, std::try_to_lock);
         if (!region.owns_lock()) return false;
+        struct Mark {   // loops nested in this one's body, on this thread, do not touch the lock
+            Mark() { inRegion() = true; }
+            ~Mark() { inRegion() = false; }
+        } mark;
         const unsigned helpers = std::min<unsigned>(n > 0 ? n - 1 : 0, nWorkers_);
         job_ = &work;
         pending_.store(helpers, std::memory_order_relaxed);
@@ -54,8 +58,9 @@ public:
     }
     // Whether this process started the pool (not a forked child).
     bool own_process() const { return ::getpid() == pid_; }
-    // Whether the calling thread is one of the pool's workers.
-    static bool in_worker() { return inWorker(); }
+    // Whether the calling thread is one of the pool's workers, or runs a
+    // pool loop's body on the calling side.
+    static bool in_worker() { return inWorker() || inRegion(); }
 
 private:
     HostPool() : pid_(::getpid()) {
@@ -66,6 +71,10 @@ private:
     static bool& inWorker() {
         static thread_local bool w = false;
         return w;
+    }
+    static bool& inRegion() {
+        static thread_local bool r = false;
+        return r;
     }
     // After each loop a worker polls for the next one for a while (the
     // loops of one batch come a few hundred microseconds apart), then
