@@ -78,27 +78,31 @@ int check_dir(const HostIndex& ix, int32_t p) {
 bool build_steps(Builder& b, const std::vector<Atom>& body, const Atom* head, int32_t hO, bool pairs) {
     DevPlan& P = b.P;
     const HostIndex& ix = b.ix;
-    int nb = (int)body.size();
-    std::vector<int> level(nb, -1);
-    std::vector<int> order;
-    std::vector<std::vector<DevCheck>> checks(kMaxBody + 1);
+    const int nb = (int)body.size();   // at most kMaxBody (plan_rule checks)
+    // fixed-size bookkeeping (no allocation per plan): levels and order of
+    // the atoms, and the checks in the order they were found
+    int level[kMaxBody], order[kMaxBody], nOrder = 0;
+    for (int i = 0; i < nb; ++i) level[i] = -1;
+    struct LevelCheck { int lvl; DevCheck c; };
+    LevelCheck found[kMaxBody];
+    int nFound = 0;
     auto add_checks = [&](int lvl) {
         for (int i = 0; i < nb; ++i) {
             if (level[i] >= 0 || !b.bound(body[i].s) || !b.bound(body[i].o)) continue;
             level[i] = lvl;
-            order.push_back(i);
+            order[nOrder++] = i;
             DevCheck c{};
             c.pred = body[i].pred;
             c.s = b.ref(body[i].s);
             c.o = b.ref(body[i].o);
             c.dir = (int8_t)check_dir(ix, body[i].pred);
-            checks[lvl].push_back(c);
+            found[nFound++] = LevelCheck{lvl, c};
         }
     };
     P.tupleLen[0] = b.tupleLen;
     add_checks(0);
     int lvl = 0;
-    while ((int)order.size() < nb) {
+    while (nOrder < nb) {
         int best = -1, bestDir = 0;
         double bestFan = std::numeric_limits<double>::infinity();
         for (int i = 0; i < nb; ++i) {
@@ -146,44 +150,52 @@ bool build_steps(Builder& b, const std::vector<Atom>& body, const Atom* head, in
             }
         }
         level[best] = lvl;
-        order.push_back(best);
+        order[nOrder++] = best;
         P.tupleLen[lvl] = b.tupleLen;
         add_checks(lvl);
     }
     P.m = lvl;
 
     // used-triple comparisons, attached where the later atom is grounded
-    std::vector<std::vector<DevUsed>> used(kMaxBody + 1);
-    std::vector<const Atom*> seq;
-    std::vector<int> seqLevel;
-    if (head) { seq.push_back(head); seqLevel.push_back(0); }
-    for (int i : order) { seq.push_back(&body[i]); seqLevel.push_back(level[i]); }
-    for (size_t j = 0; j < seq.size(); ++j) {
-        for (size_t i = 0; i < j; ++i) {
+    const Atom* seq[kMaxBody + 1];
+    int seqLevel[kMaxBody + 1], nSeq = 0;
+    if (head) { seq[nSeq] = head; seqLevel[nSeq++] = 0; }
+    for (int k = 0; k < nOrder; ++k) { seq[nSeq] = &body[order[k]]; seqLevel[nSeq++] = level[order[k]]; }
+    struct LevelUsed { int lvl; DevUsed u; };
+    LevelUsed pairs_[(kMaxBody + 1) * kMaxBody / 2];
+    int nPairs = 0;
+    for (int j = 0; j < nSeq; ++j) {
+        for (int i = 0; i < j; ++i) {
             const Atom& A = *seq[i];
             const Atom& B = *seq[j];
             if (A.pred != B.pred) continue;
             Rel rs = rel(A.s, B.s), ro = rel(A.o, B.o);
             if (rs == kNe || ro == kNe) continue;
             if (rs == kEq && ro == kEq) return false;
-            DevUsed u{b.ref(A.s), b.ref(A.o), b.ref(B.s), b.ref(B.o)};
-            used[seqLevel[j]].push_back(u);
+            pairs_[nPairs++] = LevelUsed{seqLevel[j], DevUsed{b.ref(A.s), b.ref(A.o), b.ref(B.s), b.ref(B.o)}};
         }
     }
+    // per level, in the order found
     int nc = 0, nu = 0;
     for (int l = 0; l <= kMaxBody; ++l) {
         P.chkBeg[l] = (int8_t)nc;
-        P.chkN[l] = (int8_t)checks[l].size();
-        for (auto& c : checks[l]) {
-            if (nc >= kMaxChecks) { b.ok = false; break; }
-            P.checks[nc++] = c;
+        int cnt = 0;
+        for (int k = 0; k < nFound; ++k) {
+            if (found[k].lvl != l) continue;
+            ++cnt;
+            if (nc >= kMaxChecks) { b.ok = false; continue; }
+            P.checks[nc++] = found[k].c;
         }
+        P.chkN[l] = (int8_t)cnt;
         P.usedBeg[l] = (int8_t)nu;
-        P.usedN[l] = (int8_t)used[l].size();
-        for (auto& u : used[l]) {
-            if (nu >= kMaxUsed) { b.ok = false; break; }
-            P.used[nu++] = u;
+        cnt = 0;
+        for (int k = 0; k < nPairs; ++k) {
+            if (pairs_[k].lvl != l) continue;
+            ++cnt;
+            if (nu >= kMaxUsed) { b.ok = false; continue; }
+            P.used[nu++] = pairs_[k].u;
         }
+        P.usedN[l] = (int8_t)cnt;
     }
     return true;
 }

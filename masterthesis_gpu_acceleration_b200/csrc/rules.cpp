@@ -6,7 +6,7 @@
 namespace gr {
 namespace {
 
-std::string trim(const std::string& s) {
+std::string_view trim(std::string_view s) {
     size_t b = 0, e = s.size();
     while (b < e && std::isspace((unsigned char)s[b])) ++b;
     while (e > b && std::isspace((unsigned char)s[e - 1])) --e;
@@ -17,36 +17,37 @@ std::string trim(const std::string& s) {
 // `istringstream(s) >> a >> b >> c` reads them (RuleParser.cpp reads an atom
 // that way): leading whitespace skipped, missing tokens left empty, anything
 // after the third ignored.
-void three_tokens(const std::string& s, std::string& a, std::string& b, std::string& c) {
-    std::string* out[3] = {&a, &b, &c};
+void three_tokens(std::string_view s, std::string_view& a, std::string_view& b, std::string_view& c) {
+    std::string_view* out[3] = {&a, &b, &c};
     size_t i = 0;
     const size_t n = s.size();
-    for (std::string* t : out) {
+    for (std::string_view* t : out) {
         while (i < n && std::isspace((unsigned char)s[i])) ++i;
         size_t j = i;
         while (j < n && !std::isspace((unsigned char)s[j])) ++j;
-        t->assign(s, i, j - i);
+        *t = s.substr(i, j - i);
         i = j;
     }
 }
 
-// Splits the body on '^' outside parentheses (RuleParser.cpp:155-184).
-std::vector<std::string> split_atoms(const std::string& body) {
-    std::vector<std::string> out;
-    std::string cur;
+// Calls fn(atom) for the body's atoms: split on '^' outside parentheses,
+// trimmed, empty ones skipped (RuleParser.cpp:155-184).
+template <class Fn>
+void for_atoms(std::string_view body, Fn fn) {
     int depth = 0;
-    for (char ch : body) {
-        if (ch == '(') { ++depth; cur.push_back(ch); }
-        else if (ch == ')') { --depth; cur.push_back(ch); }
+    size_t start = 0;
+    for (size_t i = 0; i < body.size(); ++i) {
+        const char ch = body[i];
+        if (ch == '(') ++depth;
+        else if (ch == ')') --depth;
         else if (ch == '^' && depth == 0) {
-            std::string t = trim(cur);
-            if (!t.empty()) out.push_back(t);
-            cur.clear();
-        } else cur.push_back(ch);
+            const std::string_view t = trim(body.substr(start, i - start));
+            if (!t.empty()) fn(t);
+            start = i + 1;
+        }
     }
-    std::string t = trim(cur);
-    if (!t.empty()) out.push_back(t);
-    return out;
+    const std::string_view t = trim(body.substr(start));
+    if (!t.empty()) fn(t);
 }
 
 // "key": "value" lookup without escape handling (RuleParser.cpp:10-21).
@@ -88,24 +89,33 @@ std::vector<std::string> json_objects(const std::string& arr) {
 
 }  // namespace
 
-std::string RuleParser::expand(const std::string& token) const {
-    if (token.empty()) return token;
-    if (token.front() == '<' && token.back() == '>') return token.substr(1, token.size() - 2);
-    if (token.front() == '?' || token.front() == '"') return token;
-    size_t c = token.find(':');
-    if (c == std::string::npos) return token;
-    auto it = prefixes_.find(token.substr(0, c));
-    if (it != prefixes_.end()) return it->second + token.substr(c + 1);
-    return token;
+void RuleParser::expand(std::string_view token, std::string& out) const {
+    if (token.size() >= 2 && token.front() == '<' && token.back() == '>') {
+        out.assign(token.substr(1, token.size() - 2));
+        return;
+    }
+    if (!token.empty() && token.front() != '?' && token.front() != '"') {
+        const size_t c = token.find(':');
+        if (c != std::string_view::npos) {
+            out.assign(token.substr(0, c));
+            auto it = prefixes_.find(out);
+            if (it != prefixes_.end()) {
+                out = it->second;
+                out.append(token.substr(c + 1));
+                return;
+            }
+        }
+    }
+    out.assign(token);
 }
 
-Term RuleParser::var_term(const std::string& name, Scope& sc) const {
+Term RuleParser::var_term(std::string_view name, Scope& sc) const {
     Term t;
     t.isVar = true;
     for (const auto& v : sc.vars)
-        if (v.first == name) { t.id = v.second; return t; }
+        if (std::string_view(v.first) == name) { t.id = v.second; return t; }
     t.id = sc.nextVar++;
-    sc.vars.emplace_back(name, t.id);
+    sc.vars.emplace_back(std::string(name), t.id);
     return t;
 }
 
@@ -121,41 +131,47 @@ Term RuleParser::const_term(const std::string& spelled, Scope& sc) const {
     return t;
 }
 
-Term RuleParser::text_term(const std::string& token, Scope& sc) const {
-    std::string c = trim(token);
+Term RuleParser::text_term(std::string_view token, Scope& sc) const {
+    const std::string_view c = trim(token);
     if (c.empty()) throw RuleError("Empty term token");
     if (c.front() == '?') return var_term(c, sc);
-    return const_term(expand(c), sc);
+    static thread_local std::string key;   // reused: no allocation per term once grown
+    expand(c, key);
+    return const_term(key, sc);
 }
 
-int32_t RuleParser::pred_id(const std::string& token) const {
-    return preds_.find(expand(token));
+int32_t RuleParser::pred_id(std::string_view token) const {
+    static thread_local std::string key;
+    expand(token, key);
+    return preds_.find(key);
 }
 
 Rule RuleParser::parse_text(const std::string& line) const {
-    std::string clean = trim(line);
+    std::string_view clean = trim(line);
     if (clean.empty()) throw RuleError("Empty rule line");
-    size_t bar = clean.find('|');
-    if (bar != std::string::npos) clean = trim(clean.substr(0, bar));
-    size_t arrow = clean.find("=>");
-    if (arrow == std::string::npos) throw RuleError("Rule line missing => : " + line);
-    std::string bodyText = trim(clean.substr(0, arrow));
-    std::string headText = trim(clean.substr(arrow + 2));
+    const size_t bar = clean.find('|');
+    if (bar != std::string_view::npos) clean = trim(clean.substr(0, bar));
+    const size_t arrow = clean.find("=>");
+    if (arrow == std::string_view::npos) throw RuleError("Rule line missing => : " + line);
+    const std::string_view bodyText = trim(clean.substr(0, arrow));
+    const std::string_view headText = trim(clean.substr(arrow + 2));
     Scope sc;
     Rule r;
-    auto atom_of = [&](const std::string& raw, const char* what) {
-        std::string s = trim(raw);
-        if (s.empty() || s.front() != '(' || s.back() != ')') throw RuleError(std::string("Invalid ") + what + ": " + raw);
-        std::string st, pt, ot;
+    auto atom_of = [&](std::string_view raw, const char* what) {
+        const std::string_view s = trim(raw);
+        if (s.empty() || s.front() != '(' || s.back() != ')')
+            throw RuleError(std::string("Invalid ") + what + ": " + std::string(raw));
+        std::string_view st, pt, ot;
         three_tokens(s.substr(1, s.size() - 2), st, pt, ot);
-        if (st.empty() || pt.empty() || ot.empty()) throw RuleError(std::string("Invalid ") + what + ": " + raw);
+        if (st.empty() || pt.empty() || ot.empty())
+            throw RuleError(std::string("Invalid ") + what + ": " + std::string(raw));
         Atom a;
         a.s = text_term(st, sc);
         a.o = text_term(ot, sc);
         a.pred = pred_id(pt);
         return a;
     };
-    for (const auto& a : split_atoms(bodyText)) r.body.push_back(atom_of(a, "body atom"));
+    for_atoms(bodyText, [&](std::string_view a) { r.body.push_back(atom_of(a, "body atom")); });
     r.head = atom_of(headText, "head atom");
     r.nVars = sc.nextVar;
     return r;
@@ -169,7 +185,9 @@ Rule RuleParser::parse_json(const std::string& json) const {
         std::string value = json_str(tj, "value");
         if (value.empty()) throw RuleError("JSON term missing 'value': " + tj);
         if (type == "variable") return var_term(value, sc);
-        return const_term(expand(value), sc);
+        std::string spelled;
+        expand(value, spelled);
+        return const_term(spelled, sc);
     };
     auto atom_of = [&](const std::string& aj) {
         size_t sp = aj.find("\"subject\"");

@@ -3,6 +3,7 @@
 #include <cstdint>
 #include <stdexcept>
 #include <string>
+#include <string_view>
 #include <unordered_map>
 #include <vector>
 
@@ -51,17 +52,19 @@ private:
     const TermDict& preds_;
     std::unordered_map<std::string, std::string> prefixes_;
 
-    std::string expand(const std::string& token) const;
+    // The token's IRI as the dictionaries spell it ('<...>' stripped, a
+    // known prefix expanded), written into `out`.
+    void expand(std::string_view token, std::string& out) const;
     // Names seen in one rule: a handful, so searched linearly.
     struct Scope {
         std::vector<std::pair<std::string, int32_t>> vars;
         std::vector<std::pair<std::string, int32_t>> unknown;
         int32_t nextVar = 0;
     };
-    Term var_term(const std::string& name, Scope& sc) const;
+    Term var_term(std::string_view name, Scope& sc) const;
     Term const_term(const std::string& spelled, Scope& sc) const;
-    Term text_term(const std::string& token, Scope& sc) const;
-    int32_t pred_id(const std::string& token) const;
+    Term text_term(std::string_view token, Scope& sc) const;
+    int32_t pred_id(std::string_view token) const;
 };
 
 }  // namespace gr
