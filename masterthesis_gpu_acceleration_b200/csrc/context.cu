@@ -938,9 +938,12 @@ void finish_load(Context* c) {
                              double* cost) -> const std::vector<uint8_t>* {
         auto it = c->memos.find(memo_key(p1, d1, p2, d2, p3, d3));
         if (it == c->memos.end() || !it->second) return nullptr;
-        // a memo word costs about a quarter of a candidate; a three-step item
-        // also looks up the rows its root reaches
-        *cost = it->second->words / 4.0 + (p3 >= 0 ? 32.0 : 8.0);
+        // a memo word costs about a quarter of a candidate; an item itself is
+        // a chain of dependent loads on one warp (exception lookups, searches
+        // of the hub row for bound values; a three-step item also looks up
+        // the rows its root reaches): c3 rule 963 (two steps, 4-word memos)
+        // measured ~12 us of block time per root against ~7 ns per candidate
+        *cost = it->second->words / 4.0 + (p3 >= 0 ? 512.0 : 256.0);
         return &it->second->rowHasMemo;
     };
     c->parser.reset(new RuleParser(c->ents, c->preds, c->prefixes));

@@ -84,7 +84,7 @@ uint64_t phase_hash(const PhasePlan& ph) {
 
 TaskBuilder::TaskBuilder(const HostIndex& ix)
     : ix_(ix), degAt_((size_t)std::max(ix.nPred, 0) * 2), sbFan_((size_t)std::max(ix.nPred, 0) * 2, 0.0),
-      hop2_(new Hop2Shard[kHop2Shards]) {
+      hop2_(new Hop2Shard[kHop2Shards]), trans_(new TransShard[kHop2Shards]) {
     for (auto& a : degAt_) a.store(nullptr, std::memory_order_relaxed);
     for (int32_t p = 0; p < ix.nPred; ++p)
         for (int dir = 0; dir < 2; ++dir) {
@@ -155,6 +155,49 @@ const TaskBuilder::Hop2& TaskBuilder::hop2(int32_t p0, int d0, int32_t p1, int d
     return ins.first->second;
 }
 
+double TaskBuilder::transition(int32_t p0, int d0, int32_t p1, int d1, bool capped) {
+    const uint64_t key = ((uint64_t)(uint32_t)p0 << 34) | ((uint64_t)d0 << 33) | ((uint64_t)(uint32_t)p1 << 2) |
+                         ((uint64_t)d1 << 1) | (capped ? 1u : 0u);
+    TransShard& sh = trans_[(key * 0x9E3779B97F4A7C15ull) >> 58];
+    {
+        std::shared_lock<std::shared_mutex> lk(sh.mu);
+        auto it = sh.map.find(key);
+        if (it != sh.map.end()) return it->second;
+    }
+    // an edge of (p0, d0) leads to v as often as v's row under (p0, 1 - d0)
+    // is long: one lookup per distinct v
+    const int rd = 1 - d0;
+    double n = 0, acc = 0;
+    for (int32_t r = ix_.predRow[rd][p0]; r < ix_.predRow[rd][p0 + 1]; ++r) {
+        const double c = ix_.rowBeg[rd][r + 1] - ix_.rowBeg[rd][r];
+        const auto rr = ix_.row_range(p1, d1, ix_.rowKey[rd][r]);
+        double d = rr.second - rr.first;
+        if (capped) d = std::min(d, (double)kHubMinDegree);
+        n += c;
+        acc += c * d;
+    }
+    const double mean = n > 0 ? acc / n : 0.0;
+    std::unique_lock<std::shared_mutex> lk(sh.mu);
+    sh.map.emplace(key, mean);
+    return mean;
+}
+
+double TaskBuilder::chain_tail(const DevPlan& P) {
+    double tail = 1.0;
+    for (int s = 2; s < P.m; ++s) {
+        const DevStep& st = P.steps[s];
+        const DevStep& pv = P.steps[s - 1];
+        double f;
+        if (st.kind == kExpand && pv.kind == kExpand && pv.nNew == 1 && st.keyRef == P.tupleLen[s - 1]) {
+            const bool capped = s == P.m - 1 && P.mode == kPairs && P.hoLevel == P.m && !ix_.hubOff.empty();
+            f = transition(pv.pred, pv.dir, st.pred, st.dir, capped);
+        } else
+            f = avg_fan(st);
+        tail *= std::max(1.0, f);
+    }
+    return tail;
+}
+
 bool TaskBuilder::chain_shaped(const DevPlan& P) const {
     return P.m >= 2 && P.steps[0].kind == kExpand && P.steps[1].kind == kExpand &&
            P.steps[1].keyRef == P.tupleLen[0] && (P.steps[0].keyRef < 0 || P.steps[0].keyRef < P.tupleLen[0]);
@@ -165,8 +208,7 @@ double TaskBuilder::estimate2(const PhasePlan& ph) {
     if (!chain_shaped(P)) return estimate(ph, false);
     const DevStep& s0 = P.steps[0];
     const DevStep& s1 = P.steps[1];
-    double tail = 1.0;
-    for (int s = 2; s < P.m; ++s) tail *= std::max(1.0, avg_fan(P.steps[s]));
+    const double tail = chain_tail(P);
     const Hop2& h = hop2(s0.pred, s0.dir, s1.pred, s1.dir);
     const bool allRows = P.rootKind == kRootRows && P.rootDir == s0.dir && P.rootPred == s0.pred &&
                          s0.keyRef == kTupleHead && ph.rootBeg == ix_.predRow[s0.dir][s0.pred] &&
@@ -237,8 +279,7 @@ const TaskBuilder::Walk& TaskBuilder::keep_walk(uint64_t sig, Walk&& wk) {
 
 TaskBuilder::Walk TaskBuilder::compute_walk(const PhasePlan& ph) {
     const DevPlan& P = ph.plan;
-    double tail = 1.0;
-    for (int s = 2; s < P.m; ++s) tail *= std::max(1.0, avg_fan(P.steps[s]));
+    const double tail = chain_tail(P);
     const bool chain = chain_shaped(P);
     const Hop2* h = chain ? &hop2(P.steps[0].pred, P.steps[0].dir, P.steps[1].pred, P.steps[1].dir) : nullptr;
     const int32_t* deg2 = (!chain && P.m >= 2 && P.steps[1].kind == kExpand) ? degrees(P.steps[1].pred, P.steps[1].dir) : nullptr;
@@ -308,7 +349,10 @@ void TaskBuilder::build(const std::vector<const PhasePlan*>& phases, int blocks,
         walks_.clear();
         deg_.clear();
         for (auto& a : degAt_) a.store(nullptr, std::memory_order_relaxed);
-        for (int k = 0; k < kHop2Shards; ++k) hop2_[k].map.clear();
+        for (int k = 0; k < kHop2Shards; ++k) {
+            hop2_[k].map.clear();
+            trans_[k].map.clear();
+        }
         cacheBytes_ = 0;
     }
     std::vector<double> estAvg(n), estHub(n), scale(n, defaultCalib_);
@@ -431,8 +475,7 @@ void TaskBuilder::build(const std::vector<const PhasePlan*>& phases, int blocks,
         // share of the phase: lighter ones cannot hold up its end, and each
         // cut costs host time per first-segment edge.
         const double splitAt = costAware ? std::max(target, pt.work * sc / std::max(blocks, 1)) : target;
-        double tail = 1.0;
-        for (int s = 2; s < P.m; ++s) tail *= std::max(1.0, avg_fan(P.steps[s]));
+        const double tail = chain_tail(P);
         const int32_t* deg2 =
             (canSplit && P.m >= 2 && P.steps[1].kind == kExpand) ? degrees(P.steps[1].pred, P.steps[1].dir) : nullptr;
         for (int32_t r = ph.rootBeg; r < ph.rootEnd; ++r) {

@@ -145,6 +145,12 @@ private:
         std::unordered_map<uint64_t, Hop2> map;
     };
     std::unique_ptr<Hop2Shard[]> hop2_;
+    // (p0, d0, p1, d1, capped) -> mean next degree per edge (see transition)
+    struct TransShard {
+        std::shared_mutex mu;
+        std::unordered_map<uint64_t, double> map;
+    };
+    std::unique_ptr<TransShard[]> trans_;
     std::unordered_map<uint64_t, double> calib_;                // phase hash -> ns per work unit
     std::unordered_map<uint64_t, bool> mustWalk_;               // phase hash -> walk next time
     double defaultCalib_ = 1.0;
@@ -162,6 +168,15 @@ private:
     const Hop2& hop2(int32_t p0, int d0, int32_t p1, int d1);
     // Plans whose second step is keyed by the value the first step binds.
     bool chain_shaped(const DevPlan& P) const;
+    // Mean row length under (p1, d1) of the value an edge of (p0, d0) leads
+    // to, over all edges of p0: the fan-out of a step reached through the
+    // step before it (hub-heavy relations make it far above the plain
+    // average).  capped: rows of kHubMinDegree edges or more count as
+    // kHubMinDegree (a hub row of a body-size leaf is OR-ed a word at a time).
+    double transition(int32_t p0, int d0, int32_t p1, int d1, bool capped);
+    // Work per level-2 item: the product of the fan-outs of steps 2..m-1,
+    // each through the step before it where the plan chains them.
+    double chain_tail(const DevPlan& P);
     // Exact work of the first two levels times average fan-outs beyond, for
     // chain-shaped plans whose roots are the first step's rows; otherwise
     // the average-fan-out estimate.
