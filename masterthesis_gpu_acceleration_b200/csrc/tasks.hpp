@@ -168,12 +168,6 @@ private:
     const Hop2& hop2(int32_t p0, int d0, int32_t p1, int d1);
     // Plans whose second step is keyed by the value the first step binds.
     bool chain_shaped(const DevPlan& P) const;
-    // Mean row length under (p1, d1) of the value an edge of (p0, d0) leads
-    // to, over all edges of p0: the fan-out of a step reached through the
-    // step before it (hub-heavy relations make it far above the plain
-    // average).  capped: rows of kHubMinDegree edges or more count as
-    // kHubMinDegree (a hub row of a body-size leaf is OR-ed a word at a time).
-    double transition(int32_t p0, int d0, int32_t p1, int d1, bool capped);
     // Work per level-2 item: the product of the fan-outs of steps 2..m-1,
     // each through the step before it where the plan chains them.
     double chain_tail(const DevPlan& P);
@@ -190,6 +184,13 @@ private:
     double child_work(const DevPlan& P, const int32_t* rootVals, int32_t e, const int32_t* deg2, double tail) const;
 
 public:
+    // Mean row length under (p1, d1) of the value an edge of (p0, d0) leads
+    // to, over all edges of p0: the fan-out of a step reached through the
+    // step before it (hub-heavy relations make it far above the plain
+    // average).  capped: rows of kHubMinDegree edges or more count as
+    // kHubMinDegree (a hub row of a body-size leaf is OR-ed a word at a time).
+    // Cached; safe to call from several threads.
+    double transition(int32_t p0, int d0, int32_t p1, int d1, bool capped);
     // The bound values of root r and the edge range of its first step: the
     // range a split root's slices [sub0, sub1) partition.
     int root_vals(const DevPlan& P, int32_t r, int32_t* vals) const;

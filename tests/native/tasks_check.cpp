@@ -7,7 +7,12 @@
 //   * hold at most the plan's group of roots per plain task (the size its
 //     dedup bitmap is laid out for);
 //   * give every split root its own global row, numbered 0 .. heavyRows-1.
+// It also checks the chained fan-out (TaskBuilder::transition) of every pair
+// of consecutive expand steps against a direct mean over the first step's
+// edges, capped and uncapped.
 // Usage: tasks_check GRAPH.ttl RULES.txt
+#include <algorithm>
+#include <cmath>
 #include <cstdio>
 #include <fstream>
 #include <map>
@@ -63,6 +68,37 @@ long check_phase(TaskBuilder& tb, const PhasePlan& ph, const PhaseTasks& pt, int
     }
     for (int c : cover) if (c != 1) ++bad;
     for (int u : rowUse) if (u != 1) ++bad;
+    return bad;
+}
+
+// Mean row length under (p1, d1) of val[d0][e] over every edge e of p0,
+// straight from the edge arrays.
+double direct_transition(const HostIndex& ix, int32_t p0, int d0, int32_t p1, int d1, bool capped) {
+    double n = 0, acc = 0;
+    for (int32_t r = ix.predRow[d0][p0]; r < ix.predRow[d0][p0 + 1]; ++r)
+        for (int32_t e = ix.rowBeg[d0][r]; e < ix.rowBeg[d0][r + 1]; ++e) {
+            const auto rr = ix.row_range(p1, d1, ix.val[d0][e]);
+            double d = rr.second - rr.first;
+            if (capped) d = std::min(d, (double)kHubMinDegree);
+            n += 1;
+            acc += d;
+        }
+    return n > 0 ? acc / n : 0.0;
+}
+
+long check_transitions(TaskBuilder& tb, const HostIndex& ix, const DevPlan& P, size_t& checked) {
+    long bad = 0;
+    for (int s = 1; s < P.m; ++s) {
+        const DevStep& a = P.steps[s - 1];
+        const DevStep& b = P.steps[s];
+        if (a.kind != kExpand || b.kind != kExpand) continue;
+        for (bool capped : {false, true}) {
+            const double got = tb.transition(a.pred, a.dir, b.pred, b.dir, capped);
+            const double want = direct_transition(ix, a.pred, a.dir, b.pred, b.dir, capped);
+            if (std::fabs(got - want) > 1e-9 * std::max(1.0, want)) ++bad;
+            ++checked;
+        }
+    }
     return bad;
 }
 
@@ -127,6 +163,12 @@ int main(int argc, char** argv) {
             if (!one.empty()) run(tb, one, 4.0e6, true);
         }
     }
-    std::printf("phases %zu tasks %zu split roots %zu violations %ld\n", phases.size(), tasks, splitRoots, bad);
+    size_t transitions = 0;
+    {   // chained fan-outs against the edge arrays
+        TaskBuilder tb(ix);
+        for (const PhasePlan* ph : phases) bad += check_transitions(tb, ix, ph->plan, transitions);
+    }
+    std::printf("phases %zu tasks %zu split roots %zu transitions %zu violations %ld\n", phases.size(), tasks,
+                splitRoots, transitions, bad);
     return bad == 0 ? 0 : 1;
 }
