@@ -406,11 +406,16 @@ void Context::ensure_memos(const std::vector<std::array<int, 6>>& keys, cudaStre
         const int p1 = fresh[i][0], d1 = fresh[i][1], p2 = fresh[i][2], d2 = fresh[i][3];
         const int p3 = fresh[i][4], d3 = fresh[i][5];
         const int words = (int)((domain(fresh[i]) + 31) / 32);
-        const int32_t* deg = tasks->degrees(p3 >= 0 ? p3 : p2, p3 >= 0 ? d3 : d2);
+        const double need = memoGain * words;
+        // the count only grows: a row stops being summed once it qualifies
+        // (a hub row's own values mostly do), and the degree array is made
+        // only for a row that needs it
+        const int32_t* deg = nullptr;
         for (int32_t r = h.predRow[d1][p1]; r < h.predRow[d1][p1 + 1]; ++r) {
             if (h.hubOf[d1][r] < 0) continue;
             double cand = (double)(h.rowBeg[d1][r + 1] - h.rowBeg[d1][r]);
-            for (int32_t e = h.rowBeg[d1][r]; e < h.rowBeg[d1][r + 1]; ++e) {
+            for (int32_t e = h.rowBeg[d1][r]; e < h.rowBeg[d1][r + 1] && cand < need; ++e) {
+                if (!deg) deg = tasks->degrees(p3 >= 0 ? p3 : p2, p3 >= 0 ? d3 : d2);
                 if (p3 < 0) {
                     cand += deg[h.val[d1][e]];
                 } else {
@@ -418,7 +423,7 @@ void Context::ensure_memos(const std::vector<std::array<int, 6>>& keys, cudaStre
                     for (int32_t e2 = r2.first; e2 < r2.second; ++e2) cand += 1.0 + deg[h.val[d2][e2]];
                 }
             }
-            if (cand >= memoGain * words) rowsOf[i].push_back(r);
+            if (cand >= need) rowsOf[i].push_back(r);
         }
     }, 1);
     // per memo slot: S1 and S2 (two steps), or S1 and one count per rank
