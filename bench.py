@@ -517,7 +517,7 @@ def engine_arm(args):
 
     # ---- end to end through the C ABI with host strings (warm: the rules
     # were prepared and autotuned on this context above) ----
-    for _ in range(max(1, args.warmup // 2)):
+    for _ in range(max(1, args.warmup)):
         lib.evaluate_rules_batch(rules)
     barrier()
     t0 = time.perf_counter()
